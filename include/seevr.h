@@ -1,0 +1,245 @@
+/*
+ * seevr.h — C ABI of libseevr_cuda, the sm_100a rigid-body physics step.
+ *
+ * This library replaces the Vulkan dispatches of seeVR's physics step.  The
+ * entry points below are what the Zig host (src/physics.zig, src/bvh.zig)
+ * binds in place of its compute pipeline; each declaration names the
+ * reference interface it replaces.
+ *
+ * Conventions
+ *  - Every function returns seevr_status (0 = OK) and never aborts.  A
+ *    human-readable message for the last failure on the calling thread is
+ *    available from seevr_last_error().
+ *  - Device buffers are owned by the caller (CUDA device pointers).  The
+ *    library owns only its scratch space (pair/contact staging, scans, sort
+ *    and solver work arrays) and frees it in seevr_physics_destroy().
+ *  - Buffer layout is the SoA layout of src/data.zig:31-121 (packed float3,
+ *    quaternions xyzw, geom_data 8 floats per geom with [0]=hull_start and
+ *    [1]=hull_count stored as float).
+ *  - One handle per host thread; handles are not reentrant.
+ */
+#ifndef SEEVR_H
+#define SEEVR_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SEEVR_ABI_VERSION 1
+
+typedef enum seevr_status {
+    SEEVR_OK = 0,
+    SEEVR_ERR_INVALID_ARGUMENT = 1, /* NULL/undersized buffer, bad count      */
+    SEEVR_ERR_CAPACITY = 2,         /* pairs or contacts overflowed the caps;
+                                       the step completed with the first
+                                       max_pairs/max_contacts in canonical
+                                       order, counters hold the true totals  */
+    SEEVR_ERR_CUDA = 3,             /* a CUDA runtime call failed            */
+    SEEVR_ERR_TIMEOUT = 4,          /* a bounded device-side wait gave up    */
+    SEEVR_ERR_NO_DEVICE = 5,        /* no usable CUDA device                 */
+    SEEVR_ERR_OUT_OF_MEMORY = 6,    /* scratch allocation failed             */
+    SEEVR_ERR_NOT_SUPPORTED = 7     /* option combination not implemented    */
+} seevr_status;
+
+/* Binding indices: identical to the `binding=` numbers of physics.comp:16-57
+ * and to the buffer order of Physics.init (physics.zig:37-68). */
+enum seevr_binding {
+    SEEVR_B_BODY_POS = 0,          /* f32[N*3]            rw */
+    SEEVR_B_BODY_QUAT = 1,         /* f32[N*4] xyzw       rw */
+    SEEVR_B_BODY_VEL = 2,          /* f32[N*3]            rw */
+    SEEVR_B_BODY_OMEGA = 3,        /* f32[N*3]            rw */
+    SEEVR_B_BODY_INV_MASS = 4,     /* f32[N]              r  */
+    SEEVR_B_BODY_INV_INERTIA = 5,  /* f32[N*3] local diag r  */
+    SEEVR_B_BODY_VERT_START = 6,   /* u32[N]              r  */
+    SEEVR_B_BODY_VERT_COUNT = 7,   /* u32[N]              r  */
+    SEEVR_B_GEOM_BODY_IDX = 8,     /* u32[G]              r  */
+    SEEVR_B_GEOM_DATA = 9,         /* f32[G*8]            r  */
+    SEEVR_B_GEOM_FRICTION = 10,    /* f32[G]              r  */
+    SEEVR_B_GEOM_RESTITUTION = 11, /* f32[G]              r  */
+    SEEVR_B_HULL_VERTS = 12,       /* f32[HV*3] local     r  */
+    SEEVR_B_VERTICES = 13,         /* f32[V*3] world      w  */
+    SEEVR_B_ORIG_VERTICES = 14,    /* f32[V*3] local      r  */
+    SEEVR_B_CONTACT_POS = 15,      /* f32[MAXC*3]         w  */
+    SEEVR_B_CONTACT_NORMAL = 16,   /* f32[MAXC*3]         w  */
+    SEEVR_B_CONTACT_PEN = 17,      /* f32[MAXC]           w  */
+    SEEVR_B_CONTACT_GEOM_A = 18,   /* u32[MAXC]           w  */
+    SEEVR_B_CONTACT_GEOM_B = 19,   /* u32[MAXC]           w  */
+    SEEVR_B_LAMBDA_N = 20,         /* f32[MAXC]           w  */
+    SEEVR_B_COUNTERS = 21,         /* u32[4] [0]=pairs [1]=contacts         */
+    SEEVR_B_BODY_AABB_MIN = 22,    /* f32[N*3]            w  */
+    SEEVR_B_BODY_AABB_MAX = 23,    /* f32[N*3]            w  */
+    SEEVR_B_COLLISION_PAIRS = 24,  /* u32[MAXP*2]         w  */
+    SEEVR_B_AABB_TEMP_MIN = 25,    /* unused: the segmented AABB reduce needs
+                                      no cascade temp (may be NULL)          */
+    SEEVR_B_AABB_TEMP_MAX = 26,    /* unused (may be NULL)                   */
+    SEEVR_B_AABB_TEMP_BODY = 27,   /* unused (may be NULL)                   */
+    SEEVR_B_SUPPORT_OFFSET = 28,   /* u32[G] 0 = brute force                 */
+    SEEVR_B_SUPPORT_LOOKUP = 29,   /* u32[1+192*k]                           */
+    /* Extension (no reference binding): u32[G*2] (hull_start, hull_count)
+     * per geom.  geom_data stores hull_start as a float (data.zig:468-473),
+     * exact only below 2^24 hull vertices; when this pointer is non-NULL it
+     * replaces geom_data[0..1].  May be NULL. */
+    SEEVR_B_HULL_RANGE = 30,
+    SEEVR_NUM_BINDINGS = 31
+};
+
+/* The 30 storage buffers of Physics.init (physics.zig:37-68) plus the
+ * optional hull-range extension: device pointer and size in bytes,
+ * index == binding. */
+typedef struct seevr_bindings {
+    void* ptr[SEEVR_NUM_BINDINGS];
+    uint64_t bytes[SEEVR_NUM_BINDINGS];
+} seevr_bindings;
+
+/* Capacities.  The reference hard-codes them (data.zig:11-18 and
+ * physics.comp:69-70); here they are per handle. */
+typedef struct seevr_caps {
+    uint32_t max_bodies;     /* MAX_BODIES (data.zig:13)            */
+    uint32_t max_hull_verts; /* MAX_HULL_VERTS (data.zig:17)        */
+    uint32_t max_vertices;   /* MAX_VERTICES (data.zig:11)          */
+    uint32_t max_pairs;      /* MAX_COLLISION_PAIRS (data.zig:16)   */
+    uint32_t max_contacts;   /* MAX_CONTACTS (data.zig:15)          */
+    uint32_t max_scenes;     /* independent scenes per handle (>=1) */
+} seevr_caps;
+
+enum seevr_broadphase {
+    SEEVR_BROADPHASE_N2 = 0,   /* all-pairs per scene (physics.comp:451-472) */
+    SEEVR_BROADPHASE_LBVH = 1  /* Morton/radix/Karras tree (bvh.comp spec)   */
+};
+
+enum seevr_solver {
+    SEEVR_SOLVER_SEQUENTIAL = 0, /* one thread per scene, contacts in order
+                                    (physics.comp:500-583)                   */
+    SEEVR_SOLVER_WAVEFRONT = 1,  /* same contact order, independent contacts
+                                    run in parallel waves: bit-identical to
+                                    SEQUENTIAL                               */
+    SEEVR_SOLVER_COLORED = 2     /* graph-coloured Gauss-Seidel: a different
+                                    contact order, judged by drift          */
+};
+
+enum seevr_flags {
+    SEEVR_FLAG_NO_SYNC = 1u << 0,      /* do not synchronize before return  */
+    SEEVR_FLAG_CUDA_GRAPH = 1u << 1,   /* capture the frame once, replay    */
+    SEEVR_FLAG_SKIP_RENDER_VERTS = 1u << 2 /* omit step 7 (update_verts)    */
+};
+
+/* Solver and collision constants.  Defaults equal the reference constants. */
+typedef struct seevr_params {
+    uint32_t pgs_iterations;   /* PGS_ITERATIONS = 4 (physics.comp:68)      */
+    float baumgarte;           /* BAUMGARTE = 0.2 (physics.comp:66)         */
+    float slop;                /* SLOP = 0.005 (physics.comp:67)            */
+    float linear_damping;      /* 0.999 (physics.comp:422-424)              */
+    float angular_damping;     /* 0.998 (physics.comp:425-427)              */
+    float mpr_eps;             /* CCD_EPS = 1e-6 (physics.comp:174)         */
+    float mpr_tolerance;       /* CCD_TOLERANCE = 1e-6 (physics.comp:175)   */
+    uint32_t mpr_iterations;   /* CCD_ITERATIONS = 50 (physics.comp:176)    */
+    uint32_t mpr_discover_trials; /* 15 (physics.comp:290)                  */
+    uint32_t broadphase;       /* enum seevr_broadphase                     */
+    uint32_t solver;           /* enum seevr_solver                         */
+    uint32_t flags;            /* enum seevr_flags                          */
+} seevr_params;
+
+/* Per-stage device timings in milliseconds, summed over the substeps of one
+ * call.  Section names follow Physics.step_names (physics.zig:22-32). */
+#define SEEVR_NUM_STAGES 9
+typedef struct seevr_profile {
+    float ms[SEEVR_NUM_STAGES];
+    uint32_t calls;
+} seevr_profile;
+/* Stage order inside seevr_profile.ms: gravity, aabb, broad_phase,
+ * narrow_phase, clear_impulse, pgs_solve, integrate, render_verts,
+ * clear_counters — the order of physics.zig:22-32. */
+
+typedef struct seevr_physics seevr_physics;
+
+/* Fill *p with the reference constants. */
+void seevr_params_default(seevr_params* p);
+
+/* Replaces Physics.init(vk, data, allocator, prof) (physics.zig:34-78):
+ * binds the caller's buffers and allocates scratch sized by *caps.
+ * The handle is bound to the CUDA device current on the calling thread. */
+seevr_status seevr_physics_create(const seevr_bindings* bindings,
+                                  const seevr_caps* caps,
+                                  const seevr_params* params,
+                                  seevr_physics** out);
+
+/* Declare independent scenes: scene s owns bodies
+ * [body_offset[s], body_offset[s+1]) (host array of num_scenes+1 entries,
+ * body_offset[0] = 0, non-decreasing).  Bodies of different scenes never
+ * collide.  Without this call a handle steps one scene.  No counterpart in
+ * the reference (it steps one scene, physics.zig:80). */
+seevr_status seevr_physics_set_scenes(seevr_physics* h,
+                                      const uint32_t* body_offset,
+                                      uint32_t num_scenes);
+
+/* Replaces Physics.step(num_bodies, num_vertices, num_hull_verts, substeps,
+ * dt, gravity, prof) (physics.zig:80-165): `substeps` substeps of
+ * sub_dt = dt/substeps, each running gravity, AABB, broadphase, MPR
+ * narrowphase, impulse clear, PGS and integration, then one render-vertex
+ * update.  Synchronous unless SEEVR_FLAG_NO_SYNC; `prof` may be NULL (fast
+ * mode, physics.zig:118-164) or receive per-stage device timings
+ * (profiling mode, physics.zig:97-117). */
+seevr_status seevr_physics_step(seevr_physics* h,
+                                uint32_t num_bodies,
+                                uint32_t num_vertices,
+                                uint32_t num_hull_verts,
+                                uint32_t substeps,
+                                float dt,
+                                const float gravity[3],
+                                seevr_profile* prof);
+
+/* Same as seevr_physics_step, ordered on `stream` (a cudaStream_t) and never
+ * synchronizing; `frames` consecutive calls are issued back to back.  With
+ * SEEVR_FLAG_CUDA_GRAPH the frame is captured into a CUDA graph on first
+ * use and replayed (re-captured when an argument changes).  No counterpart
+ * in the reference. */
+seevr_status seevr_physics_step_async(seevr_physics* h,
+                                      uint32_t num_bodies,
+                                      uint32_t num_vertices,
+                                      uint32_t num_hull_verts,
+                                      uint32_t substeps,
+                                      float dt,
+                                      const float gravity[3],
+                                      uint32_t frames,
+                                      void* stream);
+
+/* Replaces Physics.readCounters (physics.zig:213-217): out[0] = pairs found,
+ * out[1] = contacts found, in the last substep (true totals, may exceed the
+ * caps). */
+seevr_status seevr_physics_read_counters(seevr_physics* h, uint32_t out[2]);
+
+/* Overflow and error flags accumulated since the last call (bit 0: pairs
+ * overflowed, bit 1: contacts overflowed, bit 2: a device wait timed out,
+ * bit 3: a scene exceeded the solver's per-scene limits and took the
+ * global-memory path).  Cleared by the call. */
+seevr_status seevr_physics_read_flags(seevr_physics* h, uint32_t* flags);
+
+/* Copy the mutable body state between host memory and the bound device
+ * buffers (pos, quat, vel, omega of num_bodies bodies), ordered on the
+ * handle's stream and synchronous.  Mirrors Data.upload (data.zig:599-611)
+ * and Vulkan.readBuffer (vulkan.zig:317-328) for the state the step
+ * changes; any pointer may be NULL to skip that array. */
+seevr_status seevr_physics_upload_state(seevr_physics* h, uint32_t num_bodies,
+                                        const float* pos, const float* quat,
+                                        const float* vel, const float* omega);
+seevr_status seevr_physics_download_state(seevr_physics* h, uint32_t num_bodies,
+                                          float* pos, float* quat,
+                                          float* vel, float* omega);
+
+/* Replaces Physics.deinit (physics.zig:219-221). */
+void seevr_physics_destroy(seevr_physics* h);
+
+/* Number of kernels the library launched on this handle since creation. */
+uint64_t seevr_physics_kernel_launches(const seevr_physics* h);
+
+const char* seevr_status_string(seevr_status s);
+const char* seevr_last_error(void);
+int seevr_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SEEVR_H */

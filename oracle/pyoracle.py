@@ -1,0 +1,172 @@
+"""TEST INFRASTRUCTURE — ctypes wrapper of oracle/liboracle.so, the CPU
+restatement of seeVR's physics.comp / bvh.comp (seevr_oracle.hpp).
+
+Only tests, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
+module, as the checker.  Parity is unpinned against reference outputs (the
+reference has no tests or fixtures and cannot run here); see the header of
+seevr_oracle.hpp.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "liboracle.so"
+
+_f = C.POINTER(C.c_float)
+_u = C.POINTER(C.c_uint32)
+_d = C.POINTER(C.c_double)
+
+
+class OracleScene(C.Structure):
+    _fields_ = [("num_bodies", C.c_uint32), ("num_geoms", C.c_uint32),
+                ("num_hull_verts", C.c_uint32), ("num_vertices", C.c_uint32),
+                ("num_scenes", C.c_uint32),
+                ("body_pos", _f), ("body_quat", _f), ("body_vel", _f), ("body_omega", _f),
+                ("body_inv_mass", _f), ("body_inv_inertia", _f),
+                ("body_vert_start", _u), ("body_vert_count", _u), ("geom_body_idx", _u),
+                ("geom_data", _f), ("geom_friction", _f), ("geom_restitution", _f),
+                ("hull_verts", _f), ("orig_verts", _f),
+                ("support_offset", _u), ("support_lookup", _u), ("scene_body_offset", _u),
+                ("hull_range", _u)]
+
+
+class OracleParams(C.Structure):
+    _fields_ = [("pgs_iterations", C.c_uint32), ("baumgarte", C.c_float), ("slop", C.c_float),
+                ("lin_damp", C.c_float), ("ang_damp", C.c_float), ("eps", C.c_float),
+                ("tol", C.c_float), ("mpr_iterations", C.c_uint32),
+                ("discover_trials", C.c_uint32), ("max_pairs", C.c_uint32),
+                ("max_contacts", C.c_uint32)]
+
+
+class OracleOut(C.Structure):
+    _fields_ = [("pos", _d), ("quat", _d), ("vel", _d), ("omega", _d),
+                ("aabb_min", _d), ("aabb_max", _d), ("verts", _d), ("pairs", _u),
+                ("c_pos", _d), ("c_normal", _d), ("c_pen", _d), ("lambda_", _d),
+                ("c_a", _u), ("c_b", _u), ("counters", C.c_uint32 * 2),
+                ("ops", C.c_uint64 * 10)]
+
+
+OP_NAMES = ("support_brute", "support_brute_verts", "support_lookup", "mpr_calls",
+            "mpr_support_calls", "pgs_contact_iters", "pgs_friction_iters", "aabb_verts",
+            "broad_tests", "body_substeps")
+
+
+def _load():
+    if not LIB_PATH.exists():
+        subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    lib = C.CDLL(str(LIB_PATH))
+    lib.oracle_run.restype = C.c_int
+    lib.oracle_run.argtypes = [C.POINTER(OracleScene), C.POINTER(OracleParams), C.c_int,
+                               C.c_uint32, C.c_uint32, C.c_float, _f, C.c_int, C.c_int,
+                               C.POINTER(OracleOut)]
+    lib.oracle_morton.argtypes = [_f, C.c_uint32, _u, _f]
+    lib.oracle_radix_sort.argtypes = [_u, C.c_uint32, _u, _u]
+    lib.oracle_karras.argtypes = [_u, C.c_uint32, _u, _u, _u]
+    lib.oracle_atan2f.restype = C.c_float
+    lib.oracle_atan2f.argtypes = [C.c_float, C.c_float]
+    lib.oracle_atan2d.restype = C.c_double
+    lib.oracle_atan2d.argtypes = [C.c_double, C.c_double]
+    lib.oracle_num_threads.restype = C.c_int
+    return lib
+
+
+lib = _load()
+
+
+def _p(a, t):
+    return a.ctypes.data_as(t) if a is not None else None
+
+
+def run(arrays: dict, *, frames=1, substeps=10, dt=1.0 / 60.0, gravity=(0.0, -9.81, 0.0),
+        pgs_iterations=4, max_pairs=10000, max_contacts=4000, precision=32,
+        update_verts=True, threads=0, use_hull_range=True, **consts) -> dict:
+    """Run `frames` Physics.step calls on a copy of the scene `arrays`
+    (Data.arrays()).  Returns final state and last-substep outputs (float64)."""
+    a = {k: np.ascontiguousarray(v) for k, v in arrays.items()}
+    nb = len(a["body_inv_mass"])
+    ng = len(a["geom_body_idx"])
+    nhv = len(a["hull_verts"])
+    nv = len(a["orig_vertices"]) if update_verts else 0
+    off = a.get("scene_body_offset")
+    ns = len(off) - 1 if off is not None and len(off) > 1 else 1
+    s = OracleScene(nb, ng, nhv, nv, ns,
+                    _p(a["body_pos"], _f), _p(a["body_quat"], _f), _p(a["body_vel"], _f),
+                    _p(a["body_omega"], _f), _p(a["body_inv_mass"], _f),
+                    _p(a["body_inv_inertia"], _f), _p(a["body_vert_start"], _u),
+                    _p(a["body_vert_count"], _u), _p(a["geom_body_idx"], _u),
+                    _p(a["geom_data"], _f), _p(a["geom_friction"], _f),
+                    _p(a["geom_restitution"], _f), _p(a["hull_verts"], _f),
+                    _p(a["orig_vertices"], _f) if nv else None,
+                    _p(a["support_offset"], _u), _p(a["support_lookup"], _u),
+                    _p(off, _u) if off is not None and len(off) > 1 else None,
+                    _p(a["hull_range"], _u) if use_hull_range and "hull_range" in a else None)
+    P = OracleParams(pgs_iterations, consts.get("baumgarte", 0.2), consts.get("slop", 0.005),
+                     consts.get("lin_damp", 0.999), consts.get("ang_damp", 0.998),
+                     consts.get("eps", 1e-6), consts.get("tol", 1e-6),
+                     consts.get("mpr_iterations", 50), consts.get("discover_trials", 15),
+                     max_pairs, max_contacts)
+    out = {
+        "pos": np.zeros((nb, 3)), "quat": np.zeros((nb, 4)), "vel": np.zeros((nb, 3)),
+        "omega": np.zeros((nb, 3)), "aabb_min": np.zeros((nb, 3)), "aabb_max": np.zeros((nb, 3)),
+        "verts": np.zeros((max(nv, 1), 3)), "pairs": np.zeros((max_pairs, 2), np.uint32),
+        "c_pos": np.zeros((max_contacts, 3)), "c_normal": np.zeros((max_contacts, 3)),
+        "c_pen": np.zeros(max_contacts), "lambda": np.zeros(max_contacts),
+        "c_a": np.zeros(max_contacts, np.uint32), "c_b": np.zeros(max_contacts, np.uint32),
+    }
+    o = OracleOut(_p(out["pos"], _d), _p(out["quat"], _d), _p(out["vel"], _d),
+                  _p(out["omega"], _d), _p(out["aabb_min"], _d), _p(out["aabb_max"], _d),
+                  _p(out["verts"], _d), _p(out["pairs"], _u), _p(out["c_pos"], _d),
+                  _p(out["c_normal"], _d), _p(out["c_pen"], _d), _p(out["lambda"], _d),
+                  _p(out["c_a"], _u), _p(out["c_b"], _u))
+    g = (C.c_float * 3)(*gravity)
+    rc = lib.oracle_run(C.byref(s), C.byref(P), precision, frames, substeps, dt, g,
+                        1 if nv else 0, threads, C.byref(o))
+    if rc != 0:
+        raise RuntimeError(f"oracle_run failed ({rc})")
+    npairs, ncont = int(o.counters[0]), int(o.counters[1])
+    out["num_pairs"], out["num_contacts"] = npairs, ncont
+    out["pairs"] = out["pairs"][: min(npairs, max_pairs)]
+    for k in ("c_pos", "c_normal", "c_pen", "lambda", "c_a", "c_b"):
+        out[k] = out[k][: min(ncont, max_contacts)]
+    out["verts"] = out["verts"][:nv]
+    out["ops"] = dict(zip(OP_NAMES, [int(x) for x in o.ops]))
+    return out
+
+
+def morton(centroids: np.ndarray):
+    c = np.ascontiguousarray(centroids, dtype=np.float32).reshape(-1, 3)
+    codes = np.zeros(len(c), np.uint32)
+    bounds = np.zeros(6, np.float32)
+    lib.oracle_morton(_p(c, _f), len(c), _p(codes, _u), _p(bounds, _f))
+    return codes, bounds
+
+
+def radix_sort(codes: np.ndarray):
+    k = np.ascontiguousarray(codes, dtype=np.uint32)
+    s = np.zeros_like(k)
+    perm = np.zeros_like(k)
+    lib.oracle_radix_sort(_p(k, _u), len(k), _p(s, _u), _p(perm, _u))
+    return s, perm
+
+
+def karras(sorted_codes: np.ndarray):
+    m = np.ascontiguousarray(sorted_codes, dtype=np.uint32)
+    n = len(m)
+    left = np.zeros(2 * n - 1, np.uint32)
+    right = np.zeros(2 * n - 1, np.uint32)
+    parent = np.zeros(2 * n - 1, np.uint32)
+    lib.oracle_karras(_p(m, _u), n, _p(left, _u), _p(right, _u), _p(parent, _u))
+    return left, right, parent
+
+
+def atan2f(y: float, x: float) -> float:
+    return float(lib.oracle_atan2f(y, x))
+
+
+def atan2d(y: float, x: float) -> float:
+    return float(lib.oracle_atan2d(y, x))

@@ -1,0 +1,136 @@
+"""ctypes binding of libseevr_cuda.so (include/seevr.h, include/seevr_scene.h).
+
+The library is built in-tree by ``python -m seevr_b200.build``.  There is no
+fallback: importing this module without the built library raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libseevr_cuda.so"
+
+NUM_BINDINGS = 31
+NUM_STAGES = 9
+STAGE_NAMES = (  # physics.zig:22-32
+    "phys/gravity", "phys/aabb", "phys/broad_phase", "phys/narrow_phase",
+    "phys/clear_impulse", "phys/pgs_solve", "phys/integrate", "phys/render_verts",
+    "phys/clear_counters",
+)
+
+# seevr_status
+OK, ERR_INVALID_ARGUMENT, ERR_CAPACITY, ERR_CUDA, ERR_TIMEOUT, ERR_NO_DEVICE, \
+    ERR_OUT_OF_MEMORY, ERR_NOT_SUPPORTED = range(8)
+
+BROADPHASE_N2, BROADPHASE_LBVH = 0, 1
+SOLVER_SEQUENTIAL, SOLVER_WAVEFRONT, SOLVER_COLORED = 0, 1, 2
+FLAG_NO_SYNC, FLAG_CUDA_GRAPH, FLAG_SKIP_RENDER_VERTS = 1, 2, 4
+
+# binding indices (physics.comp:16-57 + extension 30)
+(B_BODY_POS, B_BODY_QUAT, B_BODY_VEL, B_BODY_OMEGA, B_BODY_INV_MASS, B_BODY_INV_INERTIA,
+ B_BODY_VERT_START, B_BODY_VERT_COUNT, B_GEOM_BODY_IDX, B_GEOM_DATA, B_GEOM_FRICTION,
+ B_GEOM_RESTITUTION, B_HULL_VERTS, B_VERTICES, B_ORIG_VERTICES, B_CONTACT_POS,
+ B_CONTACT_NORMAL, B_CONTACT_PEN, B_CONTACT_GEOM_A, B_CONTACT_GEOM_B, B_LAMBDA_N,
+ B_COUNTERS, B_BODY_AABB_MIN, B_BODY_AABB_MAX, B_COLLISION_PAIRS, B_AABB_TEMP_MIN,
+ B_AABB_TEMP_MAX, B_AABB_TEMP_BODY, B_SUPPORT_OFFSET, B_SUPPORT_LOOKUP,
+ B_HULL_RANGE) = range(31)
+
+
+class Bindings(C.Structure):
+    _fields_ = [("ptr", C.c_void_p * NUM_BINDINGS), ("bytes", C.c_uint64 * NUM_BINDINGS)]
+
+
+class Caps(C.Structure):
+    _fields_ = [("max_bodies", C.c_uint32), ("max_hull_verts", C.c_uint32),
+                ("max_vertices", C.c_uint32), ("max_pairs", C.c_uint32),
+                ("max_contacts", C.c_uint32), ("max_scenes", C.c_uint32)]
+
+
+class Params(C.Structure):
+    _fields_ = [("pgs_iterations", C.c_uint32), ("baumgarte", C.c_float), ("slop", C.c_float),
+                ("linear_damping", C.c_float), ("angular_damping", C.c_float),
+                ("mpr_eps", C.c_float), ("mpr_tolerance", C.c_float),
+                ("mpr_iterations", C.c_uint32), ("mpr_discover_trials", C.c_uint32),
+                ("broadphase", C.c_uint32), ("solver", C.c_uint32), ("flags", C.c_uint32)]
+
+
+class Profile(C.Structure):
+    _fields_ = [("ms", C.c_float * NUM_STAGES), ("calls", C.c_uint32)]
+
+
+class SeevrError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"seevr status {status}: {message}")
+        self.status = status
+
+
+def _load():
+    if not LIB_PATH.exists():
+        raise ImportError(f"{LIB_PATH} is not built; run `python -m seevr_b200.build`")
+    lib = C.CDLL(str(LIB_PATH))
+    P, U32, U64, F, I = C.c_void_p, C.c_uint32, C.c_uint64, C.c_float, C.c_int
+    FP = C.POINTER(C.c_float)
+    UP = C.POINTER(C.c_uint32)
+    sig = {
+        "seevr_params_default": (None, [C.POINTER(Params)]),
+        "seevr_physics_create": (I, [C.POINTER(Bindings), C.POINTER(Caps), C.POINTER(Params),
+                                     C.POINTER(P)]),
+        "seevr_physics_set_scenes": (I, [P, UP, U32]),
+        "seevr_physics_step": (I, [P, U32, U32, U32, U32, F, FP, C.POINTER(Profile)]),
+        "seevr_physics_step_async": (I, [P, U32, U32, U32, U32, F, FP, U32, P]),
+        "seevr_physics_read_counters": (I, [P, UP]),
+        "seevr_physics_read_flags": (I, [P, UP]),
+        "seevr_physics_upload_state": (I, [P, U32, P, P, P, P]),
+        "seevr_physics_download_state": (I, [P, U32, P, P, P, P]),
+        "seevr_physics_destroy": (None, [P]),
+        "seevr_physics_kernel_launches": (U64, [P]),
+        "seevr_status_string": (C.c_char_p, [I]),
+        "seevr_last_error": (C.c_char_p, []),
+        "seevr_abi_version": (I, []),
+        # scene builder
+        "seevr_scene_create": (P, []),
+        "seevr_scene_destroy": (None, [P]),
+        "seevr_scene_begin": (None, [P]),
+        "seevr_scene_add_material": (U32, [P, FP, F, F, FP, F, F]),
+        "seevr_scene_add_box": (U32, [P, FP, FP, FP, F, F, U32]),
+        "seevr_scene_add_sphere": (U32, [P, FP, F, FP, U32, F, F, U32]),
+        "seevr_scene_add_hull": (U32, [P, FP, FP, U32, FP, F, F, U32]),
+        "seevr_scene_set_body_quat": (None, [P, U32, FP]),
+        "seevr_scene_set_body_vel": (None, [P, U32, FP, FP]),
+        "seevr_scene_set_geom_friction": (None, [P, U32, F]),
+        "seevr_scene_gen_pile": (None, [P, U64, U32, U32, U32]),
+        "seevr_scene_gen_large": (None, [P, U64, U32, U32]),
+        "seevr_scene_gen_batch": (None, [P, U32, U32, U32, U32, U64]),
+        "seevr_scene_gen_rollout": (None, [P, U32, U32, U32, U64]),
+        "seevr_scene_gen_towers": (None, [P, U64, U32, U32, F]),
+        "seevr_scene_array": (P, [P, I]),
+        "seevr_scene_count": (U64, [P, I]),
+        "seevr_scene_save": (I, [P, C.c_char_p]),
+        "seevr_scene_load": (P, [C.c_char_p]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def check(status: int) -> None:
+    if status != OK:
+        msg = lib.seevr_last_error().decode(errors="replace")
+        raise SeevrError(status, msg or lib.seevr_status_string(status).decode())
+
+
+def default_params() -> Params:
+    p = Params()
+    lib.seevr_params_default(C.byref(p))
+    return p
+
+
+def fptr(values, n: int):
+    """ctypes float[n] from a sequence."""
+    arr = (C.c_float * n)(*[float(v) for v in values])
+    return arr

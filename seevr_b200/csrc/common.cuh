@@ -1,0 +1,118 @@
+// common.cuh — kernel-side view of the bound buffers, library scratch, and
+// the launchers each translation unit exports to the step driver.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "vmath.cuh"
+
+namespace seevr {
+
+// Device status word bits (seevr_physics_read_flags).
+enum : uint32_t {
+    kFlagPairOverflow = 1u << 0,
+    kFlagContactOverflow = 1u << 1,
+    kFlagTimeout = 1u << 2,
+    kFlagSolverGlobal = 1u << 3,
+};
+
+// Bounded spin for decoupled look-back: after this many polls a wait gives
+// up, raises kFlagTimeout and proceeds, so no kernel can hang.
+constexpr uint32_t kSpinLimit = 1u << 22;
+
+constexpr uint32_t kNone = 0xFFFFFFFFu;
+
+// The caller's buffers (physics.comp:16-57) plus derived read-only arrays.
+struct World {
+    float* pos;
+    float* quat;
+    float* vel;
+    float* omega;
+    const float* inv_mass;
+    const float* inv_inertia;
+    const uint32_t* vert_start;
+    const uint32_t* vert_count;
+    const uint32_t* geom_body;
+    const float* friction;
+    const float* restitution;
+    const float* hull;
+    float* verts;
+    const float* orig;
+    float* c_pos;
+    float* c_normal;
+    float* c_pen;
+    uint32_t* c_a;
+    uint32_t* c_b;
+    float* lambda;
+    uint32_t* counters;
+    float* aabb_min;
+    float* aabb_max;
+    uint32_t* pairs;
+    const uint32_t* sup_off;
+    const uint32_t* sup_lut;
+    const uint32_t* hull_range;  // (start,count) per geom: binding 30 or derived
+    const uint32_t* body_scene;  // body -> scene
+    const uint32_t* scene_off;   // scene -> first body, [num_scenes+1]
+    uint32_t nb, nv, nhv, ns;
+    uint32_t max_pairs, max_contacts;
+};
+
+// Solver / collision constants (seevr_params), as kernels see them.
+struct Consts {
+    float baumgarte, slop, lin_damp, ang_damp, eps, tol;
+    uint32_t pgs_iterations, mpr_iterations, discover_trials;
+};
+
+// Library-owned scratch (device).
+struct Scratch {
+    uint32_t* status;       // [4]: flags, scratch counters
+    uint32_t* row_count;    // [max_bodies]   broadphase pairs per row
+    uint32_t* row_off;      // [max_bodies]   exclusive scan of row_count
+    unsigned long long* scan_tiles;  // look-back tile status (+1 tile ticket)
+    uint32_t scan_tiles_cap;
+    float4* pair_res0;      // [max_pairs] contact point xyz, depth
+    float4* pair_res1;      // [max_pairs] normal xyz, found flag
+    uint32_t* pair_flag;    // [max_pairs] 1 if the pair makes a contact
+    uint32_t* pair_coff;    // [max_pairs] exclusive scan of pair_flag
+    // solver, per contact
+    float* s_ra;            // [max_contacts*3]
+    float* s_rb;            // [max_contacts*3]
+    float* s_bias;          // [max_contacts]
+    float* s_kn;            // [max_contacts]
+    float* s_mu;            // [max_contacts]
+    uint32_t* s_ab;         // [max_contacts*2] scene-local body indices, kNone = skip
+    uint32_t* s_level;      // [max_contacts]
+    uint32_t* s_order;      // [max_contacts]
+    uint32_t* s_lvl_start;  // [max_contacts + max_scenes + 1]
+    // solver, per body (global-memory path for scenes too large for smem)
+    float* s_R;             // [max_bodies*9]
+    uint32_t* s_last;       // [max_bodies]
+    uint32_t* derived_hull_range;  // [max_bodies*2]
+};
+
+// ---- launchers (one translation unit each) ------------------------------
+enum BodyStageFlags : uint32_t {
+    kIntegrate = 1u << 0,
+    kGravity = 1u << 1,
+    kAabb = 1u << 2,
+    kRenderVerts = 1u << 3,
+};
+// Every launcher returns the number of kernels it launched.
+int launch_hull_range_from_geom_data(const float* geom_data, uint32_t* out, uint32_t nb,
+                                     cudaStream_t st);
+int launch_body_stage(const World& w, const Consts& k, uint32_t flags, float dt, float gx,
+                      float gy, float gz, cudaStream_t st);
+// Exclusive scan of n_in[0..n) where n = min(*n_dev, n_cap) if n_dev else
+// n_cap.  Writes the grand total (unclamped input count semantics: the sum)
+// to *total_out when non-NULL, and sets `overflow_bit` in status[0] when the
+// total exceeds `total_cap`.
+int launch_exclusive_scan(const uint32_t* in, uint32_t* out, const uint32_t* n_dev,
+                          uint32_t n_cap, uint32_t* total_out, uint32_t total_cap,
+                          uint32_t overflow_bit, const Scratch& s, cudaStream_t st);
+int launch_broadphase_n2(const World& w, const Scratch& s, cudaStream_t st);
+int launch_narrowphase(const World& w, const Consts& k, const Scratch& s, cudaStream_t st);
+int launch_solver(const World& w, const Consts& k, const Scratch& s, uint32_t mode,
+                  float dt, uint32_t max_scene_bodies, cudaStream_t st);
+
+}  // namespace seevr

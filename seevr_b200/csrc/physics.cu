@@ -1,0 +1,579 @@
+// physics.cu — libseevr_cuda C ABI: handle, scratch, and the step driver
+// that replaces Physics.init/step/readCounters/deinit (src/physics.zig).
+//
+// One substep issues, in the reference's order (physics.zig:130-158):
+//   body stage  = integrate(prev substep) + gravity + AABB   (steps 6, 0, 9-11)
+//   broadphase  = count, scan, write                         (steps 8, 2)
+//   narrowphase = MPR, scan, scatter                         (step 3)
+//   impulse clear (memset)                                   (step 4)
+//   PGS solver                                               (step 5)
+// and the frame ends with integrate + render-vertex update (steps 6, 7).
+// Every kernel sizes its grid from capacities and reads live counts from
+// device memory, so a frame needs no host round trip and can be captured
+// into a CUDA graph.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/seevr.h"
+#include "common.cuh"
+
+using namespace seevr;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+seevr_status fail(seevr_status s, const std::string& msg) {
+    g_last_error = msg;
+    return s;
+}
+
+#define SEEVR_CUDA(call)                                                              \
+    do {                                                                              \
+        cudaError_t e_ = (call);                                                      \
+        if (e_ != cudaSuccess)                                                        \
+            return fail(SEEVR_ERR_CUDA, std::string(#call ": ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+enum Stage {
+    kStGravity = 0,
+    kStAabb = 1,
+    kStBroad = 2,
+    kStNarrow = 3,
+    kStClear = 4,
+    kStSolve = 5,
+    kStIntegrate = 6,
+    kStRender = 7,
+    kStClearCounters = 8
+};
+
+struct GraphKey {
+    uint32_t nb, nv, nhv, substeps;
+    float dt, g[3];
+    cudaStream_t stream;
+    bool operator==(const GraphKey& o) const {
+        return nb == o.nb && nv == o.nv && nhv == o.nhv && substeps == o.substeps && dt == o.dt &&
+               g[0] == o.g[0] && g[1] == o.g[1] && g[2] == o.g[2] && stream == o.stream;
+    }
+};
+
+}  // namespace
+
+struct seevr_physics {
+    int device = 0;
+    seevr_bindings b{};
+    seevr_caps caps{};
+    seevr_params params{};
+    cudaStream_t stream = nullptr;
+    World w{};
+    Consts k{};
+    Scratch s{};
+    uint32_t* body_scene = nullptr;
+    uint32_t* scene_off = nullptr;
+    uint32_t num_scenes = 1;
+    bool scenes_set = false;
+    uint32_t single_scene_nb = 0xFFFFFFFFu;
+    uint32_t max_scene_bodies = 0;
+    std::vector<void*> allocations;
+    uint64_t launches = 0;
+    uint32_t host_flags = 0;
+    // CUDA graph of one frame
+    cudaGraphExec_t graph_exec = nullptr;
+    GraphKey graph_key{};
+    uint64_t graph_kernels = 0;
+    // profiling events
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+};
+
+namespace {
+
+template <class T>
+seevr_status dev_alloc(seevr_physics* h, T** p, size_t count) {
+    void* q = nullptr;
+    const size_t bytes = count ? count * sizeof(T) : 16;
+    if (cudaMalloc(&q, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(SEEVR_ERR_OUT_OF_MEMORY, "cudaMalloc of " + std::to_string(bytes) + " bytes failed");
+    }
+    h->allocations.push_back(q);
+    *p = static_cast<T*>(q);
+    return SEEVR_OK;
+}
+
+void free_all(seevr_physics* h) {
+    if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+    for (void* p : h->allocations) cudaFree(p);
+    h->allocations.clear();
+    for (auto& e : h->ev)
+        if (e) cudaEventDestroy(e);
+    if (h->stream) cudaStreamDestroy(h->stream);
+}
+
+// Required byte size of each binding for the given capacities (0 = optional).
+uint64_t required_bytes(int i, const seevr_caps& c) {
+    const uint64_t N = c.max_bodies, HV = c.max_hull_verts, P = c.max_pairs, C = c.max_contacts;
+    switch (i) {
+        case SEEVR_B_BODY_POS: case SEEVR_B_BODY_VEL: case SEEVR_B_BODY_OMEGA:
+        case SEEVR_B_BODY_INV_INERTIA: case SEEVR_B_BODY_AABB_MIN: case SEEVR_B_BODY_AABB_MAX:
+            return N * 12;
+        case SEEVR_B_BODY_QUAT: return N * 16;
+        case SEEVR_B_BODY_INV_MASS: case SEEVR_B_BODY_VERT_START: case SEEVR_B_BODY_VERT_COUNT:
+        case SEEVR_B_GEOM_BODY_IDX: case SEEVR_B_GEOM_FRICTION: case SEEVR_B_GEOM_RESTITUTION:
+        case SEEVR_B_SUPPORT_OFFSET:
+            return N * 4;
+        case SEEVR_B_GEOM_DATA: return N * 32;
+        case SEEVR_B_HULL_VERTS: return HV * 12;
+        case SEEVR_B_CONTACT_POS: case SEEVR_B_CONTACT_NORMAL: return C * 12;
+        case SEEVR_B_CONTACT_PEN: case SEEVR_B_CONTACT_GEOM_A: case SEEVR_B_CONTACT_GEOM_B:
+        case SEEVR_B_LAMBDA_N:
+            return C * 4;
+        case SEEVR_B_COUNTERS: return 8;
+        case SEEVR_B_COLLISION_PAIRS: return P * 8;
+        case SEEVR_B_SUPPORT_LOOKUP: return 4;
+        default: return 0;  // 13, 14 checked at step time; 25-27 unused; 30 optional
+    }
+}
+
+void setup_world(seevr_physics* h) {
+    World& w = h->w;
+    auto P = [&](int i) { return h->b.ptr[i]; };
+    w.pos = static_cast<float*>(P(SEEVR_B_BODY_POS));
+    w.quat = static_cast<float*>(P(SEEVR_B_BODY_QUAT));
+    w.vel = static_cast<float*>(P(SEEVR_B_BODY_VEL));
+    w.omega = static_cast<float*>(P(SEEVR_B_BODY_OMEGA));
+    w.inv_mass = static_cast<const float*>(P(SEEVR_B_BODY_INV_MASS));
+    w.inv_inertia = static_cast<const float*>(P(SEEVR_B_BODY_INV_INERTIA));
+    w.vert_start = static_cast<const uint32_t*>(P(SEEVR_B_BODY_VERT_START));
+    w.vert_count = static_cast<const uint32_t*>(P(SEEVR_B_BODY_VERT_COUNT));
+    w.geom_body = static_cast<const uint32_t*>(P(SEEVR_B_GEOM_BODY_IDX));
+    w.friction = static_cast<const float*>(P(SEEVR_B_GEOM_FRICTION));
+    w.restitution = static_cast<const float*>(P(SEEVR_B_GEOM_RESTITUTION));
+    w.hull = static_cast<const float*>(P(SEEVR_B_HULL_VERTS));
+    w.verts = static_cast<float*>(P(SEEVR_B_VERTICES));
+    w.orig = static_cast<const float*>(P(SEEVR_B_ORIG_VERTICES));
+    w.c_pos = static_cast<float*>(P(SEEVR_B_CONTACT_POS));
+    w.c_normal = static_cast<float*>(P(SEEVR_B_CONTACT_NORMAL));
+    w.c_pen = static_cast<float*>(P(SEEVR_B_CONTACT_PEN));
+    w.c_a = static_cast<uint32_t*>(P(SEEVR_B_CONTACT_GEOM_A));
+    w.c_b = static_cast<uint32_t*>(P(SEEVR_B_CONTACT_GEOM_B));
+    w.lambda = static_cast<float*>(P(SEEVR_B_LAMBDA_N));
+    w.counters = static_cast<uint32_t*>(P(SEEVR_B_COUNTERS));
+    w.aabb_min = static_cast<float*>(P(SEEVR_B_BODY_AABB_MIN));
+    w.aabb_max = static_cast<float*>(P(SEEVR_B_BODY_AABB_MAX));
+    w.pairs = static_cast<uint32_t*>(P(SEEVR_B_COLLISION_PAIRS));
+    w.sup_off = static_cast<const uint32_t*>(P(SEEVR_B_SUPPORT_OFFSET));
+    w.sup_lut = static_cast<const uint32_t*>(P(SEEVR_B_SUPPORT_LOOKUP));
+    w.hull_range = P(SEEVR_B_HULL_RANGE) ? static_cast<const uint32_t*>(P(SEEVR_B_HULL_RANGE))
+                                         : h->s.derived_hull_range;
+    w.body_scene = h->body_scene;
+    w.scene_off = h->scene_off;
+    w.max_pairs = h->caps.max_pairs;
+    w.max_contacts = h->caps.max_contacts;
+    const seevr_params& p = h->params;
+    h->k.baumgarte = p.baumgarte;
+    h->k.slop = p.slop;
+    h->k.lin_damp = p.linear_damping;
+    h->k.ang_damp = p.angular_damping;
+    h->k.eps = p.mpr_eps;
+    h->k.tol = p.mpr_tolerance;
+    h->k.pgs_iterations = p.pgs_iterations;
+    h->k.mpr_iterations = p.mpr_iterations;
+    h->k.discover_trials = p.mpr_discover_trials;
+}
+
+__global__ void k_single_scene(uint32_t* body_scene, uint32_t* scene_off, uint32_t nb) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nb) body_scene[i] = 0;
+    if (i == 0) {
+        scene_off[0] = 0;
+        scene_off[1] = nb;
+    }
+}
+
+// Timed region helper: in profiling mode, brackets the launches of one
+// stage with events on the handle's stream and accumulates milliseconds.
+struct StageTimer {
+    seevr_physics* h;
+    seevr_profile* prof;
+    cudaStream_t st;
+    void begin() {
+        if (prof) cudaEventRecord(h->ev[0], st);
+    }
+    void end(int stage) {
+        if (!prof) return;
+        cudaEventRecord(h->ev[1], st);
+        cudaEventSynchronize(h->ev[1]);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, h->ev[0], h->ev[1]);
+        prof->ms[stage] += ms;
+    }
+};
+
+// Issue one frame (Physics.step body) on stream st; returns kernels launched.
+uint64_t issue_frame(seevr_physics* h, uint32_t nb, uint32_t nv, uint32_t nhv, uint32_t substeps,
+                     float dt, const float g[3], cudaStream_t st, seevr_profile* prof) {
+    World& w = h->w;
+    w.nb = nb;
+    w.nv = nv;
+    w.nhv = nhv;
+    w.ns = h->num_scenes;
+    uint64_t n = 0;
+    StageTimer T{h, prof, st};
+    const float sub_dt = dt / float(substeps);  // physics.zig:90
+    if (!h->b.ptr[SEEVR_B_HULL_RANGE])
+        n += launch_hull_range_from_geom_data(static_cast<const float*>(h->b.ptr[SEEVR_B_GEOM_DATA]),
+                                              h->s.derived_hull_range, nb, st);
+    for (uint32_t s = 0; s < substeps; ++s) {
+        T.begin();
+        n += launch_body_stage(w, h->k, (s > 0 ? kIntegrate : 0u) | kGravity | kAabb, sub_dt, g[0],
+                               g[1], g[2], st);
+        T.end(kStAabb);
+        T.begin();
+        n += launch_broadphase_n2(w, h->s, st);
+        T.end(kStBroad);
+        T.begin();
+        n += launch_narrowphase(w, h->k, h->s, st);
+        T.end(kStNarrow);
+        T.begin();
+        cudaMemsetAsync(w.lambda, 0, sizeof(float) * w.max_contacts, st);  // step 4
+        T.end(kStClear);
+        T.begin();
+        n += launch_solver(w, h->k, h->s, h->params.solver == SEEVR_SOLVER_SEQUENTIAL ? 0u : 1u,
+                           sub_dt, h->max_scene_bodies, st);
+        T.end(kStSolve);
+    }
+    const bool render = nv > 0 && !(h->params.flags & SEEVR_FLAG_SKIP_RENDER_VERTS);
+    T.begin();
+    n += launch_body_stage(w, h->k, kIntegrate | (render ? kRenderVerts : 0u), sub_dt, g[0], g[1],
+                           g[2], st);
+    T.end(render ? kStRender : kStIntegrate);
+    return n;
+}
+
+seevr_status check_step_args(seevr_physics* h, uint32_t nb, uint32_t nv, uint32_t nhv) {
+    if (nb > h->caps.max_bodies)
+        return fail(SEEVR_ERR_INVALID_ARGUMENT, "num_bodies exceeds caps.max_bodies");
+    if (nhv > h->caps.max_hull_verts)
+        return fail(SEEVR_ERR_INVALID_ARGUMENT, "num_hull_verts exceeds caps.max_hull_verts");
+    if (nv > h->caps.max_vertices)
+        return fail(SEEVR_ERR_INVALID_ARGUMENT, "num_vertices exceeds caps.max_vertices");
+    if (nv > 0 && !(h->params.flags & SEEVR_FLAG_SKIP_RENDER_VERTS) &&
+        (!h->b.ptr[SEEVR_B_VERTICES] || !h->b.ptr[SEEVR_B_ORIG_VERTICES]))
+        return fail(SEEVR_ERR_INVALID_ARGUMENT, "render vertices requested but bindings 13/14 are NULL");
+    if (h->scenes_set) {
+        // scene offsets were validated against max_bodies at set time; the
+        // last offset must equal num_bodies
+        if (nb != h->single_scene_nb)
+            return fail(SEEVR_ERR_INVALID_ARGUMENT, "num_bodies differs from the declared scenes' total");
+    }
+    return SEEVR_OK;
+}
+
+seevr_status ensure_single_scene(seevr_physics* h, uint32_t nb, cudaStream_t st) {
+    if (h->scenes_set || h->single_scene_nb == nb) return SEEVR_OK;
+    const uint32_t n = nb > 0 ? nb : 1;
+    k_single_scene<<<(n + 255) / 256, 256, 0, st>>>(h->body_scene, h->scene_off, nb);
+    SEEVR_CUDA(cudaGetLastError());
+    h->launches += 1;
+    h->single_scene_nb = nb;
+    h->max_scene_bodies = nb;
+    h->num_scenes = 1;
+    return SEEVR_OK;
+}
+
+seevr_status collect_flags(seevr_physics* h, cudaStream_t st, bool* overflow) {
+    uint32_t f = 0;
+    SEEVR_CUDA(cudaMemcpyAsync(&f, h->s.status, sizeof f, cudaMemcpyDeviceToHost, st));
+    SEEVR_CUDA(cudaMemsetAsync(h->s.status, 0, sizeof(uint32_t), st));
+    SEEVR_CUDA(cudaStreamSynchronize(st));
+    h->host_flags |= f;
+    *overflow = (f & (kFlagPairOverflow | kFlagContactOverflow)) != 0;
+    if (f & kFlagTimeout) return fail(SEEVR_ERR_TIMEOUT, "a device-side wait exceeded its limit");
+    return SEEVR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void seevr_params_default(seevr_params* p) {
+    if (!p) return;
+    p->pgs_iterations = 4;
+    p->baumgarte = 0.2f;
+    p->slop = 0.005f;
+    p->linear_damping = 0.999f;
+    p->angular_damping = 0.998f;
+    p->mpr_eps = 1e-6f;
+    p->mpr_tolerance = 1e-6f;
+    p->mpr_iterations = 50;
+    p->mpr_discover_trials = 15;
+    p->broadphase = SEEVR_BROADPHASE_N2;
+    p->solver = SEEVR_SOLVER_WAVEFRONT;
+    p->flags = 0;
+}
+
+seevr_status seevr_physics_create(const seevr_bindings* b, const seevr_caps* caps,
+                                  const seevr_params* params, seevr_physics** out) {
+    if (!out) return fail(SEEVR_ERR_INVALID_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    if (!b || !caps) return fail(SEEVR_ERR_INVALID_ARGUMENT, "bindings or caps is NULL");
+    if (caps->max_bodies == 0) return fail(SEEVR_ERR_INVALID_ARGUMENT, "caps.max_bodies is 0");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(SEEVR_ERR_NO_DEVICE, "no CUDA device");
+    }
+    for (int i = 0; i < SEEVR_NUM_BINDINGS; ++i) {
+        const uint64_t need = required_bytes(i, *caps);
+        if (need == 0) continue;
+        if (!b->ptr[i])
+            return fail(SEEVR_ERR_INVALID_ARGUMENT, "binding " + std::to_string(i) + " is NULL");
+        if (b->bytes[i] < need)
+            return fail(SEEVR_ERR_INVALID_ARGUMENT, "binding " + std::to_string(i) + " holds " +
+                                                        std::to_string(b->bytes[i]) + " bytes, needs " +
+                                                        std::to_string(need));
+    }
+    if (b->ptr[SEEVR_B_HULL_RANGE] && b->bytes[SEEVR_B_HULL_RANGE] < uint64_t(caps->max_bodies) * 8)
+        return fail(SEEVR_ERR_INVALID_ARGUMENT, "binding 30 (hull range) is undersized");
+    seevr_params p;
+    seevr_params_default(&p);
+    if (params) p = *params;
+    if (p.broadphase > SEEVR_BROADPHASE_LBVH || p.solver > SEEVR_SOLVER_COLORED)
+        return fail(SEEVR_ERR_INVALID_ARGUMENT, "unknown broadphase or solver");
+    if (p.broadphase != SEEVR_BROADPHASE_N2)
+        return fail(SEEVR_ERR_NOT_SUPPORTED, "LBVH broadphase is not available in this build");
+    if (p.solver == SEEVR_SOLVER_COLORED)
+        return fail(SEEVR_ERR_NOT_SUPPORTED, "coloured solver is not available in this build");
+
+    auto* h = new seevr_physics();
+    cudaGetDevice(&h->device);
+    h->b = *b;
+    h->caps = *caps;
+    if (h->caps.max_scenes == 0) h->caps.max_scenes = 1;
+    h->params = p;
+    seevr_status st = SEEVR_OK;
+    const seevr_caps& c = h->caps;
+    const uint32_t scan_n = std::max(std::max(c.max_bodies, c.max_pairs), 1u);
+    h->s.scan_tiles_cap = (scan_n + 2047) / 2048 + 2;
+#define ALLOC(ptr, n)                                   \
+    if (st == SEEVR_OK) st = dev_alloc(h, &(ptr), (n));
+    ALLOC(h->s.status, 4);
+    ALLOC(h->s.row_count, c.max_bodies);
+    ALLOC(h->s.row_off, c.max_bodies);
+    ALLOC(h->s.scan_tiles, h->s.scan_tiles_cap);
+    ALLOC(h->s.pair_res0, c.max_pairs);
+    ALLOC(h->s.pair_res1, c.max_pairs);
+    ALLOC(h->s.pair_flag, c.max_pairs);
+    ALLOC(h->s.pair_coff, c.max_pairs);
+    ALLOC(h->s.s_ra, size_t(c.max_contacts) * 3);
+    ALLOC(h->s.s_rb, size_t(c.max_contacts) * 3);
+    ALLOC(h->s.s_bias, c.max_contacts);
+    ALLOC(h->s.s_kn, c.max_contacts);
+    ALLOC(h->s.s_mu, c.max_contacts);
+    ALLOC(h->s.s_ab, size_t(c.max_contacts) * 2);
+    ALLOC(h->s.s_level, c.max_contacts);
+    ALLOC(h->s.s_order, c.max_contacts);
+    ALLOC(h->s.s_lvl_start, size_t(c.max_contacts) + c.max_scenes + 1);
+    ALLOC(h->s.s_R, size_t(c.max_bodies) * 9);
+    ALLOC(h->s.s_last, c.max_bodies);
+    ALLOC(h->s.derived_hull_range, size_t(c.max_bodies) * 2);
+    ALLOC(h->body_scene, c.max_bodies);
+    ALLOC(h->scene_off, size_t(c.max_scenes) + 1);
+#undef ALLOC
+    if (st == SEEVR_OK && cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
+        st = fail(SEEVR_ERR_CUDA, "cudaStreamCreate failed");
+    if (st == SEEVR_OK && (cudaEventCreate(&h->ev[0]) != cudaSuccess ||
+                           cudaEventCreate(&h->ev[1]) != cudaSuccess))
+        st = fail(SEEVR_ERR_CUDA, "cudaEventCreate failed");
+    if (st == SEEVR_OK && cudaMemset(h->s.status, 0, 16) != cudaSuccess)
+        st = fail(SEEVR_ERR_CUDA, "cudaMemset failed");
+    if (st != SEEVR_OK) {
+        cudaGetLastError();
+        free_all(h);
+        delete h;
+        return st;
+    }
+    setup_world(h);
+    *out = h;
+    return SEEVR_OK;
+}
+
+seevr_status seevr_physics_set_scenes(seevr_physics* h, const uint32_t* body_offset,
+                                      uint32_t num_scenes) {
+    if (!h || !body_offset || num_scenes == 0)
+        return fail(SEEVR_ERR_INVALID_ARGUMENT, "bad scene arguments");
+    if (num_scenes > h->caps.max_scenes)
+        return fail(SEEVR_ERR_INVALID_ARGUMENT, "num_scenes exceeds caps.max_scenes");
+    if (body_offset[0] != 0) return fail(SEEVR_ERR_INVALID_ARGUMENT, "body_offset[0] must be 0");
+    uint32_t maxs = 0;
+    for (uint32_t s = 0; s < num_scenes; ++s) {
+        if (body_offset[s + 1] < body_offset[s])
+            return fail(SEEVR_ERR_INVALID_ARGUMENT, "body_offset must be non-decreasing");
+        maxs = std::max(maxs, body_offset[s + 1] - body_offset[s]);
+    }
+    const uint32_t nb = body_offset[num_scenes];
+    if (nb > h->caps.max_bodies)
+        return fail(SEEVR_ERR_INVALID_ARGUMENT, "scenes hold more bodies than caps.max_bodies");
+    std::vector<uint32_t> bs(nb ? nb : 1, 0);
+    for (uint32_t s = 0; s < num_scenes; ++s)
+        for (uint32_t i = body_offset[s]; i < body_offset[s + 1]; ++i) bs[i] = s;
+    SEEVR_CUDA(cudaSetDevice(h->device));
+    SEEVR_CUDA(cudaMemcpy(h->body_scene, bs.data(), sizeof(uint32_t) * nb, cudaMemcpyHostToDevice));
+    SEEVR_CUDA(cudaMemcpy(h->scene_off, body_offset, sizeof(uint32_t) * (num_scenes + 1),
+                          cudaMemcpyHostToDevice));
+    h->num_scenes = num_scenes;
+    h->scenes_set = true;
+    h->single_scene_nb = nb;
+    h->max_scene_bodies = maxs;
+    if (h->graph_exec) {
+        cudaGraphExecDestroy(h->graph_exec);
+        h->graph_exec = nullptr;
+    }
+    return SEEVR_OK;
+}
+
+seevr_status seevr_physics_step(seevr_physics* h, uint32_t num_bodies, uint32_t num_vertices,
+                                uint32_t num_hull_verts, uint32_t substeps, float dt,
+                                const float gravity[3], seevr_profile* prof) {
+    if (!h || !gravity) return fail(SEEVR_ERR_INVALID_ARGUMENT, "handle or gravity is NULL");
+    if (num_bodies == 0 || substeps == 0) return SEEVR_OK;  // physics.zig:81
+    seevr_status st = check_step_args(h, num_bodies, num_vertices, num_hull_verts);
+    if (st != SEEVR_OK) return st;
+    SEEVR_CUDA(cudaSetDevice(h->device));
+    st = ensure_single_scene(h, num_bodies, h->stream);
+    if (st != SEEVR_OK) return st;
+    if (prof) {
+        prof->calls += 1;
+    }
+    h->launches += issue_frame(h, num_bodies, num_vertices, num_hull_verts, substeps, dt, gravity,
+                               h->stream, prof);
+    SEEVR_CUDA(cudaGetLastError());
+    if (h->params.flags & SEEVR_FLAG_NO_SYNC) return SEEVR_OK;
+    bool overflow = false;
+    st = collect_flags(h, h->stream, &overflow);
+    if (st != SEEVR_OK) return st;
+    if (overflow) return fail(SEEVR_ERR_CAPACITY, "pairs or contacts exceeded the caps");
+    return SEEVR_OK;
+}
+
+seevr_status seevr_physics_step_async(seevr_physics* h, uint32_t num_bodies, uint32_t num_vertices,
+                                      uint32_t num_hull_verts, uint32_t substeps, float dt,
+                                      const float gravity[3], uint32_t frames, void* stream) {
+    if (!h || !gravity) return fail(SEEVR_ERR_INVALID_ARGUMENT, "handle or gravity is NULL");
+    if (num_bodies == 0 || substeps == 0 || frames == 0) return SEEVR_OK;
+    seevr_status st = check_step_args(h, num_bodies, num_vertices, num_hull_verts);
+    if (st != SEEVR_OK) return st;
+    SEEVR_CUDA(cudaSetDevice(h->device));
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
+    st = ensure_single_scene(h, num_bodies, s);
+    if (st != SEEVR_OK) return st;
+    if (!(h->params.flags & SEEVR_FLAG_CUDA_GRAPH)) {
+        for (uint32_t f = 0; f < frames; ++f)
+            h->launches += issue_frame(h, num_bodies, num_vertices, num_hull_verts, substeps, dt,
+                                       gravity, s, nullptr);
+        SEEVR_CUDA(cudaGetLastError());
+        return SEEVR_OK;
+    }
+    const GraphKey key{num_bodies, num_vertices, num_hull_verts, substeps, dt,
+                       {gravity[0], gravity[1], gravity[2]}, s};
+    if (!h->graph_exec || !(h->graph_key == key)) {
+        if (h->graph_exec) {
+            cudaGraphExecDestroy(h->graph_exec);
+            h->graph_exec = nullptr;
+        }
+        cudaGraph_t g = nullptr;
+        SEEVR_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        const uint64_t n = issue_frame(h, num_bodies, num_vertices, num_hull_verts, substeps, dt,
+                                       gravity, s, nullptr);
+        cudaError_t e = cudaStreamEndCapture(s, &g);
+        if (e != cudaSuccess) return fail(SEEVR_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&h->graph_exec, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return fail(SEEVR_ERR_CUDA, std::string("instantiate: ") + cudaGetErrorString(e));
+        h->graph_key = key;
+        h->graph_kernels = n;
+    }
+    for (uint32_t f = 0; f < frames; ++f) SEEVR_CUDA(cudaGraphLaunch(h->graph_exec, s));
+    h->launches += h->graph_kernels * frames;
+    return SEEVR_OK;
+}
+
+seevr_status seevr_physics_read_counters(seevr_physics* h, uint32_t out[2]) {
+    if (!h || !out) return fail(SEEVR_ERR_INVALID_ARGUMENT, "handle or out is NULL");
+    SEEVR_CUDA(cudaSetDevice(h->device));
+    SEEVR_CUDA(cudaMemcpyAsync(out, h->w.counters, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+    SEEVR_CUDA(cudaStreamSynchronize(h->stream));
+    return SEEVR_OK;
+}
+
+seevr_status seevr_physics_read_flags(seevr_physics* h, uint32_t* flags) {
+    if (!h || !flags) return fail(SEEVR_ERR_INVALID_ARGUMENT, "handle or flags is NULL");
+    SEEVR_CUDA(cudaSetDevice(h->device));
+    bool overflow = false;
+    seevr_status st = collect_flags(h, h->stream, &overflow);
+    *flags = h->host_flags;
+    h->host_flags = 0;
+    return st;
+}
+
+seevr_status seevr_physics_upload_state(seevr_physics* h, uint32_t nb, const float* pos,
+                                        const float* quat, const float* vel, const float* omega) {
+    if (!h) return fail(SEEVR_ERR_INVALID_ARGUMENT, "handle is NULL");
+    if (nb > h->caps.max_bodies) return fail(SEEVR_ERR_INVALID_ARGUMENT, "num_bodies exceeds caps");
+    SEEVR_CUDA(cudaSetDevice(h->device));
+    const cudaStream_t s = h->stream;
+    if (pos) SEEVR_CUDA(cudaMemcpyAsync(h->w.pos, pos, size_t(nb) * 12, cudaMemcpyHostToDevice, s));
+    if (quat) SEEVR_CUDA(cudaMemcpyAsync(h->w.quat, quat, size_t(nb) * 16, cudaMemcpyHostToDevice, s));
+    if (vel) SEEVR_CUDA(cudaMemcpyAsync(h->w.vel, vel, size_t(nb) * 12, cudaMemcpyHostToDevice, s));
+    if (omega) SEEVR_CUDA(cudaMemcpyAsync(h->w.omega, omega, size_t(nb) * 12, cudaMemcpyHostToDevice, s));
+    SEEVR_CUDA(cudaStreamSynchronize(s));
+    return SEEVR_OK;
+}
+
+seevr_status seevr_physics_download_state(seevr_physics* h, uint32_t nb, float* pos, float* quat,
+                                          float* vel, float* omega) {
+    if (!h) return fail(SEEVR_ERR_INVALID_ARGUMENT, "handle is NULL");
+    if (nb > h->caps.max_bodies) return fail(SEEVR_ERR_INVALID_ARGUMENT, "num_bodies exceeds caps");
+    SEEVR_CUDA(cudaSetDevice(h->device));
+    const cudaStream_t s = h->stream;
+    if (pos) SEEVR_CUDA(cudaMemcpyAsync(pos, h->w.pos, size_t(nb) * 12, cudaMemcpyDeviceToHost, s));
+    if (quat) SEEVR_CUDA(cudaMemcpyAsync(quat, h->w.quat, size_t(nb) * 16, cudaMemcpyDeviceToHost, s));
+    if (vel) SEEVR_CUDA(cudaMemcpyAsync(vel, h->w.vel, size_t(nb) * 12, cudaMemcpyDeviceToHost, s));
+    if (omega) SEEVR_CUDA(cudaMemcpyAsync(omega, h->w.omega, size_t(nb) * 12, cudaMemcpyDeviceToHost, s));
+    SEEVR_CUDA(cudaStreamSynchronize(s));
+    return SEEVR_OK;
+}
+
+void seevr_physics_destroy(seevr_physics* h) {
+    if (!h) return;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    free_all(h);
+    delete h;
+}
+
+uint64_t seevr_physics_kernel_launches(const seevr_physics* h) { return h ? h->launches : 0; }
+
+const char* seevr_status_string(seevr_status s) {
+    switch (s) {
+        case SEEVR_OK: return "ok";
+        case SEEVR_ERR_INVALID_ARGUMENT: return "invalid argument";
+        case SEEVR_ERR_CAPACITY: return "capacity exceeded";
+        case SEEVR_ERR_CUDA: return "CUDA error";
+        case SEEVR_ERR_TIMEOUT: return "device wait timed out";
+        case SEEVR_ERR_NO_DEVICE: return "no CUDA device";
+        case SEEVR_ERR_OUT_OF_MEMORY: return "out of device memory";
+        case SEEVR_ERR_NOT_SUPPORTED: return "not supported";
+    }
+    return "unknown status";
+}
+
+const char* seevr_last_error(void) { return g_last_error.c_str(); }
+int seevr_abi_version(void) { return SEEVR_ABI_VERSION; }
+
+}  // extern "C"

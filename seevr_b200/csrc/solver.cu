@@ -1,0 +1,270 @@
+// solver.cu — PGS contact solver (step 5, physics.comp:500-583) and the
+// impulse clear (step 4, physics.comp:494-497).
+//
+// One CTA per scene.  Phase 1 stages the scene's bodies (velocity, angular
+// velocity, rotation matrix, inverse inertia, inverse mass) in shared memory
+// (global scratch when the scene is too large).  Phase 2 computes, for every
+// contact in parallel, the values the reference recomputes on every
+// iteration but which cannot change during the solve: the lever arms
+// ra, rb (positions and contact points are constant), the normal effective
+// mass k, the friction coefficient and the restitution/Baumgarte bias
+// (taken from the pre-solve velocities, as physics.comp:504-521 does).
+// Phase 3 runs the Gauss-Seidel sweeps:
+//  - SEQUENTIAL: one thread, contacts in index order (physics.comp:523-582);
+//  - WAVEFRONT: contacts are assigned levels so that a contact comes after
+//    every earlier contact sharing a dynamic body with it; contacts of one
+//    level touch disjoint dynamic bodies and run in parallel.  Each contact
+//    then sees exactly the body state it sees in the sequential sweep, so the
+//    result is bit-identical to SEQUENTIAL.
+// A body is "fixed" when inv_mass == 0 and inv_inertia == 0: its velocities
+// cannot change (the reference writes v - 0*impulse, the same value), so
+// fixed bodies create no ordering constraint and are never written.
+#include "common.cuh"
+
+namespace seevr {
+
+struct BodyView {
+    float* v;           // [n*3]
+    float* w;           // [n*3]
+    const float* R;     // [n*9]
+    const float* invI;  // [n*3]
+    const float* invm;  // [n]
+};
+
+__device__ __forceinline__ bool is_fixed(const BodyView& B, uint32_t i) {
+    return B.invm[i] == 0.0f && B.invI[i * 3] == 0.0f && B.invI[i * 3 + 1] == 0.0f &&
+           B.invI[i * 3 + 2] == 0.0f;
+}
+
+// One normal + friction update of contact c (physics.comp:525-580).
+__device__ __forceinline__ void solve_one(const BodyView& B, uint32_t la, uint32_t lb, f3 n, f3 ra,
+                                          f3 rb, float bias, float kn, float mu, float* lam) {
+    const float ima = B.invm[la], imb = B.invm[lb];
+    const m3 Ra = ld_m3(B.R, la), Rb = ld_m3(B.R, lb);
+    const f3 Ia = ld3(B.invI, la), Ib = ld3(B.invI, lb);
+    f3 va = ld3(B.v, la), wa = ld3(B.w, la), vb = ld3(B.v, lb), wb = ld3(B.w, lb);
+    f3 ua = add(va, cross(wa, ra)), ub = add(vb, cross(wb, rb));
+    const float vn = dot(sub(ub, ua), n);
+    float d_ln = (-vn + bias) / kn;
+    const float old_ln = *lam;
+    const float new_ln = gmax(old_ln + d_ln, 0.0f);
+    d_ln = new_ln - old_ln;
+    *lam = new_ln;
+    const f3 imp = scale(d_ln, n);
+    va = sub(va, scale(ima, imp));
+    vb = add(vb, scale(imb, imp));
+    wa = sub(wa, apply_inv_I(Ra, Ia, cross(ra, imp)));
+    wb = add(wb, apply_inv_I(Rb, Ib, cross(rb, imp)));
+    // Coulomb friction along the current slip direction
+    ua = add(va, cross(wa, ra));
+    ub = add(vb, cross(wb, rb));
+    const f3 dv = sub(ub, ua);
+    const f3 vt = sub(dv, scale(dot(dv, n), n));
+    const float vt_len = length(vt);
+    if (vt_len > 1e-6f) {
+        const f3 td = divs(vt, vt_len);
+        const f3 rat = cross(ra, td), rbt = cross(rb, td);
+        const float kt = ima + imb + dot(rat, apply_inv_I(Ra, Ia, rat)) + dot(rbt, apply_inv_I(Rb, Ib, rbt));
+        const float d_lt = gmin(vt_len / kt, mu * new_ln);
+        const f3 it = scale(d_lt, td);
+        va = add(va, scale(ima, it));
+        vb = sub(vb, scale(imb, it));
+        wa = add(wa, apply_inv_I(Ra, Ia, cross(ra, it)));
+        wb = sub(wb, apply_inv_I(Rb, Ib, cross(rb, it)));
+    }
+    if (!is_fixed(B, la)) {
+        st3(B.v, la, va);
+        st3(B.w, la, wa);
+    }
+    if (!is_fixed(B, lb)) {
+        st3(B.v, lb, vb);
+        st3(B.w, lb, wb);
+    }
+}
+
+__device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t* a, uint32_t n, uint32_t key) {
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (a[mid] < key) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+constexpr uint32_t kSolverThreads = 128;
+constexpr uint32_t kBodySmemWords = 20;  // v3 w3 R9 invI3 invm1 last1
+
+__global__ void __launch_bounds__(kSolverThreads)
+    k_solver(World w, Consts k, Scratch s, uint32_t mode, float dt, uint32_t smem_bodies) {
+    extern __shared__ float sm[];
+    __shared__ uint32_t sh_c0, sh_c1, sh_levels;
+    const uint32_t scene = blockIdx.x;
+    const uint32_t b0 = w.scene_off[scene], b1 = w.scene_off[scene + 1];
+    const uint32_t nbs = b1 - b0;
+    const uint32_t nc = min(w.counters[1], w.max_contacts);
+    if (threadIdx.x == 0) {
+        // contacts are in (a, b) lexicographic order, scenes own contiguous
+        // body ranges: the scene's contacts are a contiguous range
+        sh_c0 = lower_bound_u32(w.c_a, nc, b0);
+        sh_c1 = lower_bound_u32(w.c_a, nc, b1);
+    }
+    __syncthreads();
+    const uint32_t c0 = sh_c0, c1 = sh_c1;
+    if (c0 >= c1) return;
+    const uint32_t tid = threadIdx.x;
+
+    // ---- phase 1: bodies ----
+    const bool in_smem = nbs <= smem_bodies;
+    BodyView B;
+    uint32_t* last;
+    if (in_smem) {
+        float* p = sm;
+        B.v = p; p += nbs * 3;
+        B.w = p; p += nbs * 3;
+        float* R = p; p += nbs * 9;
+        float* invI = p; p += nbs * 3;
+        float* invm = p; p += nbs;
+        last = reinterpret_cast<uint32_t*>(p);
+        for (uint32_t i = tid; i < nbs; i += blockDim.x) {
+            const uint32_t g = b0 + i;
+            st3(B.v, i, ld3(w.vel, g));
+            st3(B.w, i, ld3(w.omega, g));
+            st_m3(R, i, quat_to_mat(w.quat, g));
+            st3(invI, i, ld3(w.inv_inertia, g));
+            invm[i] = w.inv_mass[g];
+            last[i] = 0;
+        }
+        B.R = R;
+        B.invI = invI;
+        B.invm = invm;
+    } else {
+        B.v = w.vel + size_t(b0) * 3;
+        B.w = w.omega + size_t(b0) * 3;
+        float* R = s.s_R + size_t(b0) * 9;
+        for (uint32_t i = tid; i < nbs; i += blockDim.x) {
+            st_m3(R, i, quat_to_mat(w.quat, b0 + i));
+            s.s_last[b0 + i] = 0;
+        }
+        B.R = R;
+        B.invI = w.inv_inertia + size_t(b0) * 3;
+        B.invm = w.inv_mass + b0;
+        last = s.s_last + b0;
+        if (tid == 0) atomicOr(&s.status[0], kFlagSolverGlobal);
+    }
+    __syncthreads();
+
+    // ---- phase 2: per-contact constants (physics.comp:504-521, 533-546) ----
+    for (uint32_t c = c0 + tid; c < c1; c += blockDim.x) {
+        const uint32_t ga = w.c_a[c], gb = w.c_b[c];
+        const uint32_t a = w.geom_body[ga], b = w.geom_body[gb];
+        const uint32_t la = a - b0, lb = b - b0;
+        const f3 n = ld3(w.c_normal, c), cp = ld3(w.c_pos, c);
+        const f3 ra = sub(cp, ld3(w.pos, a)), rb = sub(cp, ld3(w.pos, b));
+        const f3 va = add(ld3(B.v, la), cross(ld3(B.w, la), ra));
+        const f3 vb = add(ld3(B.v, lb), cross(ld3(B.w, lb), rb));
+        const float vn = dot(sub(vb, va), n);
+        const float e = gmax(w.restitution[ga], w.restitution[gb]);
+        const float bias = k.baumgarte * gmax(w.c_pen[c] - k.slop, 0.0f) / dt + e * gmax(-vn, 0.0f);
+        const float ima = B.invm[la], imb = B.invm[lb];
+        const m3 Ra = ld_m3(B.R, la), Rb = ld_m3(B.R, lb);
+        const f3 ran = cross(ra, n), rbn = cross(rb, n);
+        const float kn = ima + imb + dot(ran, apply_inv_I(Ra, ld3(B.invI, la), ran)) +
+                         dot(rbn, apply_inv_I(Rb, ld3(B.invI, lb), rbn));
+        st3(s.s_ra, c, ra);
+        st3(s.s_rb, c, rb);
+        s.s_bias[c] = bias;
+        s.s_kn[c] = kn;
+        s.s_mu[c] = sqrtf(w.friction[ga] * w.friction[gb]);
+        const bool skip = (ima == 0.0f && imb == 0.0f);  // physics.comp:531
+        s.s_ab[size_t(c) * 2] = skip ? kNone : la;
+        s.s_ab[size_t(c) * 2 + 1] = lb;
+        w.lambda[c] = 0.0f;
+    }
+    __syncthreads();
+
+    if (mode == 0) {
+        // ---- SEQUENTIAL: the reference order on one thread ----
+        if (tid == 0) {
+            for (uint32_t it = 0; it < k.pgs_iterations; ++it)
+                for (uint32_t c = c0; c < c1; ++c) {
+                    const uint32_t la = s.s_ab[size_t(c) * 2];
+                    if (la == kNone) continue;
+                    solve_one(B, la, s.s_ab[size_t(c) * 2 + 1], ld3(w.c_normal, c), ld3(s.s_ra, c),
+                              ld3(s.s_rb, c), s.s_bias[c], s.s_kn[c], s.s_mu[c], &w.lambda[c]);
+                }
+        }
+    } else {
+        // ---- WAVEFRONT: levels, counting sort by level, parallel sweeps ----
+        uint32_t* lvl = s.s_lvl_start + c0 + scene;  // [levels+1], fits in [c0+scene, c1+scene]
+        if (tid == 0) {
+            uint32_t maxl = 0;
+            for (uint32_t c = c0; c < c1; ++c) {
+                const uint32_t la = s.s_ab[size_t(c) * 2];
+                if (la == kNone) {
+                    s.s_level[c] = kNone;
+                    continue;
+                }
+                const uint32_t lb = s.s_ab[size_t(c) * 2 + 1];
+                const bool fa = is_fixed(B, la), fb = is_fixed(B, lb);
+                const uint32_t l = max(fa ? 0u : last[la], fb ? 0u : last[lb]) + 1u;
+                if (!fa) last[la] = l;
+                if (!fb) last[lb] = l;
+                s.s_level[c] = l - 1u;
+                maxl = max(maxl, l);
+            }
+            for (uint32_t l = 0; l <= maxl; ++l) lvl[l] = 0;
+            for (uint32_t c = c0; c < c1; ++c)
+                if (s.s_level[c] != kNone) lvl[s.s_level[c] + 1]++;
+            for (uint32_t l = 1; l <= maxl; ++l) lvl[l] += lvl[l - 1];
+            // stable fill: order[c0 + slot]; lvl[l] is used as a cursor and
+            // restored afterwards
+            for (uint32_t c = c0; c < c1; ++c) {
+                const uint32_t l = s.s_level[c];
+                if (l != kNone) s.s_order[c0 + lvl[l]++] = c;
+            }
+            for (uint32_t l = maxl; l > 0; --l) lvl[l] = lvl[l - 1];
+            lvl[0] = 0;
+            sh_levels = maxl;
+        }
+        __syncthreads();
+        const uint32_t levels = sh_levels;
+        for (uint32_t it = 0; it < k.pgs_iterations; ++it) {
+            for (uint32_t l = 0; l < levels; ++l) {
+                const uint32_t beg = lvl[l], end = lvl[l + 1];
+                for (uint32_t i = beg + tid; i < end; i += blockDim.x) {
+                    const uint32_t c = s.s_order[c0 + i];
+                    solve_one(B, s.s_ab[size_t(c) * 2], s.s_ab[size_t(c) * 2 + 1],
+                              ld3(w.c_normal, c), ld3(s.s_ra, c), ld3(s.s_rb, c), s.s_bias[c],
+                              s.s_kn[c], s.s_mu[c], &w.lambda[c]);
+                }
+                __syncthreads();
+            }
+        }
+    }
+    __syncthreads();
+    if (in_smem) {
+        for (uint32_t i = tid; i < nbs; i += blockDim.x) {
+            st3(w.vel, b0 + i, ld3(B.v, i));
+            st3(w.omega, b0 + i, ld3(B.w, i));
+        }
+    }
+}
+
+int launch_solver(const World& w, const Consts& k, const Scratch& s, uint32_t mode, float dt,
+                  uint32_t max_scene_bodies, cudaStream_t st) {
+    if (w.ns == 0 || w.max_contacts == 0) return 0;
+    constexpr uint32_t kMaxSmem = 160 * 1024;
+    uint32_t smem_bodies = max_scene_bodies;
+    if (smem_bodies * kBodySmemWords * 4 > kMaxSmem) smem_bodies = kMaxSmem / (kBodySmemWords * 4);
+    const size_t smem = size_t(smem_bodies) * kBodySmemWords * 4;
+    static size_t configured = 0;
+    if (smem > 48 * 1024 && smem > configured) {
+        cudaFuncSetAttribute(k_solver, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kMaxSmem));
+        configured = kMaxSmem;
+    }
+    k_solver<<<w.ns, kSolverThreads, smem, st>>>(w, k, s, mode, dt, smem_bodies);
+    return 1;
+}
+
+}  // namespace seevr

@@ -1,0 +1,108 @@
+"""Physics: the host interface of seeVR's physics step (src/physics.zig) over
+libseevr_cuda.
+
+    buf = Data.pile(seed=0).upload("cuda:0")
+    ph = Physics(buf)                                    # Physics.init
+    ph.step(buf.num_bodies, buf.num_vertices, buf.num_hull_verts,
+            10, 1/60, (0, -9.81, 0))                     # Physics.step
+    pairs, contacts = ph.read_counters()                 # Physics.readCounters
+    ph.deinit()                                          # Physics.deinit
+
+Errors raise SeevrError (the C ABI's status and message).  A capacity
+overflow raises SeevrError with status ERR_CAPACITY after the step has run
+(the first max_pairs / max_contacts in canonical order were kept).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib as L
+from .data import DeviceBuffers
+
+
+def make_params(pgs_iterations: int = 4, solver: int = L.SOLVER_WAVEFRONT,
+                broadphase: int = L.BROADPHASE_N2, flags: int = 0, **kw) -> L.Params:
+    p = L.default_params()
+    p.pgs_iterations = pgs_iterations
+    p.solver = solver
+    p.broadphase = broadphase
+    p.flags = flags
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+class Physics:
+    """One libseevr_cuda handle bound to a DeviceBuffers (Physics.init)."""
+
+    def __init__(self, buffers: DeviceBuffers, params: L.Params | None = None,
+                 use_hull_range: bool = True, scenes: bool = True):
+        import torch
+
+        self.buffers = buffers
+        self.params = params or make_params()
+        self._bind = buffers.bindings(use_hull_range=use_hull_range)
+        self._caps = buffers.caps.to_c()
+        h = C.c_void_p()
+        with torch.cuda.device(buffers.device):
+            L.check(L.lib.seevr_physics_create(C.byref(self._bind), C.byref(self._caps),
+                                               C.byref(self.params), C.byref(h)))
+        self._h = h
+        if scenes and buffers.num_scenes > 1:
+            off = np.ascontiguousarray(buffers.scene_body_offset, dtype=np.uint32)
+            L.check(L.lib.seevr_physics_set_scenes(
+                self._h, off.ctypes.data_as(C.POINTER(C.c_uint32)), buffers.num_scenes))
+
+    def step(self, num_bodies: int, num_vertices: int, num_hull_verts: int, substeps: int,
+             dt: float, gravity=(0.0, -9.81, 0.0), prof: L.Profile | None = None) -> None:
+        """Physics.step (physics.zig:80): synchronous unless FLAG_NO_SYNC."""
+        L.check(L.lib.seevr_physics_step(self._h, num_bodies, num_vertices, num_hull_verts,
+                                         substeps, dt, L.fptr(gravity, 3),
+                                         C.byref(prof) if prof is not None else None))
+
+    def step_async(self, num_bodies: int, num_vertices: int, num_hull_verts: int, substeps: int,
+                   dt: float, gravity=(0.0, -9.81, 0.0), frames: int = 1, stream=None) -> None:
+        """`frames` steps ordered on `stream` (torch.cuda.Stream or raw handle)."""
+        s = getattr(stream, "cuda_stream", stream)
+        L.check(L.lib.seevr_physics_step_async(self._h, num_bodies, num_vertices, num_hull_verts,
+                                               substeps, dt, L.fptr(gravity, 3), frames,
+                                               C.c_void_p(s) if s else None))
+
+    def read_counters(self) -> tuple[int, int]:
+        """Physics.readCounters (physics.zig:213): (pairs, contacts) of the last substep."""
+        out = (C.c_uint32 * 2)()
+        L.check(L.lib.seevr_physics_read_counters(self._h, out))
+        return int(out[0]), int(out[1])
+
+    def read_flags(self) -> int:
+        f = C.c_uint32()
+        L.check(L.lib.seevr_physics_read_flags(self._h, C.byref(f)))
+        return int(f.value)
+
+    def upload_state(self, num_bodies: int, pos=None, quat=None, vel=None, omega=None) -> None:
+        ptr = lambda a: None if a is None else C.c_void_p(a.ctypes.data if isinstance(a, np.ndarray) else a.data_ptr())
+        L.check(L.lib.seevr_physics_upload_state(self._h, num_bodies, ptr(pos), ptr(quat),
+                                                 ptr(vel), ptr(omega)))
+
+    def download_state(self, num_bodies: int, pos=None, quat=None, vel=None, omega=None) -> None:
+        ptr = lambda a: None if a is None else C.c_void_p(a.ctypes.data if isinstance(a, np.ndarray) else a.data_ptr())
+        L.check(L.lib.seevr_physics_download_state(self._h, num_bodies, ptr(pos), ptr(quat),
+                                                   ptr(vel), ptr(omega)))
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(L.lib.seevr_physics_kernel_launches(self._h))
+
+    def deinit(self) -> None:
+        """Physics.deinit (physics.zig:219)."""
+        if getattr(self, "_h", None):
+            L.lib.seevr_physics_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.deinit()
+        except Exception:
+            pass

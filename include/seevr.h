@@ -235,6 +235,15 @@ void seevr_physics_destroy(seevr_physics* h);
 /* Number of kernels the library launched on this handle since creation. */
 uint64_t seevr_physics_kernel_launches(const seevr_physics* h);
 
+/* LBVH state of the last substep of a handle created with
+ * SEEVR_BROADPHASE_LBVH: sorted 30-bit Morton codes of the body centroids
+ * (AABB centres), the body index of each sorted slot, and the centroid
+ * bounds (min xyz, max xyz).  Synchronous.  Mirrors the bvh_morton /
+ * bvh_sort_indices / bvh_scene_bounds buffers of bvh.comp:14-18 for the
+ * body tree. */
+seevr_status seevr_physics_read_lbvh(seevr_physics* h, uint32_t n, uint32_t* morton_sorted,
+                                     uint32_t* order, float bounds[6]);
+
 const char* seevr_status_string(seevr_status s);
 const char* seevr_last_error(void);
 int seevr_abi_version(void);

@@ -108,6 +108,11 @@ void seevr_scene_set_geom_friction(seevr_scene* s, uint32_t geom, float mu);
  * distributions.  Each call appends one or more scenes. */
 void seevr_scene_gen_pile(seevr_scene* s, uint64_t seed, uint32_t n_boxes,
                           uint32_t n_spheres, uint32_t segments);
+/* Same distributions, spawned in the box [lo, hi] instead of
+ * x,z in [-5,5], y in [1,21]. */
+void seevr_scene_gen_pile_in(seevr_scene* s, uint64_t seed, uint32_t n_boxes,
+                             uint32_t n_spheres, uint32_t segments,
+                             const float lo[3], const float hi[3]);
 void seevr_scene_gen_large(seevr_scene* s, uint64_t seed, uint32_t n_bodies,
                            uint32_t segments);
 void seevr_scene_gen_batch(seevr_scene* s, uint32_t num_scenes,

@@ -1,6 +1,6 @@
 """ctypes binding of libseevr_cuda.so (include/seevr.h, include/seevr_scene.h).
 
-The library is built in-tree by ``python -m seevr_b200.build``.  There is no
+The library is built in-tree by ``python seevr_b200/build.py``.  There is no
 fallback: importing this module without the built library raises.
 """
 from __future__ import annotations
@@ -66,7 +66,7 @@ class SeevrError(RuntimeError):
 
 def _load():
     if not LIB_PATH.exists():
-        raise ImportError(f"{LIB_PATH} is not built; run `python -m seevr_b200.build`")
+        raise ImportError(f"{LIB_PATH} is not built; run `python seevr_b200/build.py`")
     lib = C.CDLL(str(LIB_PATH))
     P, U32, U64, F, I = C.c_void_p, C.c_uint32, C.c_uint64, C.c_float, C.c_int
     FP = C.POINTER(C.c_float)
@@ -84,6 +84,7 @@ def _load():
         "seevr_physics_download_state": (I, [P, U32, P, P, P, P]),
         "seevr_physics_destroy": (None, [P]),
         "seevr_physics_kernel_launches": (U64, [P]),
+        "seevr_physics_read_lbvh": (I, [P, U32, UP, UP, FP]),
         "seevr_status_string": (C.c_char_p, [I]),
         "seevr_last_error": (C.c_char_p, []),
         "seevr_abi_version": (I, []),
@@ -99,6 +100,7 @@ def _load():
         "seevr_scene_set_body_vel": (None, [P, U32, FP, FP]),
         "seevr_scene_set_geom_friction": (None, [P, U32, F]),
         "seevr_scene_gen_pile": (None, [P, U64, U32, U32, U32]),
+        "seevr_scene_gen_pile_in": (None, [P, U64, U32, U32, U32, FP, FP]),
         "seevr_scene_gen_large": (None, [P, U64, U32, U32]),
         "seevr_scene_gen_batch": (None, [P, U32, U32, U32, U32, U64]),
         "seevr_scene_gen_rollout": (None, [P, U32, U32, U32, U64]),

@@ -1,6 +1,6 @@
 """Build libseevr_cuda.so in-tree (sm_100a) and the test oracle.
 
-    python -m seevr_b200.build [--force]
+    python seevr_b200/build.py [--force] [--ptxas]
 
 CUDA sources are compiled with nvcc for sm_100a only, -fmad=false so that
 every float product and sum rounds on its own (the results match the FP32

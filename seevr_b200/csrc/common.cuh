@@ -112,6 +112,7 @@ int launch_exclusive_scan(const uint32_t* in, uint32_t* out, const uint32_t* n_d
                           uint32_t overflow_bit, const Scratch& s, cudaStream_t st);
 int launch_broadphase_n2(const World& w, const Scratch& s, cudaStream_t st);
 int launch_narrowphase(const World& w, const Consts& k, const Scratch& s, cudaStream_t st);
+cudaError_t init_solver();
 int launch_solver(const World& w, const Consts& k, const Scratch& s, uint32_t mode,
                   float dt, uint32_t max_scene_bodies, cudaStream_t st);
 

@@ -21,6 +21,7 @@
 
 #include "../../include/seevr.h"
 #include "common.cuh"
+#include "lbvh.cuh"
 
 using namespace seevr;
 
@@ -88,6 +89,8 @@ struct seevr_physics {
     uint64_t graph_kernels = 0;
     // profiling events
     cudaEvent_t ev[2] = {nullptr, nullptr};
+    // LBVH broadphase work arrays (broadphase == SEEVR_BROADPHASE_LBVH)
+    LbvhScratch lb{};
 };
 
 namespace {
@@ -234,7 +237,9 @@ uint64_t issue_frame(seevr_physics* h, uint32_t nb, uint32_t nv, uint32_t nhv, u
                                g[1], g[2], st);
         T.end(kStAabb);
         T.begin();
-        n += launch_broadphase_n2(w, h->s, st);
+        n += h->params.broadphase == SEEVR_BROADPHASE_LBVH
+                 ? launch_broadphase_lbvh(w, h->s, h->lb, st)
+                 : launch_broadphase_n2(w, h->s, st);
         T.end(kStBroad);
         T.begin();
         n += launch_narrowphase(w, h->k, h->s, st);
@@ -345,8 +350,6 @@ seevr_status seevr_physics_create(const seevr_bindings* b, const seevr_caps* cap
     if (params) p = *params;
     if (p.broadphase > SEEVR_BROADPHASE_LBVH || p.solver > SEEVR_SOLVER_COLORED)
         return fail(SEEVR_ERR_INVALID_ARGUMENT, "unknown broadphase or solver");
-    if (p.broadphase != SEEVR_BROADPHASE_N2)
-        return fail(SEEVR_ERR_NOT_SUPPORTED, "LBVH broadphase is not available in this build");
     if (p.solver == SEEVR_SOLVER_COLORED)
         return fail(SEEVR_ERR_NOT_SUPPORTED, "coloured solver is not available in this build");
 
@@ -384,6 +387,28 @@ seevr_status seevr_physics_create(const seevr_bindings* b, const seevr_caps* cap
     ALLOC(h->s.derived_hull_range, size_t(c.max_bodies) * 2);
     ALLOC(h->body_scene, c.max_bodies);
     ALLOC(h->scene_off, size_t(c.max_scenes) + 1);
+    if (p.broadphase == SEEVR_BROADPHASE_LBVH) {
+        LbvhScratch& lb = h->lb;
+        const size_t n = c.max_bodies;
+        lb.cap = c.max_bodies;
+        ALLOC(lb.centroid, n * 3);
+        ALLOC(lb.bounds_o, 6);
+        ALLOC(lb.bounds_f, 6);
+        ALLOC(lb.keys_a, n);
+        ALLOC(lb.vals_a, n);
+        ALLOC(lb.keys_b, n);
+        ALLOC(lb.vals_b, n);
+        ALLOC(lb.keys_sorted, n);
+        ALLOC(lb.vals_sorted, n);
+        ALLOC(lb.hist, 4 * 256);
+        ALLOC(lb.status, lbvh_status_words(c.max_bodies));
+        ALLOC(lb.left, 2 * n);
+        ALLOC(lb.right, 2 * n);
+        ALLOC(lb.parent, 2 * n);
+        ALLOC(lb.flags, n);
+        ALLOC(lb.node_min, 6 * n);
+        ALLOC(lb.node_max, 6 * n);
+    }
 #undef ALLOC
     if (st == SEEVR_OK && cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
         st = fail(SEEVR_ERR_CUDA, "cudaStreamCreate failed");
@@ -392,6 +417,8 @@ seevr_status seevr_physics_create(const seevr_bindings* b, const seevr_caps* cap
         st = fail(SEEVR_ERR_CUDA, "cudaEventCreate failed");
     if (st == SEEVR_OK && cudaMemset(h->s.status, 0, 16) != cudaSuccess)
         st = fail(SEEVR_ERR_CUDA, "cudaMemset failed");
+    if (st == SEEVR_OK && init_solver() != cudaSuccess)
+        st = fail(SEEVR_ERR_CUDA, "cudaFuncSetAttribute for the solver failed");
     if (st != SEEVR_OK) {
         cudaGetLastError();
         free_all(h);
@@ -426,6 +453,10 @@ seevr_status seevr_physics_set_scenes(seevr_physics* h, const uint32_t* body_off
     SEEVR_CUDA(cudaMemcpy(h->body_scene, bs.data(), sizeof(uint32_t) * nb, cudaMemcpyHostToDevice));
     SEEVR_CUDA(cudaMemcpy(h->scene_off, body_offset, sizeof(uint32_t) * (num_scenes + 1),
                           cudaMemcpyHostToDevice));
+    if (h->params.broadphase == SEEVR_BROADPHASE_LBVH && num_scenes > 1)
+        return fail(SEEVR_ERR_NOT_SUPPORTED,
+                    "the LBVH broadphase steps a single scene; use the all-pairs broadphase for "
+                    "batches");
     h->num_scenes = num_scenes;
     h->scenes_set = true;
     h->single_scene_nb = nb;
@@ -558,6 +589,23 @@ void seevr_physics_destroy(seevr_physics* h) {
 }
 
 uint64_t seevr_physics_kernel_launches(const seevr_physics* h) { return h ? h->launches : 0; }
+
+seevr_status seevr_physics_read_lbvh(seevr_physics* h, uint32_t n, uint32_t* morton_sorted,
+                                     uint32_t* order, float bounds[6]) {
+    if (!h) return fail(SEEVR_ERR_INVALID_ARGUMENT, "handle is NULL");
+    if (h->params.broadphase != SEEVR_BROADPHASE_LBVH)
+        return fail(SEEVR_ERR_NOT_SUPPORTED, "handle does not use the LBVH broadphase");
+    if (n > h->lb.cap) return fail(SEEVR_ERR_INVALID_ARGUMENT, "n exceeds the handle's bodies");
+    SEEVR_CUDA(cudaSetDevice(h->device));
+    const cudaStream_t s = h->stream;
+    if (morton_sorted)
+        SEEVR_CUDA(cudaMemcpyAsync(morton_sorted, h->lb.keys_sorted, size_t(n) * 4, cudaMemcpyDeviceToHost, s));
+    if (order)
+        SEEVR_CUDA(cudaMemcpyAsync(order, h->lb.vals_sorted, size_t(n) * 4, cudaMemcpyDeviceToHost, s));
+    if (bounds) SEEVR_CUDA(cudaMemcpyAsync(bounds, h->lb.bounds_f, 24, cudaMemcpyDeviceToHost, s));
+    SEEVR_CUDA(cudaStreamSynchronize(s));
+    return SEEVR_OK;
+}
 
 const char* seevr_status_string(seevr_status s) {
     switch (s) {

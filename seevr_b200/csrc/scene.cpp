@@ -567,13 +567,15 @@ struct Placer {
 // One pile scene: static ground box, then bodies alternating box/sphere.
 // Per body the stream draws: size, orientation, position(s), then the
 // optional velocities and friction.
+const double kPileLo[3] = {-5.0, 1.0, -5.0}, kPileHi[3] = {5.0, 21.0, 5.0};
+
 void gen_pile_scene(seevr_scene* s, SplitMix64& rng, uint32_t n_boxes, uint32_t n_spheres,
-                    uint32_t segments, const Mats& m, bool random_vel, bool random_mu) {
+                    uint32_t segments, const Mats& m, bool random_vel, bool random_mu,
+                    const double lo[3] = kPileLo, const double hi[3] = kPileHi) {
     s->begin();
     const float gc[3] = {0.f, -0.25f, 0.f}, gh[3] = {50.f, 0.25f, 50.f};
     s->add_box(gc, gh, kGrey, 0.5f, 0.2f, m.ground);
     Placer placer(2.5);
-    const double lo[3] = {-5.0, 1.0, -5.0}, hi[3] = {5.0, 21.0, 5.0};
     uint32_t nb = 0, ns = 0;
     while (nb < n_boxes || ns < n_spheres) {
         const bool box = (nb < n_boxes) && (ns >= n_spheres || nb <= ns);
@@ -652,6 +654,14 @@ void seevr_scene_gen_pile(seevr_scene* s, uint64_t seed, uint32_t n_boxes, uint3
     SplitMix64 rng(seed);
     const Mats m = default_materials(s);
     gen_pile_scene(s, rng, n_boxes, n_spheres, segments, m, false, false);
+}
+
+void seevr_scene_gen_pile_in(seevr_scene* s, uint64_t seed, uint32_t n_boxes, uint32_t n_spheres,
+                             uint32_t segments, const float lo[3], const float hi[3]) {
+    SplitMix64 rng(seed);
+    const Mats m = default_materials(s);
+    const double l[3] = {lo[0], lo[1], lo[2]}, h[3] = {hi[0], hi[1], hi[2]};
+    gen_pile_scene(s, rng, n_boxes, n_spheres, segments, m, false, false, l, h);
 }
 
 void seevr_scene_gen_large(seevr_scene* s, uint64_t seed, uint32_t n_bodies, uint32_t segments) {

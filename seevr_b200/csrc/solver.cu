@@ -251,18 +251,22 @@ __global__ void __launch_bounds__(kSolverThreads)
     }
 }
 
+constexpr uint32_t kSolverMaxSmem = 160 * 1024;
+
+cudaError_t init_solver() {
+    // opt in to more than 48 KB of dynamic shared memory; done at handle
+    // creation so that no attribute call happens during graph capture
+    return cudaFuncSetAttribute(k_solver, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                int(kSolverMaxSmem));
+}
+
 int launch_solver(const World& w, const Consts& k, const Scratch& s, uint32_t mode, float dt,
                   uint32_t max_scene_bodies, cudaStream_t st) {
     if (w.ns == 0 || w.max_contacts == 0) return 0;
-    constexpr uint32_t kMaxSmem = 160 * 1024;
     uint32_t smem_bodies = max_scene_bodies;
-    if (smem_bodies * kBodySmemWords * 4 > kMaxSmem) smem_bodies = kMaxSmem / (kBodySmemWords * 4);
+    if (smem_bodies * kBodySmemWords * 4 > kSolverMaxSmem)
+        smem_bodies = kSolverMaxSmem / (kBodySmemWords * 4);
     const size_t smem = size_t(smem_bodies) * kBodySmemWords * 4;
-    static size_t configured = 0;
-    if (smem > 48 * 1024 && smem > configured) {
-        cudaFuncSetAttribute(k_solver, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kMaxSmem));
-        configured = kMaxSmem;
-    }
     k_solver<<<w.ns, kSolverThreads, smem, st>>>(w, k, s, mode, dt, smem_bodies);
     return 1;
 }

@@ -110,9 +110,15 @@ class Data:
 
     # ---- seeded workloads ----
     @classmethod
-    def pile(cls, seed=0, n_boxes=256, n_spheres=256, segments=16) -> "Data":
+    def pile(cls, seed=0, n_boxes=256, n_spheres=256, segments=16, lo=None, hi=None) -> "Data":
+        """Ground box + bodies alternating box/sphere, spawned in x,z [-5,5],
+        y [1,21] (or the box [lo, hi]) without initial overlaps."""
         d = cls()
-        L.lib.seevr_scene_gen_pile(d._h, seed, n_boxes, n_spheres, segments)
+        if lo is None and hi is None:
+            L.lib.seevr_scene_gen_pile(d._h, seed, n_boxes, n_spheres, segments)
+        else:
+            L.lib.seevr_scene_gen_pile_in(d._h, seed, n_boxes, n_spheres, segments,
+                                          _f3(lo), _f3(hi))
         return d
 
     @classmethod

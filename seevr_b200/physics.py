@@ -91,6 +91,18 @@ class Physics:
         L.check(L.lib.seevr_physics_download_state(self._h, num_bodies, ptr(pos), ptr(quat),
                                                    ptr(vel), ptr(omega)))
 
+    def read_lbvh(self, n: int):
+        """Sorted Morton codes, body order and centroid bounds of the last
+        LBVH build (broadphase=BROADPHASE_LBVH handles)."""
+        codes = np.zeros(n, np.uint32)
+        order = np.zeros(n, np.uint32)
+        bounds = np.zeros(6, np.float32)
+        U = C.POINTER(C.c_uint32)
+        L.check(L.lib.seevr_physics_read_lbvh(self._h, n, codes.ctypes.data_as(U),
+                                              order.ctypes.data_as(U),
+                                              bounds.ctypes.data_as(C.POINTER(C.c_float))))
+        return codes, order, bounds
+
     @property
     def kernel_launches(self) -> int:
         return int(L.lib.seevr_physics_kernel_launches(self._h))

@@ -59,7 +59,8 @@ enum seevr_scene_count_id {
     SEEVR_C_SUPPORT_ENTRIES = 5,
     SEEVR_C_SCENES = 6,
     SEEVR_C_MATERIALS = 7,
-    SEEVR_C_DYNAMIC_BODIES = 8
+    SEEVR_C_DYNAMIC_BODIES = 8,
+    SEEVR_C_PLACEMENT_FAILURES = 9 /* generator draws left overlapping */
 };
 
 seevr_scene* seevr_scene_create(void);

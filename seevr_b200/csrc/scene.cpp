@@ -72,6 +72,7 @@ struct seevr_scene {
     std::vector<float> hull_verts;
     std::vector<uint32_t> support_offset, support_lookup;
     uint32_t num_support_entries = 0;
+    uint32_t placement_failures = 0;  // generator placements left overlapping
     // scenes
     std::vector<uint32_t> scene_starts{0};
     std::vector<uint32_t> scene_offsets_view;
@@ -387,6 +388,7 @@ struct seevr_scene {
         }
         for (uint32_t st : o.scene_starts)
             if (scene_starts.back() != st + bi) scene_starts.push_back(st + bi);
+        placement_failures += o.placement_failures;
     }
 
     uint32_t add_material(const float albedo[3], float roughness, float metallic,
@@ -467,7 +469,8 @@ struct Placer {
     double cell;
     std::vector<PlacedShape> shapes;
     std::unordered_map<int64_t, std::vector<uint32_t>> grid;
-    explicit Placer(double cell_size) : cell(cell_size) {}
+    uint32_t& failures;  // draws that ended overlapping (volume too dense)
+    Placer(double cell_size, uint32_t& fail_count) : cell(cell_size), failures(fail_count) {}
     static int64_t key(int64_t x, int64_t y, int64_t z) {
         return ((x & 0x1FFFFF) << 42) | ((y & 0x1FFFFF) << 21) | (z & 0x1FFFFF);
     }
@@ -552,11 +555,13 @@ struct Placer {
                                 {2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)}};
         for (int k = 0; k < 3; ++k)
             for (int j = 0; j < 3; ++j) s.ax[k][j] = R[j][k];
-        for (int attempt = 0; attempt < 256; ++attempt) {
+        bool placed = false;
+        for (int attempt = 0; attempt < 256 && !placed; ++attempt) {
             for (int k = 0; k < 3; ++k) c[k] = float(rng.uniform(lo[k], hi[k]));
             for (int k = 0; k < 3; ++k) s.c[k] = c[k];
-            if (free(s)) break;
+            placed = free(s);
         }
+        failures += placed ? 0u : 1u;
         shapes.push_back(s);
         grid[key(int64_t(std::floor(s.c[0] / cell)), int64_t(std::floor(s.c[1] / cell)),
                  int64_t(std::floor(s.c[2] / cell)))]
@@ -575,7 +580,7 @@ void gen_pile_scene(seevr_scene* s, SplitMix64& rng, uint32_t n_boxes, uint32_t 
     s->begin();
     const float gc[3] = {0.f, -0.25f, 0.f}, gh[3] = {50.f, 0.25f, 50.f};
     s->add_box(gc, gh, kGrey, 0.5f, 0.2f, m.ground);
-    Placer placer(2.5);
+    Placer placer(2.5, s->placement_failures);
     uint32_t nb = 0, ns = 0;
     while (nb < n_boxes || ns < n_spheres) {
         const bool box = (nb < n_boxes) && (ns >= n_spheres || nb <= ns);
@@ -671,7 +676,7 @@ void seevr_scene_gen_large(seevr_scene* s, uint64_t seed, uint32_t n_bodies, uin
     const float gc[3] = {0.f, -0.25f, 0.f}, gh[3] = {40.f, 0.25f, 40.f};
     s->add_box(gc, gh, kGrey, 0.5f, 0.2f, m.ground);
     std::vector<float> pts;
-    Placer placer(2.5);
+    Placer placer(2.5, s->placement_failures);
     const double lo[3] = {-32.0, 1.0, -32.0}, hi[3] = {32.0, 65.0, 32.0};
     for (uint32_t i = 0; i < n_bodies; ++i) {
         const double kind = rng.uniform();
@@ -808,6 +813,7 @@ uint64_t seevr_scene_count(const seevr_scene* s, int id) {
         case SEEVR_C_SCENES: return s->num_scenes();
         case SEEVR_C_MATERIALS: return s->mat_density.size();
         case SEEVR_C_DYNAMIC_BODIES: return s->num_dynamic();
+        case SEEVR_C_PLACEMENT_FAILURES: return s->placement_failures;
         default: return 0;
     }
 }

@@ -159,6 +159,7 @@ class Data:
     num_scenes = property(lambda self: self.count(6))
     num_materials = property(lambda self: self.count(7))
     num_dynamic = property(lambda self: self.count(8))
+    placement_failures = property(lambda self: self.count(9))
 
     def array(self, name: str) -> np.ndarray:
         """A copy of one staging array, shaped (count, components)."""

@@ -50,7 +50,8 @@ def test_lbvh_pairs_equal_all_pairs_large_scene(cuda):
 def test_lbvh_dense_pile_pairs(cuda):
     """A settled pile has many overlaps per body (rows longer than one
     32-entry write chunk are exercised by the ground body's row)."""
-    d = Data.pile(seed=9, n_boxes=200, n_spheres=200, lo=(-4, 0, -4), hi=(4, 6, 4))
+    d = Data.pile(seed=9, n_boxes=200, n_spheres=200, lo=(-6, 0, -6), hi=(6, 6, 6))
+    assert d.placement_failures == 0
     a, _ = run(d, cuda, BROADPHASE_N2, frames=40, substeps=10)
     b, _ = run(d, cuda, BROADPHASE_LBVH, frames=40, substeps=10)
     assert a["num_pairs"] > 300

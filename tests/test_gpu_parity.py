@@ -32,10 +32,12 @@ def test_small_pile_bit_exact(cuda, solver):
 
 
 def low_pile(seed, n):
-    """Bodies spawned just above the ground in a 4 m wide column: contacts
-    form within the first frames."""
-    return Data.pile(seed=seed, n_boxes=n // 2, n_spheres=n - n // 2, lo=(-2, 0, -2),
-                     hi=(2, 4, 2))
+    """Bodies spawned just above the ground in a 6 m wide column, about 2 m^3
+    per body: contacts form within the first frames."""
+    d = Data.pile(seed=seed, n_boxes=n // 2, n_spheres=n - n // 2, lo=(-3, 0, -3),
+                  hi=(3, max(3.0, n / 18.0), 3))
+    assert d.placement_failures == 0
+    return d
 
 
 def test_pile_with_contacts_bit_exact(cuda):

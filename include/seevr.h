@@ -232,6 +232,39 @@ seevr_status seevr_physics_download_state(seevr_physics* h, uint32_t num_bodies,
 /* Replaces Physics.deinit (physics.zig:219-221). */
 void seevr_physics_destroy(seevr_physics* h);
 
+/* No counterpart in the reference.  One physics step of a single scene that
+ * allocates no device memory, for callers that cannot call cudaMalloc: a
+ * renderer that owns and pre-sizes all device memory (as seeVR's Data.init
+ * does for the buffers it shares with Vulkan), a real-time loop that must
+ * not allocate after start-up, or code that enqueues the step while a stream
+ * is captured in global capture mode.  It runs the same kernels as
+ * seevr_physics_step (same results, bit for bit) on scratch held in one
+ * static device array of SEEVR_NOALLOC_SCRATCH_BYTES that every device which
+ * loads the library keeps until the process exits.
+ *  - Limits: num_bodies <= SEEVR_NOALLOC_MAX_BODIES, max_pairs <=
+ *    SEEVR_NOALLOC_MAX_PAIRS, max_contacts <= SEEVR_NOALLOC_MAX_CONTACTS
+ *    (the capacities of the caller's pair and contact buffers); larger
+ *    values return SEEVR_ERR_INVALID_ARGUMENT with a message.
+ *  - All-pairs broadphase, sequential or wavefront solver.
+ *  - Ordered on `stream` (a cudaStream_t, NULL = default stream) on the
+ *    current device; synchronous unless params->flags has NO_SYNC.
+ *  - The first call on a device looks up the scratch array's device address
+ *    (cudaGetSymbolAddress) and configures the solver kernel; make that
+ *    first call before any stream capture.
+ *  - Every call shares the one array: calls whose GPU work may overlap
+ *    (other streams or host threads on the same device) race and must be
+ *    serialised by the caller.  Each call clears what must start at zero. */
+#define SEEVR_NOALLOC_MAX_BODIES 4096u
+#define SEEVR_NOALLOC_MAX_PAIRS 32768u
+#define SEEVR_NOALLOC_MAX_CONTACTS 16384u
+#define SEEVR_NOALLOC_SCRATCH_BYTES 2475008u
+seevr_status seevr_physics_step_noalloc(const seevr_bindings* bindings,
+                                        const seevr_params* params,
+                                        uint32_t max_pairs, uint32_t max_contacts,
+                                        uint32_t num_bodies, uint32_t num_vertices,
+                                        uint32_t num_hull_verts, uint32_t substeps,
+                                        float dt, const float gravity[3], void* stream);
+
 /* Number of kernels the library launched on this handle since creation. */
 uint64_t seevr_physics_kernel_launches(const seevr_physics* h);
 

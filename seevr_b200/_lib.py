@@ -85,6 +85,8 @@ def _load():
         "seevr_physics_destroy": (None, [P]),
         "seevr_physics_kernel_launches": (U64, [P]),
         "seevr_physics_read_lbvh": (I, [P, U32, UP, UP, FP]),
+        "seevr_physics_step_noalloc": (I, [C.POINTER(Bindings), C.POINTER(Params), U32, U32,
+                                           U32, U32, U32, U32, F, FP, P]),
         "seevr_status_string": (C.c_char_p, [I]),
         "seevr_last_error": (C.c_char_p, []),
         "seevr_abi_version": (I, []),

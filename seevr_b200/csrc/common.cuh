@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <string>
 
 #include "vmath.cuh"
 
@@ -113,6 +114,9 @@ int launch_exclusive_scan(const uint32_t* in, uint32_t* out, const uint32_t* n_d
 int launch_broadphase_n2(const World& w, const Scratch& s, cudaStream_t st);
 int launch_narrowphase(const World& w, const Consts& k, const Scratch& s, cudaStream_t st);
 cudaError_t init_solver();
+// Set the calling thread's message returned by seevr_last_error().
+void set_last_error(const char* msg);
+inline void set_last_error(const std::string& msg) { set_last_error(msg.c_str()); }
 int launch_solver(const World& w, const Consts& k, const Scratch& s, uint32_t mode,
                   float dt, uint32_t max_scene_bodies, cudaStream_t st);
 

@@ -34,6 +34,12 @@ seevr_status fail(seevr_status s, const std::string& msg) {
     return s;
 }
 
+}  // namespace
+
+void seevr::set_last_error(const char* msg) { g_last_error = msg; }
+
+namespace {
+
 #define SEEVR_CUDA(call)                                                              \
     do {                                                                              \
         cudaError_t e_ = (call);                                                      \

@@ -2,12 +2,25 @@
 // support function (physics.comp:107-169) and Minkowski Portal Refinement
 // (physics.comp:171-399), plus deterministic contact compaction.
 //
-// One thread per candidate pair.  Each body's rotation matrix, position,
-// hull range and lookup offset are loaded once per pair and kept in
-// registers (the reference recomputes quat_to_mat in every support call;
-// the values are identical).  The contact found for pair p is staged at
-// slot p; a scan over the found flags then writes contacts in pair order,
-// where the reference appends with atomicAdd (physics.comp:404).
+// MPR's cost per pair varies by an order of magnitude (separated pairs stop
+// after one or two support calls; touching pairs refine and search the
+// penetration for tens).  With one pair per thread, a warp waits for its
+// slowest lane.  Here every lane runs MPR as a state machine whose steps
+// each make exactly one Minkowski support call:
+//   D1   first support along -v0           (physics.comp:254-271)
+//   D2   second support                     (272-287)
+//   DT   portal discovery trials            (289-319)
+//   R    portal refinement                  (323-343)
+//   P    penetration search                 (346-365)
+// and a lane whose pair finishes takes the next pair from a global counter
+// (warp-aggregated atomics), so all lanes stay busy until the pair list is
+// exhausted and converge on the support call, the expensive part of a step.
+// The arithmetic and the order of every test are those of the reference
+// loops, so each pair's result is the same bit for bit.
+//
+// The contact found for pair p is staged at slot p; a scan over the found
+// flags then writes contacts in pair order, where the reference appends with
+// atomicAdd (physics.comp:404).
 #include "common.cuh"
 
 namespace seevr {
@@ -29,7 +42,7 @@ __device__ __forceinline__ Shape load_shape(const World& w, uint32_t b) {
 }
 
 // support (physics.comp:107-162)
-__device__ f3 support(const World& w, const Shape& s, f3 d) {
+__device__ __forceinline__ f3 support(const World& w, const Shape& s, f3 d) {
     const f3 ld = mulT(s.R, d);
     float best = -1e10f;
     f3 bv = mk(0.f, 0.f, 0.f);
@@ -70,16 +83,11 @@ __device__ f3 support(const World& w, const Shape& s, f3 d) {
     return add(s.p, mul(s.R, bv));
 }
 
+// Minkowski support point and the supporting points on A and B
+// (mink_support_pts, physics.comp:165-169)
 struct Mink {
     f3 v, sa, sb;
 };
-__device__ __forceinline__ Mink mink(const World& w, const Shape& A, const Shape& B, f3 d) {
-    Mink m;
-    m.sa = support(w, A, d);
-    m.sb = support(w, B, neg(d));
-    m.v = sub(m.sa, m.sb);
-    return m;
-}
 
 __device__ __forceinline__ f3 portal_dir(f3 v1, f3 v2, f3 v3) {
     return normalize(cross(sub(v2, v1), sub(v3, v1)));
@@ -90,29 +98,25 @@ __device__ __forceinline__ bool reach_tol(const Consts& k, f3 v1, f3 v2, f3 v3, 
     return dot1 < k.tol + k.eps * gmax(1.0f, dot1);
 }
 
-// portal vertex i: Minkowski point v and the support points on A and B
-struct Portal {
-    Mink m[4];
-};
-
 // mpr_expand_portal (physics.comp:200-221)
-__device__ __forceinline__ void expand(Portal& P, const Mink& m4) {
-    const f3 v4v0 = cross(m4.v, P.m[0].v);
-    float d = dot(P.m[1].v, v4v0);
+__device__ __forceinline__ void expand(const f3& v0, Mink& m1, Mink& m2, Mink& m3, const Mink& m4) {
+    const f3 v4v0 = cross(m4.v, v0);
+    float d = dot(m1.v, v4v0);
     if (d > 0.0f) {
-        d = dot(P.m[2].v, v4v0);
-        if (d > 0.0f) P.m[1] = m4;
-        else P.m[3] = m4;
+        d = dot(m2.v, v4v0);
+        if (d > 0.0f) m1 = m4;
+        else m3 = m4;
     } else {
-        d = dot(P.m[3].v, v4v0);
-        if (d > 0.0f) P.m[2] = m4;
-        else P.m[1] = m4;
+        d = dot(m3.v, v4v0);
+        if (d > 0.0f) m2 = m4;
+        else m1 = m4;
     }
 }
 
-// mpr_find_pos (physics.comp:224-247)
-__device__ f3 find_pos(const Consts& k, const Portal& P) {
-    const f3 v0 = P.m[0].v, v1 = P.m[1].v, v2 = P.m[2].v, v3 = P.m[3].v;
+// mpr_find_pos (physics.comp:224-247); s0a, s0b are the body positions
+__device__ f3 find_pos(const Consts& k, f3 v0, f3 s0a, f3 s0b, const Mink& m1, const Mink& m2,
+                       const Mink& m3) {
+    const f3 v1 = m1.v, v2 = m2.v, v3 = m3.v;
     float b0 = dot(cross(v1, v2), v3);
     float b1 = -dot(cross(v0, v2), v3);
     float b2 = dot(cross(v0, v1), v3);
@@ -126,128 +130,200 @@ __device__ f3 find_pos(const Consts& k, const Portal& P) {
         b3 = dot(cross(v1, v2), dir);
         sum = b0 + b1 + b2 + b3;
     }
-    const f3 p1 = add(add(add(scale(b0, P.m[0].sa), scale(b1, P.m[1].sa)), scale(b2, P.m[2].sa)),
-                      scale(b3, P.m[3].sa));
-    const f3 p2 = add(add(add(scale(b0, P.m[0].sb), scale(b1, P.m[1].sb)), scale(b2, P.m[2].sb)),
-                      scale(b3, P.m[3].sb));
+    const f3 p1 = add(add(add(scale(b0, s0a), scale(b1, m1.sa)), scale(b2, m2.sa)), scale(b3, m3.sa));
+    const f3 p2 = add(add(add(scale(b0, s0b), scale(b1, m1.sb)), scale(b2, m2.sb)), scale(b3, m3.sb));
     return scale(0.5f / sum, add(p1, p2));
 }
 
-// mpr (physics.comp:368-399) with discover (250-320), refine (323-343) and
-// penetration (346-365).  Returns found; fills normal, depth, contact point.
-__device__ bool mpr(const World& w, const Consts& k, uint32_t a, uint32_t b, f3& normal,
-                    float& depth, f3& cp) {
-    const Shape A = load_shape(w, a), B = load_shape(w, b);
-    Portal P;
-    // ---- discover portal ----
-    P.m[0].sa = A.p;
-    P.m[0].sb = B.p;
-    P.m[0].v = sub(A.p, B.p);
-    if (fabsf(P.m[0].v.x) < k.eps && fabsf(P.m[0].v.y) < k.eps && fabsf(P.m[0].v.z) < k.eps)
-        P.m[0].v.x += 10.0f * k.eps;
-    f3 dir = normalize(neg(P.m[0].v));
-    P.m[1] = mink(w, A, B, dir);
-    float d = dot(P.m[1].v, dir);
-    if (d < k.eps) return false;
-    dir = cross(P.m[0].v, P.m[1].v);
-    if (dot(dir, dir) < k.eps) {
-        const f3 v1 = P.m[1].v;
-        if (fabsf(v1.x) < k.eps && fabsf(v1.y) < k.eps && fabsf(v1.z) < k.eps) {
-            normal = normalize(P.m[0].v);  // res == 1
-            depth = 0.0f;
-        } else {
-            depth = length(v1);  // res == 2
-            normal = normalize(v1);
-        }
-        cp = scale(0.5f, add(P.m[1].sa, P.m[1].sb));
-        return true;
+enum MprState : uint32_t { kD1 = 0, kD2 = 1, kDT = 2, kR = 3, kP = 4 };
+
+// Record pair p's outcome (physics.comp:486-489: a contact when found and
+// depth > 0).
+__device__ __forceinline__ void finish(float4* res0, float4* res1, uint32_t* flag, uint32_t p,
+                                       bool found, f3 cp, f3 n, float depth) {
+    const bool keep = found && depth > 0.0f;
+    flag[p] = keep ? 1u : 0u;
+    if (keep) {
+        res0[p] = make_float4(cp.x, cp.y, cp.z, depth);
+        res1[p] = make_float4(n.x, n.y, n.z, 0.0f);
     }
-    dir = normalize(dir);
-    P.m[2] = mink(w, A, B, dir);
-    d = dot(P.m[2].v, dir);
-    if (d < k.eps) return false;
-    f3 va = sub(P.m[1].v, P.m[0].v), vb = sub(P.m[2].v, P.m[0].v);
-    dir = normalize(cross(va, vb));
-    if (dot(dir, P.m[0].v) > 0.0f) {
-        const Mink t = P.m[1];
-        P.m[1] = P.m[2];
-        P.m[2] = t;
-        dir = neg(dir);
-    }
-    bool discovered = false;
-    for (uint32_t trials = 0; trials < k.discover_trials;) {
-        const Mink c = mink(w, A, B, dir);
-        d = dot(c.v, dir);
-        if (d < k.eps) return false;
-        va = cross(P.m[1].v, c.v);
-        d = dot(va, P.m[0].v);
-        if (d < -k.eps) {
-            P.m[2] = c;
-            va = sub(P.m[1].v, P.m[0].v);
-            vb = sub(P.m[2].v, P.m[0].v);
-            dir = normalize(cross(va, vb));
-            ++trials;
-            continue;
-        }
-        va = cross(c.v, P.m[2].v);
-        d = dot(va, P.m[0].v);
-        if (d < -k.eps) {
-            P.m[1] = c;
-            va = sub(P.m[1].v, P.m[0].v);
-            vb = sub(P.m[2].v, P.m[0].v);
-            dir = normalize(cross(va, vb));
-            ++trials;
-            continue;
-        }
-        P.m[3] = c;
-        discovered = true;
-        break;
-    }
-    if (!discovered) return false;
-    // ---- refine portal ----
-    bool inside = false;
-    for (uint32_t it = 0; it < k.mpr_iterations; ++it) {
-        const f3 pd = portal_dir(P.m[1].v, P.m[2].v, P.m[3].v);
-        if (dot(P.m[1].v, pd) > -k.eps) {
-            inside = true;
-            break;
-        }
-        const Mink m4 = mink(w, A, B, pd);
-        if (!(dot(m4.v, pd) > -k.eps) || reach_tol(k, P.m[1].v, P.m[2].v, P.m[3].v, m4.v, pd))
-            return false;
-        expand(P, m4);
-    }
-    // refine returning 1 (iterations exhausted) continues like 0
-    (void)inside;
-    // ---- find penetration ----
-    for (uint32_t it = 0; it < k.mpr_iterations; ++it) {
-        const f3 pd = portal_dir(P.m[1].v, P.m[2].v, P.m[3].v);
-        const Mink m4 = mink(w, A, B, pd);
-        if (reach_tol(k, P.m[1].v, P.m[2].v, P.m[3].v, m4.v, pd) || it >= k.mpr_iterations - 1) {
-            depth = dot(pd, P.m[1].v);
-            normal = pd;
-            cp = find_pos(k, P);
-            return true;
-        }
-        expand(P, m4);
-    }
-    return false;
 }
 
-__global__ void __launch_bounds__(128) k_narrow(World w, Consts k, float4* __restrict__ res0,
-                                                float4* __restrict__ res1,
-                                                uint32_t* __restrict__ flag) {
+constexpr uint32_t kNarrowThreads = 128;
+
+__global__ void __launch_bounds__(kNarrowThreads)
+    k_narrow(World w, Consts k, float4* __restrict__ res0, float4* __restrict__ res1,
+             uint32_t* __restrict__ flag, uint32_t* __restrict__ ticket) {
     const uint32_t np = min(w.counters[0], w.max_pairs);
-    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < np; p += gridDim.x * blockDim.x) {
-        const uint32_t a = w.pairs[size_t(p) * 2], b = w.pairs[size_t(p) * 2 + 1];
-        f3 n = mk(0, 0, 0), cp = mk(0, 0, 0);
-        float depth = 0.0f;
-        const bool found = mpr(w, k, a, b, n, depth, cp);
-        const bool keep = found && depth > 0.0f;
-        flag[p] = keep ? 1u : 0u;
-        if (keep) {
-            res0[p] = make_float4(cp.x, cp.y, cp.z, depth);
-            res1[p] = make_float4(n.x, n.y, n.z, 0.0f);
+    const uint32_t lane = threadIdx.x & 31u;
+    const unsigned full = 0xFFFFFFFFu;
+
+    bool active = false, drained = false;
+    uint32_t p = 0, state = kD1, iter = 0;
+    Shape A, B;
+    f3 v0 = mk(0, 0, 0), dir = mk(0, 0, 0);
+    Mink m1{}, m2{}, m3{};
+
+    while (true) {
+        // ---- refill idle lanes with the next pairs ----
+        if (!drained) {
+            const unsigned need = __ballot_sync(full, !active);
+            if (need) {
+                const uint32_t leader = __ffs(need) - 1;
+                uint32_t base = 0;
+                if (lane == leader) base = atomicAdd(ticket, uint32_t(__popc(need)));
+                base = __shfl_sync(full, base, leader);
+                if (base + __popc(need) >= np) drained = true;
+                if (!active) {
+                    const uint32_t q = base + __popc(need & ((1u << lane) - 1u));
+                    if (q < np) {
+                        p = q;
+                        const uint32_t a = w.pairs[size_t(p) * 2], b = w.pairs[size_t(p) * 2 + 1];
+                        A = load_shape(w, a);
+                        B = load_shape(w, b);
+                        v0 = sub(A.p, B.p);  // s0a - s0b (physics.comp:254-258)
+                        if (fabsf(v0.x) < k.eps && fabsf(v0.y) < k.eps && fabsf(v0.z) < k.eps)
+                            v0.x += 10.0f * k.eps;
+                        dir = normalize(neg(v0));
+                        state = kD1;
+                        iter = 0;
+                        active = true;
+                    }
+                }
+            }
+        }
+        if (__ballot_sync(full, active) == 0u) break;
+        if (!active) continue;
+
+        // ---- prelude: the direction of this step's support call ----
+        if (state == kR) {
+            dir = portal_dir(m1.v, m2.v, m3.v);
+            if (dot(m1.v, dir) > -k.eps) {  // origin inside: refine returns 0
+                state = kP;
+                iter = 0;
+                if (k.mpr_iterations == 0) {
+                    finish(res0, res1, flag, p, false, v0, v0, 0.0f);
+                    active = false;
+                    continue;
+                }
+            }
+        } else if (state == kP) {
+            dir = portal_dir(m1.v, m2.v, m3.v);
+        }
+
+        // ---- the one Minkowski support call of the step ----
+        Mink m;
+        m.sa = support(w, A, dir);
+        m.sb = support(w, B, neg(dir));
+        m.v = sub(m.sa, m.sb);
+
+        // ---- postlude ----
+        switch (state) {
+            case kD1: {
+                if (dot(m.v, dir) < k.eps) {
+                    finish(res0, res1, flag, p, false, v0, v0, 0.0f);
+                    active = false;
+                    break;
+                }
+                m1 = m;
+                const f3 c = cross(v0, m1.v);
+                if (dot(c, c) < k.eps) {
+                    const f3 v1 = m1.v;
+                    f3 n;
+                    float depth;
+                    if (fabsf(v1.x) < k.eps && fabsf(v1.y) < k.eps && fabsf(v1.z) < k.eps) {
+                        n = normalize(v0);  // touching: res == 1
+                        depth = 0.0f;
+                    } else {
+                        depth = length(v1);  // origin on segment v0-v1: res == 2
+                        n = normalize(v1);
+                    }
+                    finish(res0, res1, flag, p, true, scale(0.5f, add(m1.sa, m1.sb)), n, depth);
+                    active = false;
+                    break;
+                }
+                dir = normalize(c);
+                state = kD2;
+                break;
+            }
+            case kD2: {
+                if (dot(m.v, dir) < k.eps) {
+                    finish(res0, res1, flag, p, false, v0, v0, 0.0f);
+                    active = false;
+                    break;
+                }
+                m2 = m;
+                dir = normalize(cross(sub(m1.v, v0), sub(m2.v, v0)));
+                if (dot(dir, v0) > 0.0f) {
+                    const Mink t = m1;
+                    m1 = m2;
+                    m2 = t;
+                    dir = neg(dir);
+                }
+                iter = 0;  // discovery trials
+                state = kDT;
+                if (k.discover_trials == 0) {
+                    finish(res0, res1, flag, p, false, v0, v0, 0.0f);
+                    active = false;
+                }
+                break;
+            }
+            case kDT: {
+                if (dot(m.v, dir) < k.eps) {
+                    finish(res0, res1, flag, p, false, v0, v0, 0.0f);
+                    active = false;
+                    break;
+                }
+                bool retry = false;
+                if (dot(cross(m1.v, m.v), v0) < -k.eps) {
+                    m2 = m;
+                    retry = true;
+                } else if (dot(cross(m.v, m2.v), v0) < -k.eps) {
+                    m1 = m;
+                    retry = true;
+                }
+                if (retry) {
+                    dir = normalize(cross(sub(m1.v, v0), sub(m2.v, v0)));
+                    if (++iter >= k.discover_trials) {
+                        finish(res0, res1, flag, p, false, v0, v0, 0.0f);
+                        active = false;
+                    }
+                    break;
+                }
+                m3 = m;  // portal found: refine
+                iter = 0;
+                state = kR;
+                if (k.mpr_iterations == 0) {  // refine returns 1, penetration finds nothing
+                    finish(res0, res1, flag, p, false, v0, v0, 0.0f);
+                    active = false;
+                }
+                break;
+            }
+            case kR: {
+                if (!(dot(m.v, dir) > -k.eps) || reach_tol(k, m1.v, m2.v, m3.v, m.v, dir)) {
+                    finish(res0, res1, flag, p, false, v0, v0, 0.0f);
+                    active = false;
+                    break;
+                }
+                expand(v0, m1, m2, m3, m);
+                if (++iter >= k.mpr_iterations) {  // refine returns 1: go on to penetration
+                    iter = 0;
+                    state = kP;
+                }
+                break;
+            }
+            default: {  // kP
+                if (reach_tol(k, m1.v, m2.v, m3.v, m.v, dir) || iter >= k.mpr_iterations - 1) {
+                    const float depth = dot(dir, m1.v);
+                    finish(res0, res1, flag, p, true, find_pos(k, v0, A.p, B.p, m1, m2, m3), dir,
+                           depth);
+                    active = false;
+                    break;
+                }
+                expand(v0, m1, m2, m3, m);
+                ++iter;
+                break;
+            }
         }
     }
 }
@@ -279,8 +355,12 @@ static uint32_t grid_for(uint32_t cap, uint32_t threads, uint32_t max_blocks) {
 
 int launch_narrowphase(const World& w, const Consts& k, const Scratch& s, cudaStream_t st) {
     if (w.max_pairs == 0) return 0;
-    k_narrow<<<grid_for(w.max_pairs, 128, 148 * 32), 128, 0, st>>>(w, k, s.pair_res0,
-                                                                   s.pair_res1, s.pair_flag);
+    // persistent grid: a few resident blocks per SM; the pair ticket lives
+    // in status[1] and is cleared here
+    cudaMemsetAsync(&s.status[1], 0, sizeof(uint32_t), st);
+    const uint32_t blocks = grid_for(w.max_pairs, kNarrowThreads, 148 * 4);
+    k_narrow<<<blocks, kNarrowThreads, 0, st>>>(w, k, s.pair_res0, s.pair_res1, s.pair_flag,
+                                                &s.status[1]);
     launch_exclusive_scan(s.pair_flag, s.pair_coff, &w.counters[0], w.max_pairs,
                           &w.counters[1], w.max_contacts, kFlagContactOverflow, s, st);
     k_contact_scatter<<<grid_for(w.max_pairs, 256, 148 * 16), 256, 0, st>>>(

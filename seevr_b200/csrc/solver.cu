@@ -251,6 +251,148 @@ __global__ void __launch_bounds__(kSolverThreads)
     }
 }
 
+// ---- warp per scene -------------------------------------------------------
+// Scenes of up to kWarpMaxBodies bodies: one warp per scene, body state in
+// global memory (L1-resident), __syncwarp between levels.  Levels are
+// assigned 32 contacts at a time: each lane starts from the latest level of
+// its bodies in earlier chunks, then lanes are visited in order and every
+// later lane sharing a dynamic body with lane j moves past lane j's level.
+constexpr uint32_t kWarpMaxBodies = 1024;
+constexpr uint32_t kWarpsPerBlock = 4;
+
+__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+    k_solver_warp(World w, Consts k, Scratch s, uint32_t mode, float dt) {
+    __shared__ uint32_t sh_last[kWarpsPerBlock][kWarpMaxBodies];
+    const unsigned full = 0xFFFFFFFFu;
+    const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+    const uint32_t scene = blockIdx.x * kWarpsPerBlock + wid;
+    if (scene >= w.ns) return;
+    const uint32_t b0 = w.scene_off[scene], b1 = w.scene_off[scene + 1];
+    const uint32_t nbs = b1 - b0;
+    const uint32_t nc = min(w.counters[1], w.max_contacts);
+    uint32_t c0 = 0, c1 = 0;
+    if (lane == 0) {
+        c0 = lower_bound_u32(w.c_a, nc, b0);
+        c1 = lower_bound_u32(w.c_a, nc, b1);
+    }
+    c0 = __shfl_sync(full, c0, 0);
+    c1 = __shfl_sync(full, c1, 0);
+    if (c0 >= c1) return;
+
+    BodyView B;
+    B.v = w.vel + size_t(b0) * 3;
+    B.w = w.omega + size_t(b0) * 3;
+    float* R = s.s_R + size_t(b0) * 9;
+    B.R = R;
+    B.invI = w.inv_inertia + size_t(b0) * 3;
+    B.invm = w.inv_mass + b0;
+    uint32_t* last = sh_last[wid];
+    for (uint32_t i = lane; i < nbs; i += 32) {
+        st_m3(R, i, quat_to_mat(w.quat, b0 + i));
+        last[i] = 0;
+    }
+    __syncwarp();
+
+    // per-contact constants (physics.comp:504-521, 533-546)
+    for (uint32_t c = c0 + lane; c < c1; c += 32) {
+        const uint32_t ga = w.c_a[c], gb = w.c_b[c];
+        const uint32_t a = w.geom_body[ga], b = w.geom_body[gb];
+        const uint32_t la = a - b0, lb = b - b0;
+        const f3 n = ld3(w.c_normal, c), cp = ld3(w.c_pos, c);
+        const f3 ra = sub(cp, ld3(w.pos, a)), rb = sub(cp, ld3(w.pos, b));
+        const f3 va = add(ld3(B.v, la), cross(ld3(B.w, la), ra));
+        const f3 vb = add(ld3(B.v, lb), cross(ld3(B.w, lb), rb));
+        const float vn = dot(sub(vb, va), n);
+        const float e = gmax(w.restitution[ga], w.restitution[gb]);
+        const float bias = k.baumgarte * gmax(w.c_pen[c] - k.slop, 0.0f) / dt + e * gmax(-vn, 0.0f);
+        const float ima = B.invm[la], imb = B.invm[lb];
+        const m3 Ra = ld_m3(B.R, la), Rb = ld_m3(B.R, lb);
+        const f3 ran = cross(ra, n), rbn = cross(rb, n);
+        const float kn = ima + imb + dot(ran, apply_inv_I(Ra, ld3(B.invI, la), ran)) +
+                         dot(rbn, apply_inv_I(Rb, ld3(B.invI, lb), rbn));
+        st3(s.s_ra, c, ra);
+        st3(s.s_rb, c, rb);
+        s.s_bias[c] = bias;
+        s.s_kn[c] = kn;
+        s.s_mu[c] = sqrtf(w.friction[ga] * w.friction[gb]);
+        const bool skip = (ima == 0.0f && imb == 0.0f);  // physics.comp:531
+        s.s_ab[size_t(c) * 2] = skip ? kNone : la;
+        s.s_ab[size_t(c) * 2 + 1] = lb;
+        w.lambda[c] = 0.0f;
+    }
+    __syncwarp();
+
+    if (mode == 0) {
+        if (lane == 0)
+            for (uint32_t it = 0; it < k.pgs_iterations; ++it)
+                for (uint32_t c = c0; c < c1; ++c) {
+                    const uint32_t la = s.s_ab[size_t(c) * 2];
+                    if (la == kNone) continue;
+                    solve_one(B, la, s.s_ab[size_t(c) * 2 + 1], ld3(w.c_normal, c), ld3(s.s_ra, c),
+                              ld3(s.s_rb, c), s.s_bias[c], s.s_kn[c], s.s_mu[c], &w.lambda[c]);
+                }
+        return;
+    }
+
+    // ---- levels, 32 contacts at a time ----
+    uint32_t maxl = 0;
+    for (uint32_t base = c0; base < c1; base += 32) {
+        const uint32_t c = base + lane;
+        const bool valid = c < c1;
+        const uint32_t la = valid ? s.s_ab[size_t(c) * 2] : kNone;
+        const uint32_t lb = valid ? s.s_ab[size_t(c) * 2 + 1] : 0u;
+        const bool use = valid && la != kNone;
+        const bool da = use && !is_fixed(B, la), db = use && !is_fixed(B, lb);
+        // dynamic bodies, or a sentinel unique to this lane and role
+        const uint32_t xa = da ? la : (0x80000000u | (lane * 2u));
+        const uint32_t xb = db ? lb : (0x80000000u | (lane * 2u + 1u));
+        uint32_t L = use ? max(da ? last[la] : 0u, db ? last[lb] : 0u) + 1u : 0u;
+        for (uint32_t j = 0; j < 32; ++j) {
+            const uint32_t aj = __shfl_sync(full, xa, j), bj = __shfl_sync(full, xb, j);
+            const uint32_t Lj = __shfl_sync(full, L, j);
+            if (use && j < lane && (aj == xa || aj == xb || bj == xa || bj == xb))
+                L = max(L, Lj + 1u);
+        }
+        if (valid) s.s_level[c] = use ? L - 1u : kNone;
+        if (da) atomicMax(&last[la], L);
+        if (db) atomicMax(&last[lb], L);
+        maxl = max(maxl, L);
+        __syncwarp();
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) maxl = max(maxl, __shfl_xor_sync(full, maxl, off));
+
+    // ---- contacts grouped by level, in index order within a level ----
+    uint32_t* lvl = s.s_lvl_start + c0 + scene;  // maxl+1 entries within [c0+scene, c1+scene]
+    uint32_t pos = 0;
+    for (uint32_t l = 0; l < maxl; ++l) {
+        if (lane == 0) lvl[l] = pos;
+        for (uint32_t base = c0; base < c1; base += 32) {
+            const uint32_t c = base + lane;
+            const bool hit = c < c1 && s.s_level[c] == l;
+            const unsigned m = __ballot_sync(full, hit);
+            if (hit) s.s_order[c0 + pos + __popc(m & ((1u << lane) - 1u))] = c;
+            pos += __popc(m);
+        }
+    }
+    if (lane == 0) lvl[maxl] = pos;
+    __syncwarp();
+
+    // ---- Gauss-Seidel sweeps ----
+    for (uint32_t it = 0; it < k.pgs_iterations; ++it) {
+        for (uint32_t l = 0; l < maxl; ++l) {
+            const uint32_t beg = lvl[l], end = lvl[l + 1];
+            for (uint32_t i = beg + lane; i < end; i += 32) {
+                const uint32_t c = s.s_order[c0 + i];
+                solve_one(B, s.s_ab[size_t(c) * 2], s.s_ab[size_t(c) * 2 + 1],
+                          ld3(w.c_normal, c), ld3(s.s_ra, c), ld3(s.s_rb, c), s.s_bias[c],
+                          s.s_kn[c], s.s_mu[c], &w.lambda[c]);
+            }
+            __syncwarp();
+        }
+    }
+}
+
 constexpr uint32_t kSolverMaxSmem = 160 * 1024;
 
 cudaError_t init_solver() {
@@ -263,6 +405,11 @@ cudaError_t init_solver() {
 int launch_solver(const World& w, const Consts& k, const Scratch& s, uint32_t mode, float dt,
                   uint32_t max_scene_bodies, cudaStream_t st) {
     if (w.ns == 0 || w.max_contacts == 0) return 0;
+    if (max_scene_bodies <= kWarpMaxBodies) {
+        const uint32_t blocks = (w.ns + kWarpsPerBlock - 1) / kWarpsPerBlock;
+        k_solver_warp<<<blocks, kWarpsPerBlock * 32, 0, st>>>(w, k, s, mode, dt);
+        return 1;
+    }
     uint32_t smem_bodies = max_scene_bodies;
     if (smem_bodies * kBodySmemWords * 4 > kSolverMaxSmem)
         smem_bodies = kSolverMaxSmem / (kBodySmemWords * 4);

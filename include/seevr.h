@@ -140,6 +140,10 @@ typedef struct seevr_params {
     uint32_t broadphase;       /* enum seevr_broadphase                     */
     uint32_t solver;           /* enum seevr_solver                         */
     uint32_t flags;            /* enum seevr_flags                          */
+    uint32_t bundle_bodies;    /* solver work unit: consecutive scenes are
+                                  solved together up to this many bodies
+                                  (0 = 512); any value gives the same
+                                  results, only speed changes              */
 } seevr_params;
 
 /* Per-stage device timings in milliseconds, summed over the substeps of one

@@ -51,7 +51,8 @@ class Params(C.Structure):
                 ("linear_damping", C.c_float), ("angular_damping", C.c_float),
                 ("mpr_eps", C.c_float), ("mpr_tolerance", C.c_float),
                 ("mpr_iterations", C.c_uint32), ("mpr_discover_trials", C.c_uint32),
-                ("broadphase", C.c_uint32), ("solver", C.c_uint32), ("flags", C.c_uint32)]
+                ("broadphase", C.c_uint32), ("solver", C.c_uint32), ("flags", C.c_uint32),
+                ("bundle_bodies", C.c_uint32)]
 
 
 class Profile(C.Structure):

@@ -55,6 +55,10 @@ struct World {
     const uint32_t* hull_range;  // (start,count) per geom: binding 30 or derived
     const uint32_t* body_scene;  // body -> scene
     const uint32_t* scene_off;   // scene -> first body, [num_scenes+1]
+    // Solver bundles: runs of whole consecutive scenes solved together by
+    // one warp or block, bundle -> first body, [nbundles+1]
+    const uint32_t* bundle_off;
+    uint32_t nbundles;
     uint32_t nb, nv, nhv, ns;
     uint32_t max_pairs, max_contacts;
 };

@@ -41,43 +41,41 @@ __device__ __forceinline__ Shape load_shape(const World& w, uint32_t b) {
     return s;
 }
 
-// support (physics.comp:107-162)
+// support (physics.comp:107-162).  Both paths of the reference visit a list
+// of candidate vertices in order and keep the first strict maximum: all
+// hull vertices when lk == 0 (brute force), else for each of the 3 axes the
+// two lookup bins around the direction's angle.  One loop over candidates
+// serves both, so lanes of a warp holding boxes and spheres share it.
 __device__ __forceinline__ f3 support(const World& w, const Shape& s, f3 d) {
     const f3 ld = mulT(s.R, d);
+    const bool lut = s.lk != 0;
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+    if (lut) {
+        a0 = seevr_atan2f(ld.z, ld.y);  // X axis
+        a1 = seevr_atan2f(ld.z, ld.x);  // Y axis
+        a2 = seevr_atan2f(ld.y, ld.x);  // Z axis
+    }
     float best = -1e10f;
     f3 bv = mk(0.f, 0.f, 0.f);
-    if (s.lk == 0) {
-        for (uint32_t i = 0; i < s.vc; ++i) {
-            const f3 v = ld3(w.hull, s.vs + i);
-            const float dd = dot(v, ld);
-            if (dd > best) {
-                best = dd;
-                bv = v;
+    const uint32_t n = lut ? 6u : s.vc;
+    uint32_t b0 = 0;
+    for (uint32_t k = 0; k < n; ++k) {
+        uint32_t idx = k;
+        if (lut) {
+            const uint32_t ax = k >> 1;
+            if ((k & 1u) == 0u) {
+                float a = ax == 0 ? a0 : (ax == 1 ? a1 : a2);
+                if (a < 0.0f) a += 6.2831853f;
+                const float bin_f = a / 6.2831853f * 64.0f;
+                b0 = uint32_t(bin_f) % 64u;
             }
+            idx = w.sup_lut[s.lk + ax * 64u + ((k & 1u) ? (b0 + 1u) % 64u : b0)];
         }
-        return add(s.p, mul(s.R, bv));
-    }
-    const float angles[3] = {seevr_atan2f(ld.z, ld.y), seevr_atan2f(ld.z, ld.x),
-                             seevr_atan2f(ld.y, ld.x)};
-#pragma unroll
-    for (uint32_t ax = 0; ax < 3; ++ax) {
-        float a = angles[ax];
-        if (a < 0.0f) a += 6.2831853f;
-        const float bin_f = a / 6.2831853f * 64.0f;
-        const uint32_t b0 = uint32_t(bin_f) % 64u;
-        const uint32_t b1 = (b0 + 1u) % 64u;
-        const uint32_t* lut = w.sup_lut + s.lk + ax * 64u;
-        const f3 v0 = ld3(w.hull, s.vs + lut[b0]);
-        const float d0 = dot(v0, ld);
-        if (d0 > best) {
-            best = d0;
-            bv = v0;
-        }
-        const f3 v1 = ld3(w.hull, s.vs + lut[b1]);
-        const float d1 = dot(v1, ld);
-        if (d1 > best) {
-            best = d1;
-            bv = v1;
+        const f3 v = ld3(w.hull, s.vs + idx);
+        const float dd = dot(v, ld);
+        if (dd > best) {
+            best = dd;
+            bv = v;
         }
     }
     return add(s.p, mul(s.R, bv));

@@ -226,6 +226,8 @@ extern "C" seevr_status seevr_physics_step_noalloc(
                              : s.derived_hull_range;
     w.body_scene = body_scene;
     w.scene_off = scene_off;
+    w.bundle_off = scene_off;  // one scene, one solver bundle
+    w.nbundles = 1;
     w.nb = num_bodies;
     w.nv = render ? num_vertices : 0;
     w.nhv = num_hull_verts;

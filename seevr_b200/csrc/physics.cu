@@ -82,6 +82,9 @@ struct seevr_physics {
     Scratch s{};
     uint32_t* body_scene = nullptr;
     uint32_t* scene_off = nullptr;
+    uint32_t* bundle_off = nullptr;  // solver bundles (runs of whole scenes)
+    uint32_t num_bundles = 1;
+    uint32_t max_bundle_bodies = 0;
     uint32_t num_scenes = 1;
     bool scenes_set = false;
     uint32_t single_scene_nb = 0xFFFFFFFFu;
@@ -181,6 +184,7 @@ void setup_world(seevr_physics* h) {
                                          : h->s.derived_hull_range;
     w.body_scene = h->body_scene;
     w.scene_off = h->scene_off;
+    w.bundle_off = h->bundle_off;
     w.max_pairs = h->caps.max_pairs;
     w.max_contacts = h->caps.max_contacts;
     const seevr_params& p = h->params;
@@ -195,13 +199,34 @@ void setup_world(seevr_physics* h) {
     h->k.discover_trials = p.mpr_discover_trials;
 }
 
-__global__ void k_single_scene(uint32_t* body_scene, uint32_t* scene_off, uint32_t nb) {
+__global__ void k_single_scene(uint32_t* body_scene, uint32_t* scene_off, uint32_t* bundle_off,
+                               uint32_t nb) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < nb) body_scene[i] = 0;
     if (i == 0) {
-        scene_off[0] = 0;
-        scene_off[1] = nb;
+        scene_off[0] = bundle_off[0] = 0;
+        scene_off[1] = bundle_off[1] = nb;
     }
+}
+
+// Greedy bundling of consecutive scenes: a bundle grows while its bodies stay
+// within `target` (a scene larger than `target` is a bundle by itself).
+std::vector<uint32_t> make_bundles(const uint32_t* body_offset, uint32_t num_scenes,
+                                   uint32_t target, uint32_t* max_bodies) {
+    std::vector<uint32_t> off{0};
+    uint32_t start = 0, mx = 0;
+    for (uint32_t s = 0; s < num_scenes; ++s) {
+        const uint32_t end = body_offset[s + 1];
+        if (end - body_offset[start] > target && s > start) {
+            off.push_back(body_offset[s]);
+            mx = std::max(mx, body_offset[s] - body_offset[start]);
+            start = s;
+        }
+    }
+    off.push_back(body_offset[num_scenes]);
+    mx = std::max(mx, body_offset[num_scenes] - body_offset[start]);
+    *max_bodies = mx;
+    return off;
 }
 
 // Timed region helper: in profiling mode, brackets the launches of one
@@ -231,6 +256,7 @@ uint64_t issue_frame(seevr_physics* h, uint32_t nb, uint32_t nv, uint32_t nhv, u
     w.nv = nv;
     w.nhv = nhv;
     w.ns = h->num_scenes;
+    w.nbundles = h->num_bundles;
     uint64_t n = 0;
     StageTimer T{h, prof, st};
     const float sub_dt = dt / float(substeps);  // physics.zig:90
@@ -255,7 +281,7 @@ uint64_t issue_frame(seevr_physics* h, uint32_t nb, uint32_t nv, uint32_t nhv, u
         T.end(kStClear);
         T.begin();
         n += launch_solver(w, h->k, h->s, h->params.solver == SEEVR_SOLVER_SEQUENTIAL ? 0u : 1u,
-                           sub_dt, h->max_scene_bodies, st);
+                           sub_dt, h->max_bundle_bodies, st);
         T.end(kStSolve);
     }
     const bool render = nv > 0 && !(h->params.flags & SEEVR_FLAG_SKIP_RENDER_VERTS);
@@ -288,12 +314,15 @@ seevr_status check_step_args(seevr_physics* h, uint32_t nb, uint32_t nv, uint32_
 seevr_status ensure_single_scene(seevr_physics* h, uint32_t nb, cudaStream_t st) {
     if (h->scenes_set || h->single_scene_nb == nb) return SEEVR_OK;
     const uint32_t n = nb > 0 ? nb : 1;
-    k_single_scene<<<(n + 255) / 256, 256, 0, st>>>(h->body_scene, h->scene_off, nb);
+    k_single_scene<<<(n + 255) / 256, 256, 0, st>>>(h->body_scene, h->scene_off, h->bundle_off,
+                                                     nb);
     SEEVR_CUDA(cudaGetLastError());
     h->launches += 1;
     h->single_scene_nb = nb;
     h->max_scene_bodies = nb;
+    h->max_bundle_bodies = nb;
     h->num_scenes = 1;
+    h->num_bundles = 1;
     return SEEVR_OK;
 }
 
@@ -326,6 +355,7 @@ void seevr_params_default(seevr_params* p) {
     p->broadphase = SEEVR_BROADPHASE_N2;
     p->solver = SEEVR_SOLVER_WAVEFRONT;
     p->flags = 0;
+    p->bundle_bodies = 0;
 }
 
 seevr_status seevr_physics_create(const seevr_bindings* b, const seevr_caps* caps,
@@ -393,6 +423,7 @@ seevr_status seevr_physics_create(const seevr_bindings* b, const seevr_caps* cap
     ALLOC(h->s.derived_hull_range, size_t(c.max_bodies) * 2);
     ALLOC(h->body_scene, c.max_bodies);
     ALLOC(h->scene_off, size_t(c.max_scenes) + 1);
+    ALLOC(h->bundle_off, size_t(c.max_scenes) + 1);
     if (p.broadphase == SEEVR_BROADPHASE_LBVH) {
         LbvhScratch& lb = h->lb;
         const size_t n = c.max_bodies;
@@ -463,6 +494,13 @@ seevr_status seevr_physics_set_scenes(seevr_physics* h, const uint32_t* body_off
         return fail(SEEVR_ERR_NOT_SUPPORTED,
                     "the LBVH broadphase steps a single scene; use the all-pairs broadphase for "
                     "batches");
+    uint32_t max_bundle = 0;
+    const uint32_t target = h->params.bundle_bodies ? h->params.bundle_bodies : 512u;
+    const std::vector<uint32_t> bundles = make_bundles(body_offset, num_scenes, target, &max_bundle);
+    SEEVR_CUDA(cudaMemcpy(h->bundle_off, bundles.data(), sizeof(uint32_t) * bundles.size(),
+                          cudaMemcpyHostToDevice));
+    h->num_bundles = uint32_t(bundles.size() - 1);
+    h->max_bundle_bodies = max_bundle;
     h->num_scenes = num_scenes;
     h->scenes_set = true;
     h->single_scene_nb = nb;

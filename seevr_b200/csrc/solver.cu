@@ -1,7 +1,13 @@
 // solver.cu — PGS contact solver (step 5, physics.comp:500-583) and the
 // impulse clear (step 4, physics.comp:494-497).
 //
-// One CTA per scene.  Phase 1 stages the scene's bodies (velocity, angular
+// Work is split into bundles: runs of whole consecutive scenes.  Scenes share
+// no body, so a bundle is solved exactly like one scene whose contacts are
+// the union of its scenes' (each scene's contacts keep their order, and the
+// wavefront levels of different scenes simply merge); small scenes are
+// bundled so that a warp's lanes have work.
+//
+// One CTA per bundle.  Phase 1 stages the bundle's bodies (velocity, angular
 // velocity, rotation matrix, inverse inertia, inverse mass) in shared memory
 // (global scratch when the scene is too large).  Phase 2 computes, for every
 // contact in parallel, the values the reference recomputes on every
@@ -99,8 +105,8 @@ __global__ void __launch_bounds__(kSolverThreads)
     k_solver(World w, Consts k, Scratch s, uint32_t mode, float dt, uint32_t smem_bodies) {
     extern __shared__ float sm[];
     __shared__ uint32_t sh_c0, sh_c1, sh_levels;
-    const uint32_t scene = blockIdx.x;
-    const uint32_t b0 = w.scene_off[scene], b1 = w.scene_off[scene + 1];
+    const uint32_t scene = blockIdx.x;  // bundle index
+    const uint32_t b0 = w.bundle_off[scene], b1 = w.bundle_off[scene + 1];
     const uint32_t nbs = b1 - b0;
     const uint32_t nc = min(w.counters[1], w.max_contacts);
     if (threadIdx.x == 0) {
@@ -251,8 +257,8 @@ __global__ void __launch_bounds__(kSolverThreads)
     }
 }
 
-// ---- warp per scene -------------------------------------------------------
-// Scenes of up to kWarpMaxBodies bodies: one warp per scene, body state in
+// ---- warp per bundle ------------------------------------------------------
+// Bundles of up to kWarpMaxBodies bodies: one warp per bundle, body state in
 // global memory (L1-resident), __syncwarp between levels.  Levels are
 // assigned 32 contacts at a time: each lane starts from the latest level of
 // its bodies in earlier chunks, then lanes are visited in order and every
@@ -265,9 +271,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
     __shared__ uint32_t sh_last[kWarpsPerBlock][kWarpMaxBodies];
     const unsigned full = 0xFFFFFFFFu;
     const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
-    const uint32_t scene = blockIdx.x * kWarpsPerBlock + wid;
-    if (scene >= w.ns) return;
-    const uint32_t b0 = w.scene_off[scene], b1 = w.scene_off[scene + 1];
+    const uint32_t scene = blockIdx.x * kWarpsPerBlock + wid;  // bundle index
+    if (scene >= w.nbundles) return;
+    const uint32_t b0 = w.bundle_off[scene], b1 = w.bundle_off[scene + 1];
     const uint32_t nbs = b1 - b0;
     const uint32_t nc = min(w.counters[1], w.max_contacts);
     uint32_t c0 = 0, c1 = 0;
@@ -404,9 +410,9 @@ cudaError_t init_solver() {
 
 int launch_solver(const World& w, const Consts& k, const Scratch& s, uint32_t mode, float dt,
                   uint32_t max_scene_bodies, cudaStream_t st) {
-    if (w.ns == 0 || w.max_contacts == 0) return 0;
+    if (w.nbundles == 0 || w.max_contacts == 0) return 0;
     if (max_scene_bodies <= kWarpMaxBodies) {
-        const uint32_t blocks = (w.ns + kWarpsPerBlock - 1) / kWarpsPerBlock;
+        const uint32_t blocks = (w.nbundles + kWarpsPerBlock - 1) / kWarpsPerBlock;
         k_solver_warp<<<blocks, kWarpsPerBlock * 32, 0, st>>>(w, k, s, mode, dt);
         return 1;
     }
@@ -414,7 +420,7 @@ int launch_solver(const World& w, const Consts& k, const Scratch& s, uint32_t mo
     if (smem_bodies * kBodySmemWords * 4 > kSolverMaxSmem)
         smem_bodies = kSolverMaxSmem / (kBodySmemWords * 4);
     const size_t smem = size_t(smem_bodies) * kBodySmemWords * 4;
-    k_solver<<<w.ns, kSolverThreads, smem, st>>>(w, k, s, mode, dt, smem_bodies);
+    k_solver<<<w.nbundles, kSolverThreads, smem, st>>>(w, k, s, mode, dt, smem_bodies);
     return 1;
 }
 

@@ -58,6 +58,7 @@ struct World {
     // Solver bundles: runs of whole consecutive scenes solved together by
     // one warp or block, bundle -> first body, [nbundles+1]
     const uint32_t* bundle_off;
+    const uint32_t* body_bundle;  // body -> bundle
     uint32_t nbundles;
     uint32_t nb, nv, nhv, ns;
     uint32_t max_pairs, max_contacts;
@@ -90,6 +91,10 @@ struct Scratch {
     uint32_t* s_level;      // [max_contacts]
     uint32_t* s_order;      // [max_contacts]
     uint32_t* s_lvl_start;  // [max_contacts + max_scenes + 1]
+    float* s_n;             // [max_contacts*3] normals in solve order
+    float* s_lam;           // [max_contacts] impulses of large bundles
+    uint32_t* s_abp;        // [max_contacts*2] body pair in solve order
+    uint32_t* bundle_c0;    // [max_scenes + 1] first contact of each bundle
     // solver, per body (global-memory path for scenes too large for smem)
     float* s_R;             // [max_bodies*9]
     uint32_t* s_last;       // [max_bodies]

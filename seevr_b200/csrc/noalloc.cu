@@ -10,7 +10,7 @@
 // entry point runs the same kernels on scratch carved from one file-scope
 // device array, so the caller provides only the bound buffers and a stream.
 //
-// The array holds NOALLOC_BYTES (2.6 MB) on every device that loads the
+// The array holds SEEVR_NOALLOC_SCRATCH_BYTES (2.9 MB) on every device that loads the
 // library, until the process exits.  All calls share it: calls whose GPU
 // work overlaps (different streams, or different host threads on one
 // device) race on it and must be serialised by the caller.  Each call
@@ -56,7 +56,11 @@ constexpr size_t kOffLast = align256(kOffR + 36ull * kNaBodies);
 constexpr size_t kOffHullRange = align256(kOffLast + 4ull * kNaBodies);
 constexpr size_t kOffBodyScene = align256(kOffHullRange + 8ull * kNaBodies);
 constexpr size_t kOffSceneOff = align256(kOffBodyScene + 4ull * kNaBodies);
-constexpr size_t kNaBytes = align256(kOffSceneOff + 8);
+constexpr size_t kOffN = align256(kOffSceneOff + 8);
+constexpr size_t kOffLam = align256(kOffN + 12ull * kNaContacts);
+constexpr size_t kOffAbp = align256(kOffLam + 4ull * kNaContacts);
+constexpr size_t kOffBundleC0 = align256(kOffAbp + 8ull * kNaContacts);
+constexpr size_t kNaBytes = align256(kOffBundleC0 + 16);
 static_assert(kNaBytes == SEEVR_NOALLOC_SCRATCH_BYTES, "header constant out of date");
 
 // The scratch itself.  In host code this name is a host-side stand-in, not
@@ -189,6 +193,10 @@ extern "C" seevr_status seevr_physics_step_noalloc(
     s.s_R = reinterpret_cast<float*>(at(kOffR));
     s.s_last = reinterpret_cast<uint32_t*>(at(kOffLast));
     s.derived_hull_range = reinterpret_cast<uint32_t*>(at(kOffHullRange));
+    s.s_n = reinterpret_cast<float*>(at(kOffN));
+    s.s_lam = reinterpret_cast<float*>(at(kOffLam));
+    s.s_abp = reinterpret_cast<uint32_t*>(at(kOffAbp));
+    s.bundle_c0 = reinterpret_cast<uint32_t*>(at(kOffBundleC0));
     uint32_t* body_scene = reinterpret_cast<uint32_t*>(at(kOffBodyScene));
     uint32_t* scene_off = reinterpret_cast<uint32_t*>(at(kOffSceneOff));
 
@@ -227,6 +235,7 @@ extern "C" seevr_status seevr_physics_step_noalloc(
     w.body_scene = body_scene;
     w.scene_off = scene_off;
     w.bundle_off = scene_off;  // one scene, one solver bundle
+    w.body_bundle = body_scene;
     w.nbundles = 1;
     w.nb = num_bodies;
     w.nv = render ? num_vertices : 0;

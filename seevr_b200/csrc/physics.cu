@@ -83,6 +83,7 @@ struct seevr_physics {
     uint32_t* body_scene = nullptr;
     uint32_t* scene_off = nullptr;
     uint32_t* bundle_off = nullptr;  // solver bundles (runs of whole scenes)
+    uint32_t* body_bundle = nullptr;  // body -> bundle
     uint32_t num_bundles = 1;
     uint32_t max_bundle_bodies = 0;
     uint32_t num_scenes = 1;
@@ -185,6 +186,7 @@ void setup_world(seevr_physics* h) {
     w.body_scene = h->body_scene;
     w.scene_off = h->scene_off;
     w.bundle_off = h->bundle_off;
+    w.body_bundle = h->body_bundle;
     w.max_pairs = h->caps.max_pairs;
     w.max_contacts = h->caps.max_contacts;
     const seevr_params& p = h->params;
@@ -199,10 +201,10 @@ void setup_world(seevr_physics* h) {
     h->k.discover_trials = p.mpr_discover_trials;
 }
 
-__global__ void k_single_scene(uint32_t* body_scene, uint32_t* scene_off, uint32_t* bundle_off,
-                               uint32_t nb) {
+__global__ void k_single_scene(uint32_t* body_scene, uint32_t* body_bundle, uint32_t* scene_off,
+                               uint32_t* bundle_off, uint32_t nb) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < nb) body_scene[i] = 0;
+    if (i < nb) body_scene[i] = body_bundle[i] = 0;
     if (i == 0) {
         scene_off[0] = bundle_off[0] = 0;
         scene_off[1] = bundle_off[1] = nb;
@@ -314,8 +316,8 @@ seevr_status check_step_args(seevr_physics* h, uint32_t nb, uint32_t nv, uint32_
 seevr_status ensure_single_scene(seevr_physics* h, uint32_t nb, cudaStream_t st) {
     if (h->scenes_set || h->single_scene_nb == nb) return SEEVR_OK;
     const uint32_t n = nb > 0 ? nb : 1;
-    k_single_scene<<<(n + 255) / 256, 256, 0, st>>>(h->body_scene, h->scene_off, h->bundle_off,
-                                                     nb);
+    k_single_scene<<<(n + 255) / 256, 256, 0, st>>>(h->body_scene, h->body_bundle, h->scene_off,
+                                                     h->bundle_off, nb);
     SEEVR_CUDA(cudaGetLastError());
     h->launches += 1;
     h->single_scene_nb = nb;
@@ -418,6 +420,11 @@ seevr_status seevr_physics_create(const seevr_bindings* b, const seevr_caps* cap
     ALLOC(h->s.s_level, c.max_contacts);
     ALLOC(h->s.s_order, c.max_contacts);
     ALLOC(h->s.s_lvl_start, size_t(c.max_contacts) + c.max_scenes + 1);
+    ALLOC(h->s.s_n, size_t(c.max_contacts) * 3);
+    ALLOC(h->s.s_lam, c.max_contacts);
+    ALLOC(h->s.s_abp, size_t(c.max_contacts) * 2);
+    ALLOC(h->s.bundle_c0, size_t(c.max_scenes) + 2);
+    ALLOC(h->body_bundle, c.max_bodies);
     ALLOC(h->s.s_R, size_t(c.max_bodies) * 9);
     ALLOC(h->s.s_last, c.max_bodies);
     ALLOC(h->s.derived_hull_range, size_t(c.max_bodies) * 2);
@@ -499,6 +506,9 @@ seevr_status seevr_physics_set_scenes(seevr_physics* h, const uint32_t* body_off
     const std::vector<uint32_t> bundles = make_bundles(body_offset, num_scenes, target, &max_bundle);
     SEEVR_CUDA(cudaMemcpy(h->bundle_off, bundles.data(), sizeof(uint32_t) * bundles.size(),
                           cudaMemcpyHostToDevice));
+    for (size_t k = 0; k + 1 < bundles.size(); ++k)
+        for (uint32_t i = bundles[k]; i < bundles[k + 1]; ++i) bs[i] = uint32_t(k);
+    SEEVR_CUDA(cudaMemcpy(h->body_bundle, bs.data(), sizeof(uint32_t) * nb, cudaMemcpyHostToDevice));
     h->num_bundles = uint32_t(bundles.size() - 1);
     h->max_bundle_bodies = max_bundle;
     h->num_scenes = num_scenes;

@@ -88,35 +88,17 @@ __device__ __forceinline__ void solve_one(const BodyView& B, uint32_t la, uint32
     }
 }
 
-__device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t* a, uint32_t n, uint32_t key) {
-    uint32_t lo = 0, hi = n;
-    while (lo < hi) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (a[mid] < key) lo = mid + 1;
-        else hi = mid;
-    }
-    return lo;
-}
-
 constexpr uint32_t kSolverThreads = 128;
 constexpr uint32_t kBodySmemWords = 20;  // v3 w3 R9 invI3 invm1 last1
 
 __global__ void __launch_bounds__(kSolverThreads)
     k_solver(World w, Consts k, Scratch s, uint32_t mode, float dt, uint32_t smem_bodies) {
     extern __shared__ float sm[];
-    __shared__ uint32_t sh_c0, sh_c1, sh_levels;
+    __shared__ uint32_t sh_levels;
     const uint32_t scene = blockIdx.x;  // bundle index
     const uint32_t b0 = w.bundle_off[scene], b1 = w.bundle_off[scene + 1];
     const uint32_t nbs = b1 - b0;
-    const uint32_t nc = min(w.counters[1], w.max_contacts);
-    if (threadIdx.x == 0) {
-        // contacts are in (a, b) lexicographic order, scenes own contiguous
-        // body ranges: the scene's contacts are a contiguous range
-        sh_c0 = lower_bound_u32(w.c_a, nc, b0);
-        sh_c1 = lower_bound_u32(w.c_a, nc, b1);
-    }
-    __syncthreads();
-    const uint32_t c0 = sh_c0, c1 = sh_c1;
+    const uint32_t c0 = s.bundle_c0[scene], c1 = s.bundle_c0[scene + 1];
     if (c0 >= c1) return;
     const uint32_t tid = threadIdx.x;
 
@@ -257,53 +239,128 @@ __global__ void __launch_bounds__(kSolverThreads)
     }
 }
 
-// ---- warp per bundle ------------------------------------------------------
-// Bundles of up to kWarpMaxBodies bodies: one warp per bundle, body state in
-// global memory (L1-resident), __syncwarp between levels.  Levels are
+// ---- contact range of every bundle ----------------------------------------
+// Contacts are in (a, b) order and bundles own consecutive body ranges, so
+// each bundle's contacts form one run; bundle_c0[k] = first contact of bundle
+// k (bundle_c0[nbundles] = the contact count).  Marked in one pass instead of
+// a binary search at the start of every solver block.
+__global__ void k_bundle_ranges(World w, uint32_t* __restrict__ bundle_c0) {
+    const uint32_t nc = min(w.counters[1], w.max_contacts);
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c <= nc; c += gridDim.x * blockDim.x) {
+        const uint32_t cur = c < nc ? w.body_bundle[w.geom_body[w.c_a[c]]] : w.nbundles;
+        const int prev = c > 0 ? int(w.body_bundle[w.geom_body[w.c_a[c - 1]]]) : -1;
+        for (int k = prev + 1; k <= int(cur); ++k) bundle_c0[k] = c;
+    }
+}
+
+// ---- warp per bundle --------------------------------------------------------
+// Bundles of up to kWarpMaxBodies bodies: one warp per bundle, __syncwarp
+// between levels.  What a solve round waits on lives in shared memory: the
+// bundle's velocities and angular velocities, the impulses and the level
+// boundaries.  The per-contact constants are computed directly in level
+// order, so the lanes of a round read consecutive entries.  Levels are
 // assigned 32 contacts at a time: each lane starts from the latest level of
 // its bodies in earlier chunks, then lanes are visited in order and every
 // later lane sharing a dynamic body with lane j moves past lane j's level.
 constexpr uint32_t kWarpMaxBodies = 1024;
 constexpr uint32_t kWarpsPerBlock = 4;
+constexpr uint32_t kWarpLamCap = 1024;   // impulses per bundle held in smem
+constexpr uint32_t kWarpLevelCap = 128;  // level boundaries held in smem
+
+__host__ __device__ constexpr uint32_t warp_smem_words(uint32_t nbmax) {
+    return 7 * nbmax + kWarpLamCap + kWarpLevelCap;
+}
 
 __global__ void __launch_bounds__(kWarpsPerBlock * 32)
-    k_solver_warp(World w, Consts k, Scratch s, uint32_t mode, float dt) {
-    __shared__ uint32_t sh_last[kWarpsPerBlock][kWarpMaxBodies];
+    k_solver_warp(World w, Consts k, Scratch s, uint32_t mode, float dt, uint32_t nbmax) {
+    extern __shared__ float sm[];
     const unsigned full = 0xFFFFFFFFu;
     const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
-    const uint32_t scene = blockIdx.x * kWarpsPerBlock + wid;  // bundle index
-    if (scene >= w.nbundles) return;
-    const uint32_t b0 = w.bundle_off[scene], b1 = w.bundle_off[scene + 1];
-    const uint32_t nbs = b1 - b0;
-    const uint32_t nc = min(w.counters[1], w.max_contacts);
-    uint32_t c0 = 0, c1 = 0;
-    if (lane == 0) {
-        c0 = lower_bound_u32(w.c_a, nc, b0);
-        c1 = lower_bound_u32(w.c_a, nc, b1);
-    }
-    c0 = __shfl_sync(full, c0, 0);
-    c1 = __shfl_sync(full, c1, 0);
+    const uint32_t bundle = blockIdx.x * kWarpsPerBlock + wid;
+    if (bundle >= w.nbundles) return;
+    const uint32_t b0 = w.bundle_off[bundle], b1 = w.bundle_off[bundle + 1];
+    const uint32_t c0 = s.bundle_c0[bundle], c1 = s.bundle_c0[bundle + 1];
     if (c0 >= c1) return;
+    const uint32_t nbs = b1 - b0, ncb = c1 - c0;
 
-    BodyView B;
-    B.v = w.vel + size_t(b0) * 3;
-    B.w = w.omega + size_t(b0) * 3;
+    float* base = sm + size_t(wid) * warp_smem_words(nbmax);
+    float* V = base;
+    float* Wv = base + 3 * nbmax;
+    uint32_t* last = reinterpret_cast<uint32_t*>(base + 6 * nbmax);
+    float* lam = ncb <= kWarpLamCap ? base + 7 * nbmax : s.s_lam + c0;
+    uint32_t* lvl_sm = reinterpret_cast<uint32_t*>(base + 7 * nbmax + kWarpLamCap);
     float* R = s.s_R + size_t(b0) * 9;
-    B.R = R;
-    B.invI = w.inv_inertia + size_t(b0) * 3;
-    B.invm = w.inv_mass + b0;
-    uint32_t* last = sh_last[wid];
     for (uint32_t i = lane; i < nbs; i += 32) {
+        st3(V, i, ld3(w.vel, b0 + i));
+        st3(Wv, i, ld3(w.omega, b0 + i));
         st_m3(R, i, quat_to_mat(w.quat, b0 + i));
         last[i] = 0;
     }
+    BodyView B{V, Wv, R, w.inv_inertia + size_t(b0) * 3, w.inv_mass + b0};
+
+    // ---- bodies of each contact; both inverse masses zero -> skipped (531)
+    for (uint32_t c = c0 + lane; c < c1; c += 32) {
+        const uint32_t la = w.geom_body[w.c_a[c]] - b0, lb = w.geom_body[w.c_b[c]] - b0;
+        const bool skip = B.invm[la] == 0.0f && B.invm[lb] == 0.0f;
+        s.s_ab[size_t(c) * 2] = skip ? kNone : la;
+        s.s_ab[size_t(c) * 2 + 1] = lb;
+    }
     __syncwarp();
 
-    // per-contact constants (physics.comp:504-521, 533-546)
-    for (uint32_t c = c0 + lane; c < c1; c += 32) {
+    // ---- levels (WAVEFRONT) or one level in index order (SEQUENTIAL) ----
+    uint32_t maxl = 0;
+    for (uint32_t cb = c0; cb < c1; cb += 32) {
+        const uint32_t c = cb + lane;
+        const bool valid = c < c1;
+        const uint32_t la = valid ? s.s_ab[size_t(c) * 2] : kNone;
+        const uint32_t lb = valid ? s.s_ab[size_t(c) * 2 + 1] : 0u;
+        const bool use = valid && la != kNone;
+        uint32_t L = use ? 1u : 0u;
+        if (mode != 0) {
+            const bool da = use && !is_fixed(B, la), db = use && !is_fixed(B, lb);
+            // dynamic bodies, or a sentinel unique to this lane and role
+            const uint32_t xa = da ? la : (0x80000000u | (lane * 2u));
+            const uint32_t xb = db ? lb : (0x80000000u | (lane * 2u + 1u));
+            if (use) L = max(da ? last[la] : 0u, db ? last[lb] : 0u) + 1u;
+            for (uint32_t j = 0; j < 32; ++j) {
+                const uint32_t aj = __shfl_sync(full, xa, j), bj = __shfl_sync(full, xb, j);
+                const uint32_t Lj = __shfl_sync(full, L, j);
+                if (use && j < lane && (aj == xa || aj == xb || bj == xa || bj == xb))
+                    L = max(L, Lj + 1u);
+            }
+            if (da) atomicMax(&last[la], L);
+            if (db) atomicMax(&last[lb], L);
+        }
+        if (valid) s.s_level[c] = use ? L - 1u : kNone;
+        maxl = max(maxl, L);
+        __syncwarp();
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) maxl = max(maxl, __shfl_xor_sync(full, maxl, off));
+
+    // ---- positions: contacts grouped by level, index order within a level
+    uint32_t* lvl = maxl < kWarpLevelCap ? lvl_sm : s.s_lvl_start + c0 + bundle;
+    uint32_t pos = 0;
+    for (uint32_t l = 0; l < maxl; ++l) {
+        if (lane == 0) lvl[l] = pos;
+        for (uint32_t cb = c0; cb < c1; cb += 32) {
+            const uint32_t c = cb + lane;
+            const bool hit = c < c1 && s.s_level[c] == l;
+            const unsigned m = __ballot_sync(full, hit);
+            if (hit) s.s_order[c0 + pos + __popc(m & ((1u << lane) - 1u))] = c;
+            pos += __popc(m);
+        }
+    }
+    if (lane == 0) lvl[maxl] = pos;
+    __syncwarp();
+
+    // ---- per-contact constants in position order (physics.comp:504-521,
+    // 533-546), from the pre-solve velocities
+    for (uint32_t i = lane; i < pos; i += 32) {
+        const uint32_t c = s.s_order[c0 + i], q = c0 + i;
         const uint32_t ga = w.c_a[c], gb = w.c_b[c];
-        const uint32_t a = w.geom_body[ga], b = w.geom_body[gb];
-        const uint32_t la = a - b0, lb = b - b0;
+        const uint32_t la = s.s_ab[size_t(c) * 2], lb = s.s_ab[size_t(c) * 2 + 1];
+        const uint32_t a = b0 + la, b = b0 + lb;
         const f3 n = ld3(w.c_normal, c), cp = ld3(w.c_pos, c);
         const f3 ra = sub(cp, ld3(w.pos, a)), rb = sub(cp, ld3(w.pos, b));
         const f3 va = add(ld3(B.v, la), cross(ld3(B.w, la), ra));
@@ -316,92 +373,58 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
         const f3 ran = cross(ra, n), rbn = cross(rb, n);
         const float kn = ima + imb + dot(ran, apply_inv_I(Ra, ld3(B.invI, la), ran)) +
                          dot(rbn, apply_inv_I(Rb, ld3(B.invI, lb), rbn));
-        st3(s.s_ra, c, ra);
-        st3(s.s_rb, c, rb);
-        s.s_bias[c] = bias;
-        s.s_kn[c] = kn;
-        s.s_mu[c] = sqrtf(w.friction[ga] * w.friction[gb]);
-        const bool skip = (ima == 0.0f && imb == 0.0f);  // physics.comp:531
-        s.s_ab[size_t(c) * 2] = skip ? kNone : la;
-        s.s_ab[size_t(c) * 2 + 1] = lb;
-        w.lambda[c] = 0.0f;
+        st3(s.s_n, q, n);
+        st3(s.s_ra, q, ra);
+        st3(s.s_rb, q, rb);
+        s.s_bias[q] = bias;
+        s.s_kn[q] = kn;
+        s.s_mu[q] = sqrtf(w.friction[ga] * w.friction[gb]);
+        s.s_abp[size_t(q) * 2] = la;
+        s.s_abp[size_t(q) * 2 + 1] = lb;
+        lam[i] = 0.0f;
     }
-    __syncwarp();
-
-    if (mode == 0) {
-        if (lane == 0)
-            for (uint32_t it = 0; it < k.pgs_iterations; ++it)
-                for (uint32_t c = c0; c < c1; ++c) {
-                    const uint32_t la = s.s_ab[size_t(c) * 2];
-                    if (la == kNone) continue;
-                    solve_one(B, la, s.s_ab[size_t(c) * 2 + 1], ld3(w.c_normal, c), ld3(s.s_ra, c),
-                              ld3(s.s_rb, c), s.s_bias[c], s.s_kn[c], s.s_mu[c], &w.lambda[c]);
-                }
-        return;
-    }
-
-    // ---- levels, 32 contacts at a time ----
-    uint32_t maxl = 0;
-    for (uint32_t base = c0; base < c1; base += 32) {
-        const uint32_t c = base + lane;
-        const bool valid = c < c1;
-        const uint32_t la = valid ? s.s_ab[size_t(c) * 2] : kNone;
-        const uint32_t lb = valid ? s.s_ab[size_t(c) * 2 + 1] : 0u;
-        const bool use = valid && la != kNone;
-        const bool da = use && !is_fixed(B, la), db = use && !is_fixed(B, lb);
-        // dynamic bodies, or a sentinel unique to this lane and role
-        const uint32_t xa = da ? la : (0x80000000u | (lane * 2u));
-        const uint32_t xb = db ? lb : (0x80000000u | (lane * 2u + 1u));
-        uint32_t L = use ? max(da ? last[la] : 0u, db ? last[lb] : 0u) + 1u : 0u;
-        for (uint32_t j = 0; j < 32; ++j) {
-            const uint32_t aj = __shfl_sync(full, xa, j), bj = __shfl_sync(full, xb, j);
-            const uint32_t Lj = __shfl_sync(full, L, j);
-            if (use && j < lane && (aj == xa || aj == xb || bj == xa || bj == xb))
-                L = max(L, Lj + 1u);
-        }
-        if (valid) s.s_level[c] = use ? L - 1u : kNone;
-        if (da) atomicMax(&last[la], L);
-        if (db) atomicMax(&last[lb], L);
-        maxl = max(maxl, L);
-        __syncwarp();
-    }
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) maxl = max(maxl, __shfl_xor_sync(full, maxl, off));
-
-    // ---- contacts grouped by level, in index order within a level ----
-    uint32_t* lvl = s.s_lvl_start + c0 + scene;  // maxl+1 entries within [c0+scene, c1+scene]
-    uint32_t pos = 0;
-    for (uint32_t l = 0; l < maxl; ++l) {
-        if (lane == 0) lvl[l] = pos;
-        for (uint32_t base = c0; base < c1; base += 32) {
-            const uint32_t c = base + lane;
-            const bool hit = c < c1 && s.s_level[c] == l;
-            const unsigned m = __ballot_sync(full, hit);
-            if (hit) s.s_order[c0 + pos + __popc(m & ((1u << lane) - 1u))] = c;
-            pos += __popc(m);
-        }
-    }
-    if (lane == 0) lvl[maxl] = pos;
     __syncwarp();
 
     // ---- Gauss-Seidel sweeps ----
-    for (uint32_t it = 0; it < k.pgs_iterations; ++it) {
-        for (uint32_t l = 0; l < maxl; ++l) {
-            const uint32_t beg = lvl[l], end = lvl[l + 1];
-            for (uint32_t i = beg + lane; i < end; i += 32) {
-                const uint32_t c = s.s_order[c0 + i];
-                solve_one(B, s.s_ab[size_t(c) * 2], s.s_ab[size_t(c) * 2 + 1],
-                          ld3(w.c_normal, c), ld3(s.s_ra, c), ld3(s.s_rb, c), s.s_bias[c],
-                          s.s_kn[c], s.s_mu[c], &w.lambda[c]);
+    if (mode == 0) {
+        if (lane == 0)
+            for (uint32_t it = 0; it < k.pgs_iterations; ++it)
+                for (uint32_t i = 0; i < pos; ++i) {
+                    const uint32_t q = c0 + i;
+                    solve_one(B, s.s_abp[size_t(q) * 2], s.s_abp[size_t(q) * 2 + 1], ld3(s.s_n, q),
+                              ld3(s.s_ra, q), ld3(s.s_rb, q), s.s_bias[q], s.s_kn[q], s.s_mu[q],
+                              &lam[i]);
+                }
+    } else {
+        for (uint32_t it = 0; it < k.pgs_iterations; ++it) {
+            for (uint32_t l = 0; l < maxl; ++l) {
+                const uint32_t beg = lvl[l], end = lvl[l + 1];
+                for (uint32_t i = beg + lane; i < end; i += 32) {
+                    const uint32_t q = c0 + i;
+                    solve_one(B, s.s_abp[size_t(q) * 2], s.s_abp[size_t(q) * 2 + 1], ld3(s.s_n, q),
+                              ld3(s.s_ra, q), ld3(s.s_rb, q), s.s_bias[q], s.s_kn[q], s.s_mu[q],
+                              &lam[i]);
+                }
+                __syncwarp();
             }
-            __syncwarp();
         }
     }
+    __syncwarp();
+    // ---- results back to the bound buffers ----
+    for (uint32_t i = lane; i < nbs; i += 32) {
+        st3(w.vel, b0 + i, ld3(V, i));
+        st3(w.omega, b0 + i, ld3(Wv, i));
+    }
+    for (uint32_t i = lane; i < pos; i += 32) w.lambda[s.s_order[c0 + i]] = lam[i];
 }
 
 constexpr uint32_t kSolverMaxSmem = 160 * 1024;
 
 cudaError_t init_solver() {
+    const cudaError_t e = cudaFuncSetAttribute(
+        k_solver_warp, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        int(kWarpsPerBlock * warp_smem_words(kWarpMaxBodies) * sizeof(float)));
+    if (e != cudaSuccess) return e;
     // opt in to more than 48 KB of dynamic shared memory; done at handle
     // creation so that no attribute call happens during graph capture
     return cudaFuncSetAttribute(k_solver, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -411,17 +434,22 @@ cudaError_t init_solver() {
 int launch_solver(const World& w, const Consts& k, const Scratch& s, uint32_t mode, float dt,
                   uint32_t max_scene_bodies, cudaStream_t st) {
     if (w.nbundles == 0 || w.max_contacts == 0) return 0;
+    uint32_t rb = (w.max_contacts + 1 + 255) / 256;
+    if (rb > 148u * 8u) rb = 148u * 8u;
+    k_bundle_ranges<<<rb, 256, 0, st>>>(w, s.bundle_c0);
     if (max_scene_bodies <= kWarpMaxBodies) {
+        const uint32_t nbmax = max_scene_bodies ? max_scene_bodies : 1u;
         const uint32_t blocks = (w.nbundles + kWarpsPerBlock - 1) / kWarpsPerBlock;
-        k_solver_warp<<<blocks, kWarpsPerBlock * 32, 0, st>>>(w, k, s, mode, dt);
-        return 1;
+        const size_t smem = size_t(kWarpsPerBlock) * warp_smem_words(nbmax) * sizeof(float);
+        k_solver_warp<<<blocks, kWarpsPerBlock * 32, smem, st>>>(w, k, s, mode, dt, nbmax);
+        return 2;
     }
     uint32_t smem_bodies = max_scene_bodies;
     if (smem_bodies * kBodySmemWords * 4 > kSolverMaxSmem)
         smem_bodies = kSolverMaxSmem / (kBodySmemWords * 4);
     const size_t smem = size_t(smem_bodies) * kBodySmemWords * 4;
     k_solver<<<w.nbundles, kSolverThreads, smem, st>>>(w, k, s, mode, dt, smem_bodies);
-    return 1;
+    return 2;
 }
 
 }  // namespace seevr

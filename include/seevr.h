@@ -281,6 +281,51 @@ uint64_t seevr_physics_kernel_launches(const seevr_physics* h);
 seevr_status seevr_physics_read_lbvh(seevr_physics* h, uint32_t n, uint32_t* morton_sorted,
                                      uint32_t* order, float bounds[6]);
 
+/* ---- triangle LBVH (bvh.zig / bvh.comp) ---------------------------------- */
+
+/* Binding indices of BVH.init (bvh.zig:32-51), identical to bvh.comp's
+ * `binding=` numbers (bvh.comp:11-28); temp (16) and temp_u (17) are one
+ * buffer in the reference and may alias here too. */
+enum seevr_bvh_binding {
+    SEEVR_BVH_VERTICES = 0,      /* f32[V*3]                r */
+    SEEVR_BVH_INDICES = 1,       /* u32[T*3]                r */
+    SEEVR_BVH_CENTROIDS = 2,     /* f32[T*3]                w */
+    SEEVR_BVH_MORTON = 3,        /* u32[T] sorted codes     w */
+    SEEVR_BVH_MORTON_TEMP = 4,   /* u32[T] sort ping-pong   w */
+    SEEVR_BVH_SORT_INDICES = 5,  /* u32[T] triangle of each sorted slot w */
+    SEEVR_BVH_SORT_TEMP = 6,     /* u32[T] sort ping-pong   w */
+    SEEVR_BVH_SCENE_BOUNDS = 7,  /* f32[6] centroid bounds  w */
+    SEEVR_BVH_NODE_MIN = 8,      /* f32[(2T-1)*3]           w */
+    SEEVR_BVH_NODE_MAX = 9,      /* f32[(2T-1)*3]           w */
+    SEEVR_BVH_LEFT = 10,         /* u32[2T-1]               w */
+    SEEVR_BVH_RIGHT = 11,        /* u32[2T-1]               w */
+    SEEVR_BVH_COUNT = 12,        /* u32[2T-1] 1 on leaves   w */
+    SEEVR_BVH_PARENT = 13,       /* u32[2T-1] root = 0xFFFFFFFF w */
+    SEEVR_BVH_PRIM_INDICES = 14, /* u32[T]                  w */
+    SEEVR_BVH_FLAGS = 15,        /* u32[T] refit flags      w */
+    SEEVR_BVH_TEMP = 16,         /* unused (may be NULL)      */
+    SEEVR_BVH_TEMP_U = 17,       /* u32 work area: 8 + 1024 + 1 + ceil(T/2048)*256 words */
+    SEEVR_BVH_NUM_BINDINGS = 18
+};
+
+typedef struct seevr_bvh_bindings {
+    void* ptr[SEEVR_BVH_NUM_BINDINGS];
+    uint64_t bytes[SEEVR_BVH_NUM_BINDINGS];
+} seevr_bvh_bindings;
+
+typedef struct seevr_bvh seevr_bvh;
+
+/* Replaces BVH.init (bvh.zig:29-61): binds the 18 buffers for up to
+ * max_tris triangles.  Allocates no device memory. */
+seevr_status seevr_bvh_create(const seevr_bvh_bindings* bindings, uint32_t max_tris,
+                              seevr_bvh** out);
+/* Replaces BVH.build(num_tris) (bvh.zig:63-172): centroids, 30-bit Morton
+ * codes, stable radix sort, Karras hierarchy, leaf boxes and bottom-up refit
+ * over the triangles `indices` makes of `vertices`.  Synchronous. */
+seevr_status seevr_bvh_build(seevr_bvh* h, uint32_t num_tris);
+/* Replaces BVH.deinit (bvh.zig:208-210). */
+void seevr_bvh_destroy(seevr_bvh* h);
+
 const char* seevr_status_string(seevr_status s);
 const char* seevr_last_error(void);
 int seevr_abi_version(void);

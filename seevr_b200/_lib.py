@@ -55,6 +55,16 @@ class Params(C.Structure):
                 ("bundle_bodies", C.c_uint32)]
 
 
+BVH_NUM_BINDINGS = 18
+(BVH_VERTICES, BVH_INDICES, BVH_CENTROIDS, BVH_MORTON, BVH_MORTON_TEMP, BVH_SORT_INDICES,
+ BVH_SORT_TEMP, BVH_SCENE_BOUNDS, BVH_NODE_MIN, BVH_NODE_MAX, BVH_LEFT, BVH_RIGHT, BVH_COUNT,
+ BVH_PARENT, BVH_PRIM_INDICES, BVH_FLAGS, BVH_TEMP, BVH_TEMP_U) = range(18)
+
+
+class BvhBindings(C.Structure):
+    _fields_ = [("ptr", C.c_void_p * BVH_NUM_BINDINGS), ("bytes", C.c_uint64 * BVH_NUM_BINDINGS)]
+
+
 class Profile(C.Structure):
     _fields_ = [("ms", C.c_float * NUM_STAGES), ("calls", C.c_uint32)]
 
@@ -88,6 +98,9 @@ def _load():
         "seevr_physics_read_lbvh": (I, [P, U32, UP, UP, FP]),
         "seevr_physics_step_noalloc": (I, [C.POINTER(Bindings), C.POINTER(Params), U32, U32,
                                            U32, U32, U32, U32, F, FP, P]),
+        "seevr_bvh_create": (I, [C.POINTER(BvhBindings), U32, C.POINTER(P)]),
+        "seevr_bvh_build": (I, [P, U32]),
+        "seevr_bvh_destroy": (None, [P]),
         "seevr_status_string": (C.c_char_p, [I]),
         "seevr_last_error": (C.c_char_p, []),
         "seevr_abi_version": (I, []),

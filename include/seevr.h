@@ -281,6 +281,34 @@ uint64_t seevr_physics_kernel_launches(const seevr_physics* h);
 seevr_status seevr_physics_read_lbvh(seevr_physics* h, uint32_t n, uint32_t* morton_sorted,
                                      uint32_t* order, float bounds[6]);
 
+/* ---- adjoint ---------------------------------------------------------------- */
+
+/* Gradient buffers of seevr_physics_adjoint_substep (device, indexed like
+ * the body and geom bindings). */
+typedef struct seevr_adjoint_grads {
+    float* pos;      /* f32[N*3]  in: dL/d state after the substep; out: before */
+    float* quat;     /* f32[N*4] */
+    float* vel;      /* f32[N*3] */
+    float* omega;    /* f32[N*3] */
+    float* friction; /* f32[G]    dL/d geom_friction, accumulated (+=)        */
+} seevr_adjoint_grads;
+
+/* No counterpart in the reference.  Reverse mode of one substep of
+ * Physics.step (gravity, contacts, PGS, integration; physics.comp:418-604)
+ * for gradient-based rollouts: the bound state buffers must hold the state
+ * at the start of the substep (pos, quat, vel, omega, e.g. restored from a
+ * checkpoint); the call recomputes the substep's contacts, recomputes the
+ * PGS sweep in the reference order and back-propagates through it.  On
+ * return `grads` holds dL/d(state before the substep) and dL/d friction has
+ * been accumulated.  The state buffers' velocities are left at their
+ * post-gravity values and the contact outputs are overwritten.  Contact
+ * selection and the solver's clamps follow the branches the forward took.
+ * Synchronous; allocates its work arrays on first use. */
+seevr_status seevr_physics_adjoint_substep(seevr_physics* h, uint32_t num_bodies,
+                                           uint32_t num_hull_verts, float dt,
+                                           const float gravity[3],
+                                           const seevr_adjoint_grads* grads);
+
 /* ---- triangle LBVH (bvh.zig / bvh.comp) ---------------------------------- */
 
 /* Binding indices of BVH.init (bvh.zig:32-51), identical to bvh.comp's

@@ -203,6 +203,38 @@ int oracle_run(const oracle_scene* s, const oracle_params* p, int precision, uin
     return run<float>(s, p, frames, substeps, dt, g, update_verts, threads, o);
 }
 
+// FP64 run of the whole batch (one instance) from a double-precision
+// initial state: pos/quat/vel/omega/friction override the scene's float
+// values (any may be NULL).  Central finite differences of the adjoint
+// tests perturb these inputs by far less than a float ulp.
+int oracle_run_f64_state(const oracle_scene* s, const oracle_params* p, uint32_t frames,
+                         uint32_t substeps, float dt, const float g[3], const double* pos,
+                         const double* quat, const double* vel, const double* omega,
+                         const double* friction, oracle_out* o) {
+    if (!s || !p || !o) return 1;
+    const oracle::SceneIn in = to_in(s);
+    const oracle::Params P = to_params(p);
+    const double gr[3] = {g[0], g[1], g[2]};
+    oracle::Physics<double> ph(in, P);
+    const size_t nb = s->num_bodies;
+    auto put = [](std::vector<double>& dst, const double* src, size_t n) {
+        if (src) std::copy(src, src + n, dst.begin());
+    };
+    put(ph.pos, pos, nb * 3);
+    put(ph.quat, quat, nb * 4);
+    put(ph.vel, vel, nb * 3);
+    put(ph.omega, omega, nb * 3);
+    put(ph.friction, friction, s->num_geoms);
+    for (uint32_t f = 0; f < frames; ++f) ph.step(substeps, double(dt), gr, false);
+    Totals t;
+    o->counters[0] = o->counters[1] = 0;
+    for (auto& x : o->ops) x = 0;
+    emit(ph, 0, 0, P.max_pairs, P.max_contacts, o, &t);
+    o->counters[0] = t.pairs;
+    o->counters[1] = t.contacts;
+    return 0;
+}
+
 // Morton codes (bvh.comp:169-183) of n centroids; bounds[6] = min, max.
 void oracle_morton(const float* centroids, uint32_t n, uint32_t* codes, float* bounds) {
     oracle::morton_codes(centroids, n, codes, bounds);

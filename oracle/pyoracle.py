@@ -64,6 +64,10 @@ def _load():
     lib.oracle_run.argtypes = [C.POINTER(OracleScene), C.POINTER(OracleParams), C.c_int,
                                C.c_uint32, C.c_uint32, C.c_float, _f, C.c_int, C.c_int,
                                C.POINTER(OracleOut)]
+    lib.oracle_run_f64_state.restype = C.c_int
+    lib.oracle_run_f64_state.argtypes = [C.POINTER(OracleScene), C.POINTER(OracleParams),
+                                         C.c_uint32, C.c_uint32, C.c_float, _f, _d, _d, _d, _d,
+                                         _d, C.POINTER(OracleOut)]
     lib.oracle_morton.argtypes = [_f, C.c_uint32, _u, _f]
     lib.oracle_radix_sort.argtypes = [_u, C.c_uint32, _u, _u]
     lib.oracle_karras.argtypes = [_u, C.c_uint32, _u, _u, _u]
@@ -82,34 +86,35 @@ def _p(a, t):
     return a.ctypes.data_as(t) if a is not None else None
 
 
-def run(arrays: dict, *, frames=1, substeps=10, dt=1.0 / 60.0, gravity=(0.0, -9.81, 0.0),
-        pgs_iterations=4, max_pairs=10000, max_contacts=4000, precision=32,
-        update_verts=True, threads=0, use_hull_range=True, **consts) -> dict:
-    """Run `frames` Physics.step calls on a copy of the scene `arrays`
-    (Data.arrays()).  Returns final state and last-substep outputs (float64)."""
-    a = {k: np.ascontiguousarray(v) for k, v in arrays.items()}
+def _scene(a: dict, update_verts: bool, use_hull_range: bool) -> OracleScene:
     nb = len(a["body_inv_mass"])
     ng = len(a["geom_body_idx"])
     nhv = len(a["hull_verts"])
     nv = len(a["orig_vertices"]) if update_verts else 0
     off = a.get("scene_body_offset")
     ns = len(off) - 1 if off is not None and len(off) > 1 else 1
-    s = OracleScene(nb, ng, nhv, nv, ns,
-                    _p(a["body_pos"], _f), _p(a["body_quat"], _f), _p(a["body_vel"], _f),
-                    _p(a["body_omega"], _f), _p(a["body_inv_mass"], _f),
-                    _p(a["body_inv_inertia"], _f), _p(a["body_vert_start"], _u),
-                    _p(a["body_vert_count"], _u), _p(a["geom_body_idx"], _u),
-                    _p(a["geom_data"], _f), _p(a["geom_friction"], _f),
-                    _p(a["geom_restitution"], _f), _p(a["hull_verts"], _f),
-                    _p(a["orig_vertices"], _f) if nv else None,
-                    _p(a["support_offset"], _u), _p(a["support_lookup"], _u),
-                    _p(off, _u) if off is not None and len(off) > 1 else None,
-                    _p(a["hull_range"], _u) if use_hull_range and "hull_range" in a else None)
-    P = OracleParams(pgs_iterations, consts.get("baumgarte", 0.2), consts.get("slop", 0.005),
-                     consts.get("lin_damp", 0.999), consts.get("ang_damp", 0.998),
-                     consts.get("eps", 1e-6), consts.get("tol", 1e-6),
-                     consts.get("mpr_iterations", 50), consts.get("discover_trials", 15),
-                     max_pairs, max_contacts)
+    return OracleScene(nb, ng, nhv, nv, ns,
+                       _p(a["body_pos"], _f), _p(a["body_quat"], _f), _p(a["body_vel"], _f),
+                       _p(a["body_omega"], _f), _p(a["body_inv_mass"], _f),
+                       _p(a["body_inv_inertia"], _f), _p(a["body_vert_start"], _u),
+                       _p(a["body_vert_count"], _u), _p(a["geom_body_idx"], _u),
+                       _p(a["geom_data"], _f), _p(a["geom_friction"], _f),
+                       _p(a["geom_restitution"], _f), _p(a["hull_verts"], _f),
+                       _p(a["orig_vertices"], _f) if nv else None,
+                       _p(a["support_offset"], _u), _p(a["support_lookup"], _u),
+                       _p(off, _u) if off is not None and len(off) > 1 else None,
+                       _p(a["hull_range"], _u) if use_hull_range and "hull_range" in a else None)
+
+
+def _params(pgs_iterations, max_pairs, max_contacts, consts) -> OracleParams:
+    return OracleParams(pgs_iterations, consts.get("baumgarte", 0.2), consts.get("slop", 0.005),
+                        consts.get("lin_damp", 0.999), consts.get("ang_damp", 0.998),
+                        consts.get("eps", 1e-6), consts.get("tol", 1e-6),
+                        consts.get("mpr_iterations", 50), consts.get("discover_trials", 15),
+                        max_pairs, max_contacts)
+
+
+def _outputs(nb: int, nv: int, max_pairs: int, max_contacts: int):
     out = {
         "pos": np.zeros((nb, 3)), "quat": np.zeros((nb, 4)), "vel": np.zeros((nb, 3)),
         "omega": np.zeros((nb, 3)), "aabb_min": np.zeros((nb, 3)), "aabb_max": np.zeros((nb, 3)),
@@ -123,11 +128,10 @@ def run(arrays: dict, *, frames=1, substeps=10, dt=1.0 / 60.0, gravity=(0.0, -9.
                   _p(out["verts"], _d), _p(out["pairs"], _u), _p(out["c_pos"], _d),
                   _p(out["c_normal"], _d), _p(out["c_pen"], _d), _p(out["lambda"], _d),
                   _p(out["c_a"], _u), _p(out["c_b"], _u))
-    g = (C.c_float * 3)(*gravity)
-    rc = lib.oracle_run(C.byref(s), C.byref(P), precision, frames, substeps, dt, g,
-                        1 if nv else 0, threads, C.byref(o))
-    if rc != 0:
-        raise RuntimeError(f"oracle_run failed ({rc})")
+    return out, o
+
+
+def _finish(out: dict, o: OracleOut, nv: int, max_pairs: int, max_contacts: int) -> dict:
     npairs, ncont = int(o.counters[0]), int(o.counters[1])
     out["num_pairs"], out["num_contacts"] = npairs, ncont
     out["pairs"] = out["pairs"][: min(npairs, max_pairs)]
@@ -136,6 +140,47 @@ def run(arrays: dict, *, frames=1, substeps=10, dt=1.0 / 60.0, gravity=(0.0, -9.
     out["verts"] = out["verts"][:nv]
     out["ops"] = dict(zip(OP_NAMES, [int(x) for x in o.ops]))
     return out
+
+
+def run(arrays: dict, *, frames=1, substeps=10, dt=1.0 / 60.0, gravity=(0.0, -9.81, 0.0),
+        pgs_iterations=4, max_pairs=10000, max_contacts=4000, precision=32,
+        update_verts=True, threads=0, use_hull_range=True, **consts) -> dict:
+    """Run `frames` Physics.step calls on a copy of the scene `arrays`
+    (Data.arrays()).  Returns final state and last-substep outputs (float64)."""
+    a = {k: np.ascontiguousarray(v) for k, v in arrays.items()}
+    nb = len(a["body_inv_mass"])
+    nv = len(a["orig_vertices"]) if update_verts else 0
+    s = _scene(a, update_verts, use_hull_range)
+    P = _params(pgs_iterations, max_pairs, max_contacts, consts)
+    out, o = _outputs(nb, nv, max_pairs, max_contacts)
+    g = (C.c_float * 3)(*gravity)
+    rc = lib.oracle_run(C.byref(s), C.byref(P), precision, frames, substeps, dt, g,
+                        1 if nv else 0, threads, C.byref(o))
+    if rc != 0:
+        raise RuntimeError(f"oracle_run failed ({rc})")
+    return _finish(out, o, nv, max_pairs, max_contacts)
+
+
+def run_f64_state(arrays: dict, *, pos=None, quat=None, vel=None, omega=None, friction=None,
+                  frames=1, substeps=10, dt=1.0 / 60.0, gravity=(0.0, -9.81, 0.0),
+                  pgs_iterations=4, max_pairs=10000, max_contacts=4000,
+                  use_hull_range=True, **consts) -> dict:
+    """FP64 run of the whole batch whose initial pos/quat/vel/omega and
+    friction come from float64 arrays (None: the scene's float values), for
+    finite differences finer than a float ulp."""
+    a = {k: np.ascontiguousarray(v) for k, v in arrays.items()}
+    nb = len(a["body_inv_mass"])
+    s = _scene(a, False, use_hull_range)
+    P = _params(pgs_iterations, max_pairs, max_contacts, consts)
+    out, o = _outputs(nb, 0, max_pairs, max_contacts)
+    d = lambda x: None if x is None else np.ascontiguousarray(x, dtype=np.float64)
+    keep = [d(pos), d(quat), d(vel), d(omega), d(friction)]
+    g = (C.c_float * 3)(*gravity)
+    rc = lib.oracle_run_f64_state(C.byref(s), C.byref(P), frames, substeps, dt, g,
+                                  *[_p(x, _d) for x in keep], C.byref(o))
+    if rc != 0:
+        raise RuntimeError(f"oracle_run_f64_state failed ({rc})")
+    return _finish(out, o, 0, max_pairs, max_contacts)
 
 
 def morton(centroids: np.ndarray):

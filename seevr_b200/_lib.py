@@ -69,6 +69,12 @@ class Profile(C.Structure):
     _fields_ = [("ms", C.c_float * NUM_STAGES), ("calls", C.c_uint32)]
 
 
+class AdjointGrads(C.Structure):
+    """seevr_adjoint_grads: device pointers of the gradient buffers."""
+    _fields_ = [("pos", C.c_void_p), ("quat", C.c_void_p), ("vel", C.c_void_p),
+                ("omega", C.c_void_p), ("friction", C.c_void_p)]
+
+
 class SeevrError(RuntimeError):
     def __init__(self, status: int, message: str):
         super().__init__(f"seevr status {status}: {message}")
@@ -96,6 +102,7 @@ def _load():
         "seevr_physics_destroy": (None, [P]),
         "seevr_physics_kernel_launches": (U64, [P]),
         "seevr_physics_read_lbvh": (I, [P, U32, UP, UP, FP]),
+        "seevr_physics_adjoint_substep": (I, [P, U32, U32, F, FP, C.POINTER(AdjointGrads)]),
         "seevr_physics_step_noalloc": (I, [C.POINTER(Bindings), C.POINTER(Params), U32, U32,
                                            U32, U32, U32, U32, F, FP, P]),
         "seevr_bvh_create": (I, [C.POINTER(BvhBindings), U32, C.POINTER(P)]),

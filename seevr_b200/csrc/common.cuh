@@ -122,7 +122,13 @@ int launch_exclusive_scan(const uint32_t* in, uint32_t* out, const uint32_t* n_d
                           uint32_t overflow_bit, const Scratch& s, cudaStream_t st);
 int launch_broadphase_n2(const World& w, const Scratch& s, cudaStream_t st);
 int launch_narrowphase(const World& w, const Consts& k, const Scratch& s, cudaStream_t st);
+// Narrowphase that also tapes the supporting hull vertices of each contact's
+// final portal (2 uint4 per pair / contact) for the adjoint.
+int launch_narrowphase_taped(const World& w, const Consts& k, const Scratch& s, uint4* pair_tape,
+                             uint4* contact_tape, cudaStream_t st);
 cudaError_t init_solver();
+// bundle_c0: the first contact of every solver bundle (one marking pass)
+int launch_bundle_ranges(const World& w, const Scratch& s, cudaStream_t st);
 // Set the calling thread's message returned by seevr_last_error().
 void set_last_error(const char* msg);
 inline void set_last_error(const std::string& msg) { set_last_error(msg.c_str()); }

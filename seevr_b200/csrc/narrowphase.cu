@@ -46,7 +46,7 @@ __device__ __forceinline__ Shape load_shape(const World& w, uint32_t b) {
 // hull vertices when lk == 0 (brute force), else for each of the 3 axes the
 // two lookup bins around the direction's angle.  One loop over candidates
 // serves both, so lanes of a warp holding boxes and spheres share it.
-__device__ __forceinline__ f3 support(const World& w, const Shape& s, f3 d) {
+__device__ __forceinline__ f3 support(const World& w, const Shape& s, f3 d, uint32_t& chosen) {
     const f3 ld = mulT(s.R, d);
     const bool lut = s.lk != 0;
     float a0 = 0.f, a1 = 0.f, a2 = 0.f;
@@ -57,6 +57,7 @@ __device__ __forceinline__ f3 support(const World& w, const Shape& s, f3 d) {
     }
     float best = -1e10f;
     f3 bv = mk(0.f, 0.f, 0.f);
+    chosen = kNone;  // no vertex beat -1e10: the support point is the body position
     const uint32_t n = lut ? 6u : s.vc;
     uint32_t b0 = 0;
     for (uint32_t k = 0; k < n; ++k) {
@@ -76,6 +77,7 @@ __device__ __forceinline__ f3 support(const World& w, const Shape& s, f3 d) {
         if (dd > best) {
             best = dd;
             bv = v;
+            chosen = idx;
         }
     }
     return add(s.p, mul(s.R, bv));
@@ -85,6 +87,7 @@ __device__ __forceinline__ f3 support(const World& w, const Shape& s, f3 d) {
 // (mink_support_pts, physics.comp:165-169)
 struct Mink {
     f3 v, sa, sb;
+    uint32_t ia, ib;  // hull-relative indices of the supporting vertices
 };
 
 __device__ __forceinline__ f3 portal_dir(f3 v1, f3 v2, f3 v3) {
@@ -149,9 +152,15 @@ __device__ __forceinline__ void finish(float4* res0, float4* res1, uint32_t* fla
 
 constexpr uint32_t kNarrowThreads = 128;
 
+// kTape: also record, per pair, which hull vertices support the final
+// portal (tape[2p] = {case, m1.ia, m1.ib, m2.ia}, tape[2p+1] = {m2.ib,
+// m3.ia, m3.ib, 0}; case 1 = penetration portal, 2 = the segment case of
+// physics.comp:267-271), from which the adjoint differentiates the contact.
+template <bool kTape>
 __global__ void __launch_bounds__(kNarrowThreads)
     k_narrow(World w, Consts k, float4* __restrict__ res0, float4* __restrict__ res1,
-             uint32_t* __restrict__ flag, uint32_t* __restrict__ ticket) {
+             uint32_t* __restrict__ flag, uint32_t* __restrict__ ticket,
+             uint4* __restrict__ tape) {
     const uint32_t np = min(w.counters[0], w.max_pairs);
     const uint32_t lane = threadIdx.x & 31u;
     const unsigned full = 0xFFFFFFFFu;
@@ -211,8 +220,8 @@ __global__ void __launch_bounds__(kNarrowThreads)
 
         // ---- the one Minkowski support call of the step ----
         Mink m;
-        m.sa = support(w, A, dir);
-        m.sb = support(w, B, neg(dir));
+        m.sa = support(w, A, dir, m.ia);
+        m.sb = support(w, B, neg(dir), m.ib);
         m.v = sub(m.sa, m.sb);
 
         // ---- postlude ----
@@ -235,6 +244,10 @@ __global__ void __launch_bounds__(kNarrowThreads)
                     } else {
                         depth = length(v1);  // origin on segment v0-v1: res == 2
                         n = normalize(v1);
+                    }
+                    if (kTape) {
+                        tape[size_t(p) * 2] = make_uint4(2u, m1.ia, m1.ib, 0u);
+                        tape[size_t(p) * 2 + 1] = make_uint4(0u, 0u, 0u, 0u);
                     }
                     finish(res0, res1, flag, p, true, scale(0.5f, add(m1.sa, m1.sb)), n, depth);
                     active = false;
@@ -313,6 +326,10 @@ __global__ void __launch_bounds__(kNarrowThreads)
             default: {  // kP
                 if (reach_tol(k, m1.v, m2.v, m3.v, m.v, dir) || iter >= k.mpr_iterations - 1) {
                     const float depth = dot(dir, m1.v);
+                    if (kTape) {
+                        tape[size_t(p) * 2] = make_uint4(1u, m1.ia, m1.ib, m2.ia);
+                        tape[size_t(p) * 2 + 1] = make_uint4(m2.ib, m3.ia, m3.ib, 0u);
+                    }
                     finish(res0, res1, flag, p, true, find_pos(k, v0, A.p, B.p, m1, m2, m3), dir,
                            depth);
                     active = false;
@@ -330,7 +347,9 @@ __global__ void __launch_bounds__(kNarrowThreads)
 __global__ void k_contact_scatter(World w, const float4* __restrict__ res0,
                                   const float4* __restrict__ res1,
                                   const uint32_t* __restrict__ flag,
-                                  const uint32_t* __restrict__ coff) {
+                                  const uint32_t* __restrict__ coff,
+                                  const uint4* __restrict__ pair_tape,
+                                  uint4* __restrict__ contact_tape) {
     const uint32_t np = min(w.counters[0], w.max_pairs);
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < np; p += gridDim.x * blockDim.x) {
         if (!flag[p]) continue;
@@ -342,6 +361,10 @@ __global__ void k_contact_scatter(World w, const float4* __restrict__ res0,
         w.c_pen[c] = r0.w;
         w.c_a[c] = w.pairs[size_t(p) * 2];
         w.c_b[c] = w.pairs[size_t(p) * 2 + 1];
+        if (contact_tape) {
+            contact_tape[size_t(c) * 2] = pair_tape[size_t(p) * 2];
+            contact_tape[size_t(c) * 2 + 1] = pair_tape[size_t(p) * 2 + 1];
+        }
     }
 }
 
@@ -351,19 +374,29 @@ static uint32_t grid_for(uint32_t cap, uint32_t threads, uint32_t max_blocks) {
     return g ? g : 1;
 }
 
-int launch_narrowphase(const World& w, const Consts& k, const Scratch& s, cudaStream_t st) {
+int launch_narrowphase_taped(const World& w, const Consts& k, const Scratch& s, uint4* pair_tape,
+                             uint4* contact_tape, cudaStream_t st) {
     if (w.max_pairs == 0) return 0;
     // persistent grid: a few resident blocks per SM; the pair ticket lives
     // in status[1] and is cleared here
     cudaMemsetAsync(&s.status[1], 0, sizeof(uint32_t), st);
     const uint32_t blocks = grid_for(w.max_pairs, kNarrowThreads, 148 * 4);
-    k_narrow<<<blocks, kNarrowThreads, 0, st>>>(w, k, s.pair_res0, s.pair_res1, s.pair_flag,
-                                                &s.status[1]);
+    if (pair_tape)
+        k_narrow<true><<<blocks, kNarrowThreads, 0, st>>>(w, k, s.pair_res0, s.pair_res1,
+                                                          s.pair_flag, &s.status[1], pair_tape);
+    else
+        k_narrow<false><<<blocks, kNarrowThreads, 0, st>>>(w, k, s.pair_res0, s.pair_res1,
+                                                           s.pair_flag, &s.status[1], nullptr);
     launch_exclusive_scan(s.pair_flag, s.pair_coff, &w.counters[0], w.max_pairs,
                           &w.counters[1], w.max_contacts, kFlagContactOverflow, s, st);
     k_contact_scatter<<<grid_for(w.max_pairs, 256, 148 * 16), 256, 0, st>>>(
-        w, s.pair_res0, s.pair_res1, s.pair_flag, s.pair_coff);
+        w, s.pair_res0, s.pair_res1, s.pair_flag, s.pair_coff, pair_tape,
+        pair_tape ? contact_tape : nullptr);
     return 3;
+}
+
+int launch_narrowphase(const World& w, const Consts& k, const Scratch& s, cudaStream_t st) {
+    return launch_narrowphase_taped(w, k, s, nullptr, nullptr, st);
 }
 
 }  // namespace seevr

@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "../../include/seevr.h"
+#include "adjoint.cuh"
 #include "common.cuh"
 #include "lbvh.cuh"
 
@@ -101,6 +102,9 @@ struct seevr_physics {
     cudaEvent_t ev[2] = {nullptr, nullptr};
     // LBVH broadphase work arrays (broadphase == SEEVR_BROADPHASE_LBVH)
     LbvhScratch lb{};
+    // adjoint work arrays, allocated by the first adjoint call
+    AdjScratch adj{};
+    bool adj_ready = false;
 };
 
 namespace {
@@ -658,6 +662,67 @@ seevr_status seevr_physics_read_lbvh(seevr_physics* h, uint32_t n, uint32_t* mor
         SEEVR_CUDA(cudaMemcpyAsync(order, h->lb.vals_sorted, size_t(n) * 4, cudaMemcpyDeviceToHost, s));
     if (bounds) SEEVR_CUDA(cudaMemcpyAsync(bounds, h->lb.bounds_f, 24, cudaMemcpyDeviceToHost, s));
     SEEVR_CUDA(cudaStreamSynchronize(s));
+    return SEEVR_OK;
+}
+
+seevr_status seevr_physics_adjoint_substep(seevr_physics* h, uint32_t num_bodies,
+                                           uint32_t num_hull_verts, float dt,
+                                           const float gravity[3],
+                                           const seevr_adjoint_grads* grads) {
+    if (!h || !gravity || !grads) return fail(SEEVR_ERR_INVALID_ARGUMENT, "handle, gravity or grads is NULL");
+    if (!grads->pos || !grads->quat || !grads->vel || !grads->omega || !grads->friction)
+        return fail(SEEVR_ERR_INVALID_ARGUMENT, "a gradient buffer is NULL");
+    if (num_bodies == 0) return SEEVR_OK;
+    seevr_status st = check_step_args(h, num_bodies, 0, num_hull_verts);
+    if (st != SEEVR_OK) return st;
+    SEEVR_CUDA(cudaSetDevice(h->device));
+    const cudaStream_t s = h->stream;
+    st = ensure_single_scene(h, num_bodies, s);
+    if (st != SEEVR_OK) return st;
+    AdjScratch& a = h->adj;
+    if (!h->adj_ready) {
+        const size_t nb = h->caps.max_bodies, nc = h->caps.max_contacts, np = h->caps.max_pairs;
+        const size_t iters = h->params.pgs_iterations;
+        st = dev_alloc(h, &a.tape, nc * iters * 13);
+        if (st == SEEVR_OK) st = dev_alloc(h, &a.ptape, np * 2);
+        if (st == SEEVR_OK) st = dev_alloc(h, &a.ctape, nc * 2);
+        if (st == SEEVR_OK) st = dev_alloc(h, &a.vw, nb * 6);
+        if (st == SEEVR_OK) st = dev_alloc(h, &a.gv, nb * 3);
+        if (st == SEEVR_OK) st = dev_alloc(h, &a.gw, nb * 3);
+        if (st == SEEVR_OK) st = dev_alloc(h, &a.gR, nb * 9);
+        if (st == SEEVR_OK) st = dev_alloc(h, &a.gp, nb * 3);
+        if (st == SEEVR_OK) st = dev_alloc(h, &a.gq, nb * 4);
+        if (st == SEEVR_OK) st = dev_alloc(h, &a.gc, nc * 12);
+        if (st == SEEVR_OK) st = dev_alloc(h, &a.glam, nc);
+        if (st == SEEVR_OK) st = dev_alloc(h, &a.lam, nc);
+        if (st == SEEVR_OK) st = dev_alloc(h, &a.par, nc * 12);
+        if (st != SEEVR_OK) return st;
+        h->adj_ready = true;
+    }
+    World& w = h->w;
+    w.nb = num_bodies;
+    w.nv = 0;
+    w.nhv = num_hull_verts;
+    w.ns = h->num_scenes;
+    w.nbundles = h->num_bundles;
+    uint64_t n = 0;
+    if (!h->b.ptr[SEEVR_B_HULL_RANGE])
+        n += launch_hull_range_from_geom_data(static_cast<const float*>(h->b.ptr[SEEVR_B_GEOM_DATA]),
+                                              h->s.derived_hull_range, num_bodies, s);
+    // the substep's forward up to its contacts, in the order of issue_frame
+    n += launch_body_stage(w, h->k, kGravity | kAabb, dt, gravity[0], gravity[1], gravity[2], s);
+    n += h->params.broadphase == SEEVR_BROADPHASE_LBVH ? launch_broadphase_lbvh(w, h->s, h->lb, s)
+                                                       : launch_broadphase_n2(w, h->s, s);
+    n += launch_narrowphase_taped(w, h->k, h->s, a.ptape, a.ctape, s);
+    n += launch_bundle_ranges(w, h->s, s);
+    const Grads g{grads->pos, grads->quat, grads->vel, grads->omega, grads->friction};
+    n += launch_adjoint(w, h->k, h->s, a, g, dt, s);
+    h->launches += n;
+    SEEVR_CUDA(cudaGetLastError());
+    bool overflow = false;
+    st = collect_flags(h, s, &overflow);
+    if (st != SEEVR_OK) return st;
+    if (overflow) return fail(SEEVR_ERR_CAPACITY, "pairs or contacts exceeded the caps");
     return SEEVR_OK;
 }
 

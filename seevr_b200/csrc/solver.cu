@@ -431,12 +431,17 @@ cudaError_t init_solver() {
                                 int(kSolverMaxSmem));
 }
 
-int launch_solver(const World& w, const Consts& k, const Scratch& s, uint32_t mode, float dt,
-                  uint32_t max_scene_bodies, cudaStream_t st) {
-    if (w.nbundles == 0 || w.max_contacts == 0) return 0;
+int launch_bundle_ranges(const World& w, const Scratch& s, cudaStream_t st) {
     uint32_t rb = (w.max_contacts + 1 + 255) / 256;
     if (rb > 148u * 8u) rb = 148u * 8u;
     k_bundle_ranges<<<rb, 256, 0, st>>>(w, s.bundle_c0);
+    return 1;
+}
+
+int launch_solver(const World& w, const Consts& k, const Scratch& s, uint32_t mode, float dt,
+                  uint32_t max_scene_bodies, cudaStream_t st) {
+    if (w.nbundles == 0 || w.max_contacts == 0) return 0;
+    launch_bundle_ranges(w, s, st);
     if (max_scene_bodies <= kWarpMaxBodies) {
         const uint32_t nbmax = max_scene_bodies ? max_scene_bodies : 1u;
         const uint32_t blocks = (w.nbundles + kWarpsPerBlock - 1) / kWarpsPerBlock;

@@ -1,0 +1,165 @@
+"""Reverse mode of the physics step (seevr_physics_adjoint_substep through
+seevr_b200.grad.rollout) against central finite differences of the FP64
+oracle.
+
+The scene is a pile settled by the FP32 oracle, so contacts are present from
+the first substep of the differentiated rollout.  The loss is a fixed random
+linear functional of the final state.  A finite difference is trusted only
+where two step sizes agree (no contact appears, vanishes or switches branch
+within the step); those components must match the adjoint, whose arithmetic
+is float32 along the float32 trajectory, to the tolerance written below.
+"""
+import numpy as np
+import pytest
+
+import pyoracle
+from helpers import DT, G
+from seevr_b200 import Caps, Data, Physics, make_params
+from seevr_b200.grad import rollout
+
+pytestmark = pytest.mark.gpu
+
+PGS = 10
+KEYS = (("pos", 3), ("quat", 4), ("vel", 3), ("omega", 3))
+
+
+def settled(seed, n, frames):
+    d = Data.pile(seed=seed, n_boxes=n // 2, n_spheres=n - n // 2, lo=(-1.5, 0, -1.5),
+                  hi=(1.5, 3, 1.5))
+    assert d.placement_failures == 0
+    a = d.arrays()
+    caps = Caps.for_data(d)
+    r = pyoracle.run(a, frames=frames, substeps=10, dt=DT, gravity=G, pgs_iterations=PGS,
+                     max_pairs=caps.max_pairs, max_contacts=caps.max_contacts,
+                     update_verts=False)
+    st = {k: r[k].astype(np.float32) for k, _ in KEYS}
+    st["friction"] = np.asarray(a["geom_friction"], np.float32).copy()
+    return d, a, caps, st
+
+
+def gpu_grads(d, caps, st, w, cuda, substeps, frames=1):
+    import torch
+
+    buf = d.upload(cuda, caps)
+    ph = Physics(buf, make_params(pgs_iterations=PGS, flags=4))
+    ins = {k: torch.tensor(st[k], device=cuda, requires_grad=True) for k in
+           ("pos", "quat", "vel", "omega", "friction")}
+    out = rollout(ph, ins["pos"], ins["quat"], ins["vel"], ins["omega"], ins["friction"],
+                  frames=frames, substeps=substeps, dt=DT, gravity=G)
+    loss = sum((torch.tensor(w[k], device=cuda, dtype=torch.float32) * o).sum()
+               for (k, _), o in zip(KEYS, out))
+    loss.backward()
+    contacts = ph.read_counters()[1]
+    res = {k: v.grad.detach().cpu().numpy().astype(np.float64) for k, v in ins.items()}
+    fwd = {k: o.detach().cpu().numpy() for (k, _), o in zip(KEYS, out)}
+    ph.deinit()
+    return res, fwd, contacts
+
+
+def fd_grads(a, caps, st, w, substeps, frames=1):
+    base = {k: st[k].astype(np.float64) for k in ("pos", "quat", "vel", "omega", "friction")}
+
+    def loss(x):
+        r = pyoracle.run_f64_state(a, pos=x["pos"], quat=x["quat"], vel=x["vel"],
+                                   omega=x["omega"], friction=x["friction"], frames=frames,
+                                   substeps=substeps, dt=DT, gravity=G, pgs_iterations=PGS,
+                                   max_pairs=caps.max_pairs, max_contacts=caps.max_contacts)
+        return sum(float((w[k] * r[k]).sum()) for k, _ in KEYS)
+
+    fd, smooth = {}, {}
+    for k, x0 in base.items():
+        g = np.zeros(x0.shape)
+        ok = np.zeros(x0.shape, bool)
+        for idx in np.ndindex(x0.shape):
+            est = []
+            for h in (1e-6, 2.5e-7):
+                x = {kk: vv.copy() for kk, vv in base.items()}
+                x[k][idx] += h
+                lp = loss(x)
+                x[k][idx] -= 2 * h
+                lm = loss(x)
+                est.append((lp - lm) / (2 * h))
+            g[idx] = est[0]
+            ok[idx] = abs(est[0] - est[1]) <= 1e-5 * (abs(est[0]) + 1.0)
+        fd[k], smooth[k] = g, ok
+    return fd, smooth
+
+
+def weights(nb, seed):
+    rng = np.random.default_rng(seed)
+    return {k: rng.standard_normal((nb, c)) for k, c in KEYS}
+
+
+@pytest.mark.parametrize("seed", [3, 11])
+def test_adjoint_matches_fp64_finite_differences(cuda, seed):
+    d, a, caps, st = settled(seed, 12, frames=40)
+    nb = d.num_bodies
+    w = weights(nb, seed)
+    substeps = 4
+    ga, _, contacts = gpu_grads(d, caps, st, w, cuda, substeps)
+    assert contacts > 0
+    fd, smooth = fd_grads(a, caps, st, w, substeps)
+    n_all = sum(v.size for v in smooth.values())
+    n_ok = sum(int(v.sum()) for v in smooth.values())
+    assert n_ok >= 0.8 * n_all, (n_ok, n_all)
+    for k in fd:
+        scale = np.abs(fd[k]).max() + 1e-12
+        err = np.abs(ga[k] - fd[k])
+        bad = smooth[k] & (err > 2e-3 * scale + 1e-2 * np.abs(fd[k]))
+        assert not bad.any(), (k, np.argwhere(bad)[:4].tolist(), ga[k][bad][:4], fd[k][bad][:4])
+    # the gradient is not trivially zero where contacts act
+    assert np.abs(ga["friction"]).max() > 0.0
+
+
+def test_rollout_forward_equals_step_and_backward_is_deterministic(cuda):
+    import torch
+
+    d, a, caps, st = settled(5, 12, frames=30)
+    nb = d.num_bodies
+    w = weights(nb, 5)
+    g1, fwd, _ = gpu_grads(d, caps, st, w, cuda, substeps=10, frames=2)
+    g2, _, _ = gpu_grads(d, caps, st, w, cuda, substeps=10, frames=2)
+    for k in g1:
+        assert np.array_equal(g1[k], g2[k]), k
+    # the substep-by-substep forward is the regular 10-substep frame, bit for bit
+    buf = d.upload(cuda, caps)
+    for k, c in KEYS:
+        buf.tensors["body_" + k][: nb * c].copy_(torch.tensor(st[k].reshape(-1)))
+    buf.tensors["geom_friction"][:nb].copy_(torch.tensor(st["friction"]))
+    ph = Physics(buf, make_params(pgs_iterations=PGS, flags=4))
+    for _ in range(2):
+        ph.step(nb, 0, buf.num_hull_verts, 10, DT, G)
+    torch.cuda.synchronize()
+    for k, c in KEYS:
+        ref = buf.tensors["body_" + k][: nb * c].cpu().numpy().reshape(nb, c)
+        assert np.array_equal(fwd[k], ref), k
+    ph.deinit()
+
+
+def test_free_flight_gradient_is_analytic(cuda):
+    """One body far from everything: vel_T = d^S v0 + g dt sum d^i,
+    pos_T = pos0 + dt sum_s vel_s, so dL/dv0 = d^S w_v + dt sum_s d^s w_p."""
+    import torch
+
+    d = Data.pile(seed=0, n_boxes=1, n_spheres=0, lo=(-1, 5, -1), hi=(1, 6, 1))
+    nb = d.num_bodies
+    caps = Caps.for_data(d)
+    buf = d.upload(cuda, caps)
+    ph = Physics(buf, make_params(pgs_iterations=4, flags=4))
+    st = {k: buf.tensors["body_" + k][: nb * c].clone().reshape(nb, c) for k, c in KEYS}
+    v0 = st["vel"].clone().requires_grad_()
+    S = 10
+    pos, quat, vel, omega = rollout(ph, st["pos"], st["quat"], v0, st["omega"], frames=1,
+                                    substeps=S, dt=DT, gravity=G)
+    wp = torch.zeros_like(pos)
+    wv = torch.zeros_like(vel)
+    wp[nb - 1] = torch.tensor([0.3, -0.7, 1.1], device=cuda)
+    wv[nb - 1] = torch.tensor([0.5, 0.25, -2.0], device=cuda)
+    ((wp * pos).sum() + (wv * vel).sum()).backward()
+    dmp = 0.999
+    sub = float(np.float32(np.float32(DT) / np.float32(S)))
+    expect = dmp ** S * wv[nb - 1].double().cpu().numpy() + \
+        sub * sum(dmp ** s for s in range(1, S + 1)) * wp[nb - 1].double().cpu().numpy()
+    got = v0.grad[nb - 1].double().cpu().numpy()
+    np.testing.assert_allclose(got, expect, rtol=1e-5, atol=1e-6)
+    ph.deinit()

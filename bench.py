@@ -50,6 +50,10 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--adjoint-scenes", type=int, default=1024)
+    ap.add_argument("--adjoint-bodies", type=int, default=64)
+    ap.add_argument("--adjoint-frames", type=int, default=60)
+    ap.add_argument("--no-adjoint", action="store_true")
     return ap.parse_args()
 
 
@@ -317,6 +321,8 @@ def ours(a, rank, world, local_rank):
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         cpu = cpu_baseline(a, d, pre_state)
 
+    adj = None if a.no_adjoint else adjoint_leg(a, rank, world, dev)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
@@ -331,12 +337,87 @@ def ours(a, rank, world, local_rank):
             "roofline": roof,
             "cpu_baseline": cpu,
             "plain": plain,
+            "adjoint": adj,
             "stage_ms_per_frame": stage_ms,
             "last_substep": {"pairs": pairs, "contacts": contacts},
         }
         print(json.dumps(line))
     ph.deinit()
     return 0
+
+
+def adjoint_leg(a, rank, world, dev):
+    """Differentiable rollout: --adjoint-scenes scenes of --adjoint-bodies
+    bodies (half boxes, half spheres, v and omega N(0,1), friction
+    U(0.2,0.8)), --adjoint-frames frames of 10 substeps x 30 PGS iterations.
+    Loss: sum over scenes of the squared distance of the scene's first
+    dynamic body's final position to a target drawn in a 2 m cube.  One
+    forward + backward yields every scene's gradient with respect to its
+    initial velocities, angular velocities and friction coefficients."""
+    import torch
+    import torch.distributed as dist
+
+    from seevr_b200 import Caps, Data, Physics, make_params
+    from seevr_b200.grad import rollout
+
+    d = Data.rollout(num_scenes=a.adjoint_scenes, bodies=a.adjoint_bodies, segments=a.segments,
+                     seed_base=(1 << 32) + rank * a.adjoint_scenes)
+    nb = d.num_bodies
+    caps = Caps.for_data(d, pairs_per_body=8.0, contacts_per_body=4.0)
+    buf = d.upload(dev, caps)
+    ph = Physics(buf, make_params(pgs_iterations=a.pgs, flags=4,
+                                  bundle_bodies=a.adjoint_bodies + 1))
+    off = d.scene_body_offset()
+    first = torch.tensor(off[:-1].astype(np.int64) + 1, device=dev)  # body 0 is the ground
+    rng = np.random.default_rng(7 + rank)
+    target = torch.tensor(rng.uniform(-1.0, 1.0, (a.adjoint_scenes, 3)) + [0.0, 1.0, 0.0],
+                          dtype=torch.float32, device=dev)
+    t = buf.tensors
+    init = {k: t[n][: nb * c].clone().reshape(nb, c) for k, n, c in (
+        ("pos", "body_pos", 3), ("quat", "body_quat", 4), ("vel", "body_vel", 3),
+        ("omega", "body_omega", 3))}
+    fr0 = t["geom_friction"][:nb].clone()
+
+    def one(frames):
+        v0 = init["vel"].clone().requires_grad_()
+        w0 = init["omega"].clone().requires_grad_()
+        mu = fr0.clone().requires_grad_()
+        pos, _, _, _ = rollout(ph, init["pos"], init["quat"], v0, w0, mu, frames=frames,
+                               substeps=a.substeps, dt=DT, gravity=G)
+        loss = ((pos[first] - target) ** 2).sum()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        loss.backward()
+        torch.cuda.synchronize()
+        return t1, v0.grad, w0.grad, mu.grad
+
+    one(1)  # warm-up: work arrays, first-call paths
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    e0.record()
+    t1, gv, gw, gmu = one(a.adjoint_frames)
+    e1.record()
+    e1.synchronize()
+    fwd_s, bwd_s = t1 - t0, time.perf_counter() - t1
+    ms = e0.elapsed_time(e1)
+    tt = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    total = a.adjoint_scenes * world
+    finite = bool(torch.isfinite(gv).all() and torch.isfinite(gw).all() and
+                  torch.isfinite(gmu).all())
+    ph.deinit()
+    return {
+        "value": total / (float(tt.item()) / 1e3), "unit": "scene-gradients/s",
+        "scenes": total, "bodies_per_scene": a.adjoint_bodies + 1,
+        "frames": a.adjoint_frames, "substeps": a.substeps, "pgs_iterations": a.pgs,
+        "forward_s": fwd_s, "backward_s": bwd_s, "grads_finite": finite,
+        "wrt": "initial velocities, angular velocities, friction",
+        "timing": "CUDA events around one forward + backward, max over ranks",
+    }
 
 
 def plain_dropin(a, d, pre_state, dev):

@@ -1,14 +1,21 @@
-// body.cu — per-body stages of physics.comp, fused into one warp-per-body
-// kernel:  integrate (step 6, physics.comp:586-604) of the previous substep,
-// gravity + damping (step 0, 418-428), the world AABB of the body's hull
-// (steps 9-11, 686-844) and the render-vertex update (step 7, 607-627).
+// body.cu — per-body stages of physics.comp fused into one kernel:
+// integrate (step 6, physics.comp:586-604) of the previous substep, gravity +
+// damping (step 0, 418-428), the world AABB of the body's hull (steps 9-11,
+// 686-844) and the render-vertex update (step 7, 607-627).
+//
+// The stage streams every hull vertex once per substep (12 bytes each, the
+// bulk of its HBM traffic).  A block takes 256 consecutive bodies: each
+// thread updates its body's state with coalesced loads and handles a small
+// hull itself; bodies whose hull or render mesh has more than 32 vertices go
+// to a per-block queue that the block's warps then drain, lanes striding
+// over the vertices, so no warp waits on a single lane's state update.
 //
 // The reference reduces AABBs with a thread-0 serial loop per 256-vertex
 // workgroup and a multi-launch cascade; min/max are exact in any order, so
-// a warp-shuffle reduction over the body's contiguous hull range gives the
-// same values in one pass.  Hull vertex ownership: body b owns
-// [hull_start, hull_start+hull_count), which is what the reference's binary
-// search (physics.comp:695-703) yields for contiguous hull ranges.
+// the reductions here give the same values in one pass.  Hull vertex
+// ownership: body b owns [hull_start, hull_start+hull_count), which is what
+// the reference's binary search (physics.comp:695-703) yields for
+// contiguous hull ranges.
 #include "common.cuh"
 
 namespace seevr {
@@ -29,116 +36,185 @@ int launch_hull_range_from_geom_data(const float* geom_data, uint32_t* out, uint
     return 1;
 }
 
-__global__ void __launch_bounds__(256) k_body_stage(World w, Consts k, uint32_t flags, float dt,
-                                                    float gx, float gy, float gz) {
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (b >= w.nb) return;
+constexpr uint32_t kBodyThreads = 256;
+// Hulls (and render meshes) up to this many vertices are transformed by the
+// body's own thread; larger ones by a warp in the block's second phase.
+constexpr uint32_t kSmallVerts = 32;
 
-    float px = 0, py = 0, pz = 0, qx = 0, qy = 0, qz = 0, qw = 1;
-    if (lane == 0) {
-        px = w.pos[size_t(b) * 3];
-        py = w.pos[size_t(b) * 3 + 1];
-        pz = w.pos[size_t(b) * 3 + 2];
-        qx = w.quat[size_t(b) * 4];
-        qy = w.quat[size_t(b) * 4 + 1];
-        qz = w.quat[size_t(b) * 4 + 2];
-        qw = w.quat[size_t(b) * 4 + 3];
-        const float im = w.inv_mass[b];
-        if ((flags & (kIntegrate | kGravity)) && im > 0.0f) {
-            float vx = w.vel[size_t(b) * 3], vy = w.vel[size_t(b) * 3 + 1],
-                  vz = w.vel[size_t(b) * 3 + 2];
-            float ox = w.omega[size_t(b) * 3], oy = w.omega[size_t(b) * 3 + 1],
-                  oz = w.omega[size_t(b) * 3 + 2];
-            if (flags & kIntegrate) {  // step 6 of the previous substep
-                px += vx * dt;
-                py += vy * dt;
-                pz += vz * dt;
-                const float dx = ox * qw + oy * qz - oz * qy;
-                const float dy = -ox * qz + oy * qw + oz * qx;
-                const float dz = ox * qy - oy * qx + oz * qw;
-                const float dw = -ox * qx - oy * qy - oz * qz;
-                qx += 0.5f * dx * dt;
-                qy += 0.5f * dy * dt;
-                qz += 0.5f * dz * dt;
-                qw += 0.5f * dw * dt;
-                const float l = sqrtf(qx * qx + qy * qy + qz * qz + qw * qw);
-                if (l > 1e-8f) {
-                    qx /= l;
-                    qy /= l;
-                    qz /= l;
-                    qw /= l;
-                }
-                w.pos[size_t(b) * 3] = px;
-                w.pos[size_t(b) * 3 + 1] = py;
-                w.pos[size_t(b) * 3 + 2] = pz;
-                w.quat[size_t(b) * 4] = qx;
-                w.quat[size_t(b) * 4 + 1] = qy;
-                w.quat[size_t(b) * 4 + 2] = qz;
-                w.quat[size_t(b) * 4 + 3] = qw;
+// Integrate (physics.comp:586-604) and gravity (418-428) of body b, in the
+// reference's arithmetic; returns the (possibly updated) pose.
+__device__ __forceinline__ void body_state(const World& w, const Consts& k, uint32_t flags,
+                                           uint32_t b, float dt, float gx, float gy, float gz,
+                                           f3& p, float (&q)[4]) {
+    float px = w.pos[size_t(b) * 3], py = w.pos[size_t(b) * 3 + 1], pz = w.pos[size_t(b) * 3 + 2];
+    float qx = w.quat[size_t(b) * 4], qy = w.quat[size_t(b) * 4 + 1],
+          qz = w.quat[size_t(b) * 4 + 2], qw = w.quat[size_t(b) * 4 + 3];
+    const float im = w.inv_mass[b];
+    if ((flags & (kIntegrate | kGravity)) && im > 0.0f) {
+        float vx = w.vel[size_t(b) * 3], vy = w.vel[size_t(b) * 3 + 1], vz = w.vel[size_t(b) * 3 + 2];
+        const float ox = w.omega[size_t(b) * 3], oy = w.omega[size_t(b) * 3 + 1],
+                    oz = w.omega[size_t(b) * 3 + 2];
+        if (flags & kIntegrate) {  // step 6 of the previous substep
+            px += vx * dt;
+            py += vy * dt;
+            pz += vz * dt;
+            const float dx = ox * qw + oy * qz - oz * qy;
+            const float dy = -ox * qz + oy * qw + oz * qx;
+            const float dz = ox * qy - oy * qx + oz * qw;
+            const float dw = -ox * qx - oy * qy - oz * qz;
+            qx += 0.5f * dx * dt;
+            qy += 0.5f * dy * dt;
+            qz += 0.5f * dz * dt;
+            qw += 0.5f * dw * dt;
+            const float l = sqrtf(qx * qx + qy * qy + qz * qz + qw * qw);
+            if (l > 1e-8f) {
+                qx /= l;
+                qy /= l;
+                qz /= l;
+                qw /= l;
             }
-            if (flags & kGravity) {  // step 0 of this substep
-                vx = vx * k.lin_damp + gx * dt;
-                vy = vy * k.lin_damp + gy * dt;
-                vz = vz * k.lin_damp + gz * dt;
-                w.vel[size_t(b) * 3] = vx;
-                w.vel[size_t(b) * 3 + 1] = vy;
-                w.vel[size_t(b) * 3 + 2] = vz;
-                w.omega[size_t(b) * 3] = ox * k.ang_damp;
-                w.omega[size_t(b) * 3 + 1] = oy * k.ang_damp;
-                w.omega[size_t(b) * 3 + 2] = oz * k.ang_damp;
-            }
+            w.pos[size_t(b) * 3] = px;
+            w.pos[size_t(b) * 3 + 1] = py;
+            w.pos[size_t(b) * 3 + 2] = pz;
+            w.quat[size_t(b) * 4] = qx;
+            w.quat[size_t(b) * 4 + 1] = qy;
+            w.quat[size_t(b) * 4 + 2] = qz;
+            w.quat[size_t(b) * 4 + 3] = qw;
+        }
+        if (flags & kGravity) {  // step 0 of this substep
+            vx = vx * k.lin_damp + gx * dt;
+            vy = vy * k.lin_damp + gy * dt;
+            vz = vz * k.lin_damp + gz * dt;
+            w.vel[size_t(b) * 3] = vx;
+            w.vel[size_t(b) * 3 + 1] = vy;
+            w.vel[size_t(b) * 3 + 2] = vz;
+            w.omega[size_t(b) * 3] = ox * k.ang_damp;
+            w.omega[size_t(b) * 3 + 1] = oy * k.ang_damp;
+            w.omega[size_t(b) * 3 + 2] = oz * k.ang_damp;
         }
     }
-    if (!(flags & (kAabb | kRenderVerts))) return;
+    p = mk(px, py, pz);
+    q[0] = qx;
+    q[1] = qy;
+    q[2] = qz;
+    q[3] = qw;
+}
+
+// Phase 1, one thread per body: state update, then the AABB and render
+// vertices of small meshes in vertex order.  Bodies with a large hull or
+// render mesh are queued in shared memory with their pose; phase 2 gives
+// each a warp whose lanes stride over the vertices and reduce with shuffles
+// (min/max are exact in any order).
+__global__ void __launch_bounds__(kBodyThreads) k_body_stage(World w, Consts k, uint32_t flags,
+                                                             float dt, float gx, float gy,
+                                                             float gz) {
+    __shared__ float sh_pose[kBodyThreads][12];  // p xyz, R by columns
+    __shared__ uint32_t sh_body[kBodyThreads];
+    __shared__ uint32_t sh_n;
+    if (threadIdx.x == 0) sh_n = 0;
+    __syncthreads();
+
+    const uint32_t b = blockIdx.x * kBodyThreads + threadIdx.x;
+    const float inf = __int_as_float(0x7f800000);
+    if (b < w.nb) {
+        uint32_t hs = 0, hc = 0, vs = 0, ve = 0;
+        if (flags & kAabb) {
+            hs = w.hull_range[size_t(b) * 2];
+            hc = w.hull_range[size_t(b) * 2 + 1];
+        }
+        if (flags & kRenderVerts) {
+            vs = w.vert_start[b];
+            ve = vs + w.vert_count[b];
+            if (ve > w.nv) ve = w.nv;
+            if (ve < vs) ve = vs;
+        }
+        f3 p;
+        float q[4];
+        body_state(w, k, flags, b, dt, gx, gy, gz, p, q);
+        const m3 R = quat_to_mat(q[0], q[1], q[2], q[3]);
+        const bool big = hc > kSmallVerts || ve - vs > kSmallVerts;
+        if ((flags & kAabb) && hc <= kSmallVerts) {
+            f3 mn = mk(inf, inf, inf), mx = mk(-inf, -inf, -inf);
+#pragma unroll 8
+            for (uint32_t i = 0; i < hc; ++i) {
+                const f3 wv = add(p, mul(R, ld3(w.hull, hs + i)));
+                mn = vmin(mn, wv);
+                mx = vmax(mx, wv);
+            }
+            if (hc > 0) {
+                st3(w.aabb_min, b, mn);
+                st3(w.aabb_max, b, mx);
+            }
+        }
+        if ((flags & kRenderVerts) && ve - vs <= kSmallVerts) {
+#pragma unroll 4
+            for (uint32_t i = vs; i < ve; ++i) st3(w.verts, i, add(p, mul(R, ld3(w.orig, i))));
+        }
+        if (big) {
+            const uint32_t e = atomicAdd(&sh_n, 1u);
+            sh_body[e] = b;
+            float* o = sh_pose[e];
+            o[0] = p.x; o[1] = p.y; o[2] = p.z;
+            o[3] = R.c0.x; o[4] = R.c0.y; o[5] = R.c0.z;
+            o[6] = R.c1.x; o[7] = R.c1.y; o[8] = R.c1.z;
+            o[9] = R.c2.x; o[10] = R.c2.y; o[11] = R.c2.z;
+        }
+    }
+    __syncthreads();
+
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const unsigned full = 0xFFFFFFFFu;
-    px = __shfl_sync(full, px, 0);
-    py = __shfl_sync(full, py, 0);
-    pz = __shfl_sync(full, pz, 0);
-    qx = __shfl_sync(full, qx, 0);
-    qy = __shfl_sync(full, qy, 0);
-    qz = __shfl_sync(full, qz, 0);
-    qw = __shfl_sync(full, qw, 0);
-    const m3 R = quat_to_mat(qx, qy, qz, qw);
-    const f3 p = mk(px, py, pz);
-
-    if (flags & kAabb) {
-        const uint32_t hs = w.hull_range[size_t(b) * 2], hc = w.hull_range[size_t(b) * 2 + 1];
-        const float inf = __int_as_float(0x7f800000);
-        f3 mn = mk(inf, inf, inf), mx = mk(-inf, -inf, -inf);
-        for (uint32_t i = lane; i < hc; i += 32) {
-            const f3 wv = add(p, mul(R, ld3(w.hull, hs + i)));
-            mn = vmin(mn, wv);
-            mx = vmax(mx, wv);
-        }
+    for (uint32_t e = warp; e < sh_n; e += kBodyThreads / 32) {
+        const uint32_t bb = sh_body[e];
+        const float* o = sh_pose[e];
+        const f3 p = mk(o[0], o[1], o[2]);
+        m3 R;
+        R.c0 = mk(o[3], o[4], o[5]);
+        R.c1 = mk(o[6], o[7], o[8]);
+        R.c2 = mk(o[9], o[10], o[11]);
+        if (flags & kAabb) {
+            const uint32_t hs = w.hull_range[size_t(bb) * 2], hc = w.hull_range[size_t(bb) * 2 + 1];
+            if (hc > kSmallVerts) {
+                f3 mn = mk(inf, inf, inf), mx = mk(-inf, -inf, -inf);
+#pragma unroll 4
+                for (uint32_t i = lane; i < hc; i += 32) {
+                    const f3 wv = add(p, mul(R, ld3(w.hull, hs + i)));
+                    mn = vmin(mn, wv);
+                    mx = vmax(mx, wv);
+                }
 #pragma unroll
-        for (int off = 16; off > 0; off >>= 1) {
-            mn.x = gmin(mn.x, __shfl_xor_sync(full, mn.x, off));
-            mn.y = gmin(mn.y, __shfl_xor_sync(full, mn.y, off));
-            mn.z = gmin(mn.z, __shfl_xor_sync(full, mn.z, off));
-            mx.x = gmax(mx.x, __shfl_xor_sync(full, mx.x, off));
-            mx.y = gmax(mx.y, __shfl_xor_sync(full, mx.y, off));
-            mx.z = gmax(mx.z, __shfl_xor_sync(full, mx.z, off));
+                for (int off = 16; off > 0; off >>= 1) {
+                    mn.x = gmin(mn.x, __shfl_xor_sync(full, mn.x, off));
+                    mn.y = gmin(mn.y, __shfl_xor_sync(full, mn.y, off));
+                    mn.z = gmin(mn.z, __shfl_xor_sync(full, mn.z, off));
+                    mx.x = gmax(mx.x, __shfl_xor_sync(full, mx.x, off));
+                    mx.y = gmax(mx.y, __shfl_xor_sync(full, mx.y, off));
+                    mx.z = gmax(mx.z, __shfl_xor_sync(full, mx.z, off));
+                }
+                if (lane == 0) {
+                    st3(w.aabb_min, bb, mn);
+                    st3(w.aabb_max, bb, mx);
+                }
+            }
         }
-        if (lane == 0 && hc > 0) {
-            st3(w.aabb_min, b, mn);
-            st3(w.aabb_max, b, mx);
+        if (flags & kRenderVerts) {
+            const uint32_t vs = w.vert_start[bb];
+            uint32_t ve = vs + w.vert_count[bb];
+            if (ve > w.nv) ve = w.nv;
+            if (ve > vs && ve - vs > kSmallVerts) {
+#pragma unroll 4
+                for (uint32_t i = vs + lane; i < ve; i += 32)
+                    st3(w.verts, i, add(p, mul(R, ld3(w.orig, i))));
+            }
         }
-    }
-    if (flags & kRenderVerts) {
-        const uint32_t vs = w.vert_start[b];
-        uint32_t ve = vs + w.vert_count[b];
-        if (ve > w.nv) ve = w.nv;
-        for (uint32_t i = vs + lane; i < ve; i += 32) st3(w.verts, i, add(p, mul(R, ld3(w.orig, i))));
     }
 }
 
 int launch_body_stage(const World& w, const Consts& k, uint32_t flags, float dt, float gx,
                       float gy, float gz, cudaStream_t st) {
     if (w.nb == 0) return 0;
-    const uint32_t threads = 256;
-    const uint64_t blocks = (uint64_t(w.nb) * 32 + threads - 1) / threads;
-    k_body_stage<<<uint32_t(blocks), threads, 0, st>>>(w, k, flags, dt, gx, gy, gz);
+    const uint32_t blocks = (w.nb + kBodyThreads - 1) / kBodyThreads;
+    k_body_stage<<<blocks, kBodyThreads, 0, st>>>(w, k, flags, dt, gx, gy, gz);
     return 1;
 }
 

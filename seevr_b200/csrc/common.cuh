@@ -99,6 +99,10 @@ struct Scratch {
     float* s_R;             // [max_bodies*9]
     uint32_t* s_last;       // [max_bodies]
     uint32_t* derived_hull_range;  // [max_bodies*2]
+    // all-pairs broadphase: per row, the 32-column overlap words of the
+    // count pass (NULL: the write pass re-tests)
+    uint32_t* bp_mask;      // [rows * bp_stride]
+    uint32_t bp_stride;     // words per row
 };
 
 // ---- launchers (one translation unit each) ------------------------------

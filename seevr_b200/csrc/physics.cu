@@ -105,6 +105,8 @@ struct seevr_physics {
     // adjoint work arrays, allocated by the first adjoint call
     AdjScratch adj{};
     bool adj_ready = false;
+    // broadphase overlap words (s.bp_mask), sized for the scene layout
+    size_t bp_mask_cap = 0;
 };
 
 namespace {
@@ -124,6 +126,8 @@ seevr_status dev_alloc(seevr_physics* h, T** p, size_t count) {
 
 void free_all(seevr_physics* h) {
     if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+    if (h->s.bp_mask) cudaFree(h->s.bp_mask);
+    h->s.bp_mask = nullptr;
     for (void* p : h->allocations) cudaFree(p);
     h->allocations.clear();
     for (auto& e : h->ev)
@@ -317,8 +321,39 @@ seevr_status check_step_args(seevr_physics* h, uint32_t nb, uint32_t nv, uint32_
     return SEEVR_OK;
 }
 
+// Overlap-word rows of the all-pairs broadphase for nb bodies in scenes of
+// at most maxs bodies: one 32-bit word per 32 columns of the longest row.
+// Layouts needing more than 1 GiB go without (the write pass re-tests).
+seevr_status ensure_bp_mask(seevr_physics* h, uint32_t nb, uint32_t maxs) {
+    const uint32_t stride = maxs > 1 ? (maxs - 1 + 31) / 32 : 1u;
+    const size_t words = size_t(nb ? nb : 1) * stride;
+    if (words * sizeof(uint32_t) > (size_t(1) << 30)) {
+        if (h->s.bp_mask) cudaFree(h->s.bp_mask);
+        h->s.bp_mask = nullptr;
+        h->s.bp_stride = 0;
+        h->bp_mask_cap = 0;
+        return SEEVR_OK;
+    }
+    if (words > h->bp_mask_cap) {
+        if (h->s.bp_mask) cudaFree(h->s.bp_mask);
+        h->s.bp_mask = nullptr;
+        h->bp_mask_cap = 0;
+        void* q = nullptr;
+        if (cudaMalloc(&q, words * sizeof(uint32_t)) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(SEEVR_ERR_OUT_OF_MEMORY, "cudaMalloc of the broadphase overlap words failed");
+        }
+        h->s.bp_mask = static_cast<uint32_t*>(q);
+        h->bp_mask_cap = words;
+    }
+    h->s.bp_stride = stride;
+    return SEEVR_OK;
+}
+
 seevr_status ensure_single_scene(seevr_physics* h, uint32_t nb, cudaStream_t st) {
     if (h->scenes_set || h->single_scene_nb == nb) return SEEVR_OK;
+    const seevr_status ms = ensure_bp_mask(h, nb, nb);
+    if (ms != SEEVR_OK) return ms;
     const uint32_t n = nb > 0 ? nb : 1;
     k_single_scene<<<(n + 255) / 256, 256, 0, st>>>(h->body_scene, h->body_bundle, h->scene_off,
                                                      h->bundle_off, nb);
@@ -505,6 +540,8 @@ seevr_status seevr_physics_set_scenes(seevr_physics* h, const uint32_t* body_off
         return fail(SEEVR_ERR_NOT_SUPPORTED,
                     "the LBVH broadphase steps a single scene; use the all-pairs broadphase for "
                     "batches");
+    const seevr_status ms = ensure_bp_mask(h, nb, maxs);
+    if (ms != SEEVR_OK) return ms;
     uint32_t max_bundle = 0;
     const uint32_t target = h->params.bundle_bodies ? h->params.bundle_bodies : 512u;
     const std::vector<uint32_t> bundles = make_bundles(body_offset, num_scenes, target, &max_bundle);

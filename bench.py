@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--adjoint-frames", type=int, default=60)
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--prof-frames", type=int, default=3)
+    ap.add_argument("--bundle-bodies", type=int, default=0,
+                    help="solver bundle size in bodies (0: the library default)")
     return ap.parse_args()
 
 
@@ -235,7 +237,7 @@ def ours(a, rank, world, local_rank):
     nb, nhv, nv, ndyn = d.num_bodies, d.num_hull_verts, d.num_vertices, d.num_dynamic
     caps = Caps.for_data(d, pairs_per_body=8.0, contacts_per_body=4.0)
     buf = d.upload(dev, caps)
-    ph = Physics(buf, make_params(pgs_iterations=a.pgs, flags=FLAG_CUDA_GRAPH))
+    ph = Physics(buf, make_params(pgs_iterations=a.pgs, flags=FLAG_CUDA_GRAPH, bundle_bodies=a.bundle_bodies))
     stream = torch.cuda.Stream(dev)
 
     def frames(n):
@@ -279,7 +281,7 @@ def ours(a, rank, world, local_rank):
     counters = ph.read_counters()
 
     # ---- per-stage device times of one frame (profiling mode)
-    ph_prof = Physics(buf, make_params(pgs_iterations=a.pgs))
+    ph_prof = Physics(buf, make_params(pgs_iterations=a.pgs, bundle_bodies=a.bundle_bodies))
     prof = Profile()
     for _ in range(a.prof_frames):
         ph_prof.step(nb, nv, nhv, a.substeps, DT, G, prof)
@@ -290,7 +292,7 @@ def ours(a, rank, world, local_rank):
     # ---- e2e: host state in pinned memory -> device, frame, device -> host
     host = {k: torch.from_numpy(np.ascontiguousarray(v, dtype=np.float32)).pin_memory()
             for k, v in pre_state.items()}
-    ph_e2e = Physics(buf, make_params(pgs_iterations=a.pgs, flags=FLAG_CUDA_GRAPH))
+    ph_e2e = Physics(buf, make_params(pgs_iterations=a.pgs, flags=FLAG_CUDA_GRAPH, bundle_bodies=a.bundle_bodies))
     h2d = d2h = nb * (12 + 16 + 12 + 12)
     ph_e2e.upload_state(nb, host["pos"], host["quat"], host["vel"], host["omega"])
     ph_e2e.step_async(nb, nv, nhv, a.substeps, DT, G, frames=1)  # capture

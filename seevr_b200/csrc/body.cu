@@ -40,6 +40,8 @@ constexpr uint32_t kBodyThreads = 256;
 // Hulls (and render meshes) up to this many vertices are transformed by the
 // body's own thread; larger ones by a warp in the block's second phase.
 constexpr uint32_t kSmallVerts = 32;
+// Vertices per lane per round of loads in the warp phase.
+constexpr uint32_t kLaneVerts = 10;
 
 // Integrate (physics.comp:586-604) and gravity (418-428) of body b, in the
 // reference's arithmetic; returns the (possibly updated) pose.
@@ -176,11 +178,26 @@ __global__ void __launch_bounds__(kBodyThreads) k_body_stage(World w, Consts k, 
             const uint32_t hs = w.hull_range[size_t(bb) * 2], hc = w.hull_range[size_t(bb) * 2 + 1];
             if (hc > kSmallVerts) {
                 f3 mn = mk(inf, inf, inf), mx = mk(-inf, -inf, -inf);
-#pragma unroll 4
-                for (uint32_t i = lane; i < hc; i += 32) {
-                    const f3 wv = add(p, mul(R, ld3(w.hull, hs + i)));
-                    mn = vmin(mn, wv);
-                    mx = vmax(mx, wv);
+                // all loads of a chunk (kLaneVerts per lane) in flight at once:
+                // a 16-segment sphere (289 vertices) is one memory latency
+                for (uint32_t c0 = 0; c0 < hc; c0 += 32u * kLaneVerts) {
+                    f3 v[kLaneVerts];
+#pragma unroll
+                    for (uint32_t j = 0; j < kLaneVerts; ++j) {
+                        const uint32_t i = c0 + lane + 32u * j;
+                        if (i < hc) {
+                            const float* q = w.hull + size_t(hs + i) * 3;
+                            v[j] = mk(__ldg(q), __ldg(q + 1), __ldg(q + 2));
+                        }
+                    }
+#pragma unroll
+                    for (uint32_t j = 0; j < kLaneVerts; ++j) {
+                        if (c0 + lane + 32u * j < hc) {
+                            const f3 wv = add(p, mul(R, v[j]));
+                            mn = vmin(mn, wv);
+                            mx = vmax(mx, wv);
+                        }
+                    }
                 }
 #pragma unroll
                 for (int off = 16; off > 0; off >>= 1) {

@@ -136,7 +136,9 @@ int launch_bundle_ranges(const World& w, const Scratch& s, cudaStream_t st);
 // Set the calling thread's message returned by seevr_last_error().
 void set_last_error(const char* msg);
 inline void set_last_error(const std::string& msg) { set_last_error(msg.c_str()); }
+// max_scene_bodies: the largest bundle; smem_bodies: bodies per bundle kept
+// in shared memory by the warp solver (larger bundles solve in place)
 int launch_solver(const World& w, const Consts& k, const Scratch& s, uint32_t mode,
-                  float dt, uint32_t max_scene_bodies, cudaStream_t st);
+                  float dt, uint32_t max_scene_bodies, uint32_t smem_bodies, cudaStream_t st);
 
 }  // namespace seevr

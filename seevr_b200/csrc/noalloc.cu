@@ -270,7 +270,7 @@ extern "C" seevr_status seevr_physics_step_noalloc(
         launch_broadphase_n2(w, s, st);
         launch_narrowphase(w, k, s, st);
         cudaMemsetAsync(w.lambda, 0, sizeof(float) * max_contacts, st);
-        launch_solver(w, k, s, mode, sub_dt, num_bodies, st);
+        launch_solver(w, k, s, mode, sub_dt, num_bodies, num_bodies, st);
     }
     launch_body_stage(w, k, kIntegrate | (render ? kRenderVerts : 0u), sub_dt, gravity[0],
                       gravity[1], gravity[2], st);

@@ -87,6 +87,10 @@ struct seevr_physics {
     uint32_t* body_bundle = nullptr;  // body -> bundle
     uint32_t num_bundles = 1;
     uint32_t max_bundle_bodies = 0;
+    // bodies per bundle the warp solver keeps in shared memory: the bundle
+    // size, so that single scenes above it (solved in place) do not cut
+    // the number of resident warps
+    uint32_t smem_bundle_bodies = 0;
     uint32_t num_scenes = 1;
     bool scenes_set = false;
     uint32_t single_scene_nb = 0xFFFFFFFFu;
@@ -291,7 +295,7 @@ uint64_t issue_frame(seevr_physics* h, uint32_t nb, uint32_t nv, uint32_t nhv, u
         T.end(kStClear);
         T.begin();
         n += launch_solver(w, h->k, h->s, h->params.solver == SEEVR_SOLVER_SEQUENTIAL ? 0u : 1u,
-                           sub_dt, h->max_bundle_bodies, st);
+                           sub_dt, h->max_bundle_bodies, h->smem_bundle_bodies, st);
         T.end(kStSolve);
     }
     const bool render = nv > 0 && !(h->params.flags & SEEVR_FLAG_SKIP_RENDER_VERTS);
@@ -362,6 +366,7 @@ seevr_status ensure_single_scene(seevr_physics* h, uint32_t nb, cudaStream_t st)
     h->single_scene_nb = nb;
     h->max_scene_bodies = nb;
     h->max_bundle_bodies = nb;
+    h->smem_bundle_bodies = nb;
     h->num_scenes = 1;
     h->num_bundles = 1;
     return SEEVR_OK;
@@ -552,6 +557,7 @@ seevr_status seevr_physics_set_scenes(seevr_physics* h, const uint32_t* body_off
     SEEVR_CUDA(cudaMemcpy(h->body_bundle, bs.data(), sizeof(uint32_t) * nb, cudaMemcpyHostToDevice));
     h->num_bundles = uint32_t(bundles.size() - 1);
     h->max_bundle_bodies = max_bundle;
+    h->smem_bundle_bodies = h->num_bundles > 1 ? std::min(max_bundle, target) : max_bundle;
     h->num_scenes = num_scenes;
     h->scenes_set = true;
     h->single_scene_nb = nb;

@@ -273,6 +273,9 @@ __host__ __device__ constexpr uint32_t warp_smem_words(uint32_t nbmax) {
 
 __global__ void __launch_bounds__(kWarpsPerBlock * 32)
     k_solver_warp(World w, Consts k, Scratch s, uint32_t mode, float dt, uint32_t nbmax) {
+    // nbmax: bodies per warp held in shared memory; a bundle with more
+    // bodies (a single scene above the bundle size) solves on the bound
+    // velocity buffers in place
     extern __shared__ float sm[];
     const unsigned full = 0xFFFFFFFFu;
     const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
@@ -284,18 +287,22 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
     const uint32_t nbs = b1 - b0, ncb = c1 - c0;
 
     float* base = sm + size_t(wid) * warp_smem_words(nbmax);
-    float* V = base;
-    float* Wv = base + 3 * nbmax;
-    uint32_t* last = reinterpret_cast<uint32_t*>(base + 6 * nbmax);
+    const bool in_smem = nbs <= nbmax;
+    float* V = in_smem ? base : w.vel + size_t(b0) * 3;
+    float* Wv = in_smem ? base + 3 * nbmax : w.omega + size_t(b0) * 3;
+    uint32_t* last = in_smem ? reinterpret_cast<uint32_t*>(base + 6 * nbmax) : s.s_last + b0;
     float* lam = ncb <= kWarpLamCap ? base + 7 * nbmax : s.s_lam + c0;
     uint32_t* lvl_sm = reinterpret_cast<uint32_t*>(base + 7 * nbmax + kWarpLamCap);
     float* R = s.s_R + size_t(b0) * 9;
     for (uint32_t i = lane; i < nbs; i += 32) {
-        st3(V, i, ld3(w.vel, b0 + i));
-        st3(Wv, i, ld3(w.omega, b0 + i));
+        if (in_smem) {
+            st3(V, i, ld3(w.vel, b0 + i));
+            st3(Wv, i, ld3(w.omega, b0 + i));
+        }
         st_m3(R, i, quat_to_mat(w.quat, b0 + i));
         last[i] = 0;
     }
+    __syncwarp();
     BodyView B{V, Wv, R, w.inv_inertia + size_t(b0) * 3, w.inv_mass + b0};
 
     // ---- bodies of each contact; both inverse masses zero -> skipped (531)
@@ -411,10 +418,11 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
     }
     __syncwarp();
     // ---- results back to the bound buffers ----
-    for (uint32_t i = lane; i < nbs; i += 32) {
-        st3(w.vel, b0 + i, ld3(V, i));
-        st3(w.omega, b0 + i, ld3(Wv, i));
-    }
+    if (in_smem)
+        for (uint32_t i = lane; i < nbs; i += 32) {
+            st3(w.vel, b0 + i, ld3(V, i));
+            st3(w.omega, b0 + i, ld3(Wv, i));
+        }
     for (uint32_t i = lane; i < pos; i += 32) w.lambda[s.s_order[c0 + i]] = lam[i];
 }
 
@@ -439,21 +447,22 @@ int launch_bundle_ranges(const World& w, const Scratch& s, cudaStream_t st) {
 }
 
 int launch_solver(const World& w, const Consts& k, const Scratch& s, uint32_t mode, float dt,
-                  uint32_t max_scene_bodies, cudaStream_t st) {
+                  uint32_t max_scene_bodies, uint32_t smem_bodies, cudaStream_t st) {
     if (w.nbundles == 0 || w.max_contacts == 0) return 0;
     launch_bundle_ranges(w, s, st);
     if (max_scene_bodies <= kWarpMaxBodies) {
-        const uint32_t nbmax = max_scene_bodies ? max_scene_bodies : 1u;
+        uint32_t nbmax = smem_bodies < max_scene_bodies ? smem_bodies : max_scene_bodies;
+        if (nbmax == 0) nbmax = 1;
         const uint32_t blocks = (w.nbundles + kWarpsPerBlock - 1) / kWarpsPerBlock;
         const size_t smem = size_t(kWarpsPerBlock) * warp_smem_words(nbmax) * sizeof(float);
         k_solver_warp<<<blocks, kWarpsPerBlock * 32, smem, st>>>(w, k, s, mode, dt, nbmax);
         return 2;
     }
-    uint32_t smem_bodies = max_scene_bodies;
-    if (smem_bodies * kBodySmemWords * 4 > kSolverMaxSmem)
-        smem_bodies = kSolverMaxSmem / (kBodySmemWords * 4);
-    const size_t smem = size_t(smem_bodies) * kBodySmemWords * 4;
-    k_solver<<<w.nbundles, kSolverThreads, smem, st>>>(w, k, s, mode, dt, smem_bodies);
+    uint32_t cta_bodies = max_scene_bodies;
+    if (cta_bodies * kBodySmemWords * 4 > kSolverMaxSmem)
+        cta_bodies = kSolverMaxSmem / (kBodySmemWords * 4);
+    const size_t smem = size_t(cta_bodies) * kBodySmemWords * 4;
+    k_solver<<<w.nbundles, kSolverThreads, smem, st>>>(w, k, s, mode, dt, cta_bodies);
     return 2;
 }
 

@@ -195,8 +195,10 @@ seevr_status seevr_physics_step(seevr_physics* h,
                                 const float gravity[3],
                                 seevr_profile* prof);
 
-/* Same as seevr_physics_step, ordered on `stream` (a cudaStream_t) and never
- * synchronizing; `frames` consecutive calls are issued back to back.  With
+/* Same as seevr_physics_step, ordered on `stream` (a cudaStream_t; NULL =
+ * the handle's own stream, pass cudaStreamLegacy for the legacy default
+ * stream) and never synchronizing; `frames` consecutive calls are issued
+ * back to back.  With
  * SEEVR_FLAG_CUDA_GRAPH the frame is captured into a CUDA graph on first
  * use and replayed (re-captured when an argument changes).  No counterpart
  * in the reference. */
@@ -283,14 +285,16 @@ seevr_status seevr_physics_read_lbvh(seevr_physics* h, uint32_t n, uint32_t* mor
 
 /* ---- adjoint ---------------------------------------------------------------- */
 
-/* Gradient buffers of seevr_physics_adjoint_substep (device, indexed like
- * the body and geom bindings). */
+/* Gradient buffers of seevr_physics_adjoint_substep (device, FP64, indexed
+ * like the body and geom bindings).  The forward is FP32; the reverse pass
+ * runs in FP64 because the PGS sweep's per-iteration sensitivities nearly
+ * cancel. */
 typedef struct seevr_adjoint_grads {
-    float* pos;      /* f32[N*3]  in: dL/d state after the substep; out: before */
-    float* quat;     /* f32[N*4] */
-    float* vel;      /* f32[N*3] */
-    float* omega;    /* f32[N*3] */
-    float* friction; /* f32[G]    dL/d geom_friction, accumulated (+=)        */
+    double* pos;      /* f64[N*3]  in: dL/d state after the substep; out: before */
+    double* quat;     /* f64[N*4] */
+    double* vel;      /* f64[N*3] */
+    double* omega;    /* f64[N*3] */
+    double* friction; /* f64[G]    dL/d geom_friction, accumulated (+=)        */
 } seevr_adjoint_grads;
 
 /* No counterpart in the reference.  Reverse mode of one substep of

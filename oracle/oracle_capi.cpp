@@ -141,38 +141,99 @@ void add_ops(const oracle::OpCounts& c, uint64_t* ops) {
     for (int i = 0; i < 10; ++i) ops[i] += v[i];
 }
 
+constexpr uint64_t kBranchSeed = 1469598103934665603ull;
+
+// Decision tapes of the last recording run, one per instance (the whole
+// batch, or one per scene); replay runs read them.  Test infrastructure:
+// callers are single-threaded.
+std::vector<std::vector<uint32_t>> g_tapes;
+
+// Instrumentation options of a run: per-scene branch hashes and branch
+// locking (lock_mode 0 off, 1 record, 2 replay).
+struct Instr {
+    uint64_t* branch_sig;
+    int lock_mode;
+};
+
+// Set up instance `k` (covering `nsig` scenes) before its run.
+template <class R>
+bool instr_begin(oracle::Physics<R>& ph, const Instr& in, size_t k, uint32_t nsig) {
+    using L = typename oracle::Physics<R>::Lock;
+    if (in.branch_sig) ph.branch.assign(nsig, kBranchSeed);
+    if (in.lock_mode == 1) ph.lock_mode = L::Record;
+    if (in.lock_mode == 2) {
+        if (k >= g_tapes.size()) return false;
+        ph.lock_mode = L::Replay;
+        ph.lock = g_tapes[k];
+    }
+    return true;
+}
+
+// Collect instance `k`'s outputs: hashes at scene offset sig0; the tape
+// (record); false when a replay did not consume its tape exactly.
+template <class R>
+bool instr_end(oracle::Physics<R>& ph, const Instr& in, size_t k, uint32_t sig0) {
+    if (in.branch_sig) std::copy(ph.branch.begin(), ph.branch.end(), in.branch_sig + sig0);
+    if (in.lock_mode == 1) g_tapes[k] = std::move(ph.lock);
+    if (in.lock_mode == 2) return !ph.lock_error && ph.lock_pos == ph.lock.size();
+    return true;
+}
+
 template <class R>
 int run(const oracle_scene* s, const oracle_params* p, uint32_t frames, uint32_t substeps,
-        float dt, const float g[3], int update_verts, int threads, oracle_out* o) {
+        float dt, const float g[3], int update_verts, int threads, oracle_out* o,
+        const Instr& ins, const double* const st[5]) {
     const oracle::SceneIn in = to_in(s);
     const oracle::Params P = to_params(p);
     const R gr[3] = {R(g[0]), R(g[1]), R(g[2])};
     o->counters[0] = o->counters[1] = 0;
     for (auto& x : o->ops) x = 0;
+    // optional double-precision initial state (pos, quat, vel, omega, friction)
+    auto put = [&](oracle::Physics<R>& ph, uint32_t b0, uint32_t nb) {
+        if (!st) return;
+        auto cp = [](std::vector<R>& dst, const double* src, size_t off, size_t n) {
+            if (src)
+                for (size_t i = 0; i < n; ++i) dst[i] = R(src[off + i]);
+        };
+        cp(ph.pos, st[0], size_t(b0) * 3, size_t(nb) * 3);
+        cp(ph.quat, st[1], size_t(b0) * 4, size_t(nb) * 4);
+        cp(ph.vel, st[2], size_t(b0) * 3, size_t(nb) * 3);
+        cp(ph.omega, st[3], size_t(b0) * 3, size_t(nb) * 3);
+        cp(ph.friction, st[4], b0, nb);
+    };
     if (threads <= 0 || s->num_scenes <= 1 || !s->scene_body_offset) {
         // whole batch in one instance: global caps, global canonical order
         oracle::Physics<R> ph(in, P);
+        if (ins.lock_mode == 1) g_tapes.assign(1, {});
+        const uint32_t nsig = s->scene_body_offset && s->num_scenes > 0 ? s->num_scenes : 1u;
+        if (!instr_begin(ph, ins, 0, nsig)) return 3;
+        put(ph, 0, s->num_bodies);
         for (uint32_t f = 0; f < frames; ++f) ph.step(substeps, R(dt), gr, update_verts != 0);
         Totals t;
         emit(ph, 0, 0, P.max_pairs, P.max_contacts, o, &t);
         o->counters[0] = t.pairs;
         o->counters[1] = t.contacts;
         add_ops<R>(ph.ops, o->ops);
-        return 0;
+        return instr_end(ph, ins, 0, 0) ? 0 : 3;
     }
     // one instance per scene, scenes in parallel; identical results to the
     // whole-batch instance as long as no cap overflows (scenes share no body)
     const uint32_t ns = s->num_scenes;
     std::vector<oracle::Physics<R>*> inst(ns, nullptr);
+    if (ins.lock_mode == 1) g_tapes.assign(ns, {});
+    int bad = 0;
 #ifdef _OPENMP
     omp_set_num_threads(threads);
 #endif
-#pragma omp parallel for schedule(dynamic, 1)
+#pragma omp parallel for schedule(dynamic, 1) reduction(| : bad)
     for (int64_t sc = 0; sc < int64_t(ns); ++sc) {
         const uint32_t b0 = s->scene_body_offset[sc], b1 = s->scene_body_offset[sc + 1];
         if (b1 <= b0) continue;
         auto* ph = new oracle::Physics<R>(in, P, b0, b1);
+        if (!instr_begin(*ph, ins, size_t(sc), 1u)) bad = 1;
+        put(*ph, b0, b1 - b0);
         for (uint32_t f = 0; f < frames; ++f) ph->step(substeps, R(dt), gr, update_verts != 0);
+        if (!instr_end(*ph, ins, size_t(sc), uint32_t(sc))) bad = 1;
         inst[size_t(sc)] = ph;
     }
     Totals t;
@@ -185,7 +246,7 @@ int run(const oracle_scene* s, const oracle_params* p, uint32_t frames, uint32_t
     }
     o->counters[0] = t.pairs;
     o->counters[1] = t.contacts;
-    return 0;
+    return bad ? 3 : 0;
 }
 
 }  // namespace
@@ -194,45 +255,35 @@ extern "C" {
 
 // Run `frames` calls of Physics.step on a copy of the scene.  precision 32
 // or 64; threads <= 0 runs the batch as one instance, otherwise one
-// instance per scene on `threads` OpenMP threads.  Returns 0 on success.
+// instance per scene on `threads` OpenMP threads.  Test instrumentation:
+// branch_sig (NULL = off) receives per scene a hash of the run's structural
+// decisions (support vertices, pairs, contacts); lock_mode 1 records every
+// branch decision, 2 replays the last recording (same instance layout)
+// instead of deciding.  Returns 0 on success, 3 when a replay did not match
+// its recording's length.
 int oracle_run(const oracle_scene* s, const oracle_params* p, int precision, uint32_t frames,
                uint32_t substeps, float dt, const float g[3], int update_verts, int threads,
-               oracle_out* o) {
+               oracle_out* o, uint64_t* branch_sig, int lock_mode) {
     if (!s || !p || !o) return 1;
-    if (precision == 64) return run<double>(s, p, frames, substeps, dt, g, update_verts, threads, o);
-    return run<float>(s, p, frames, substeps, dt, g, update_verts, threads, o);
+    const Instr ins{branch_sig, lock_mode};
+    if (precision == 64)
+        return run<double>(s, p, frames, substeps, dt, g, update_verts, threads, o, ins, nullptr);
+    return run<float>(s, p, frames, substeps, dt, g, update_verts, threads, o, ins, nullptr);
 }
 
-// FP64 run of the whole batch (one instance) from a double-precision
-// initial state: pos/quat/vel/omega/friction override the scene's float
-// values (any may be NULL).  Central finite differences of the adjoint
-// tests perturb these inputs by far less than a float ulp.
+// FP64 run from a double-precision initial state: pos/quat/vel/omega/
+// friction override the scene's float values (any may be NULL).  Central
+// finite differences of the adjoint tests perturb these inputs by far less
+// than a float ulp.  Other arguments as oracle_run.
 int oracle_run_f64_state(const oracle_scene* s, const oracle_params* p, uint32_t frames,
                          uint32_t substeps, float dt, const float g[3], const double* pos,
                          const double* quat, const double* vel, const double* omega,
-                         const double* friction, oracle_out* o) {
+                         const double* friction, int threads, oracle_out* o,
+                         uint64_t* branch_sig, int lock_mode) {
     if (!s || !p || !o) return 1;
-    const oracle::SceneIn in = to_in(s);
-    const oracle::Params P = to_params(p);
-    const double gr[3] = {g[0], g[1], g[2]};
-    oracle::Physics<double> ph(in, P);
-    const size_t nb = s->num_bodies;
-    auto put = [](std::vector<double>& dst, const double* src, size_t n) {
-        if (src) std::copy(src, src + n, dst.begin());
-    };
-    put(ph.pos, pos, nb * 3);
-    put(ph.quat, quat, nb * 4);
-    put(ph.vel, vel, nb * 3);
-    put(ph.omega, omega, nb * 3);
-    put(ph.friction, friction, s->num_geoms);
-    for (uint32_t f = 0; f < frames; ++f) ph.step(substeps, double(dt), gr, false);
-    Totals t;
-    o->counters[0] = o->counters[1] = 0;
-    for (auto& x : o->ops) x = 0;
-    emit(ph, 0, 0, P.max_pairs, P.max_contacts, o, &t);
-    o->counters[0] = t.pairs;
-    o->counters[1] = t.contacts;
-    return 0;
+    const double* st[5] = {pos, quat, vel, omega, friction};
+    return run<double>(s, p, frames, substeps, dt, g, 0, threads, o, Instr{branch_sig, lock_mode},
+                       st);
 }
 
 // Morton codes (bvh.comp:169-183) of n centroids; bounds[6] = min, max.

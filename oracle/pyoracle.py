@@ -20,6 +20,7 @@ LIB_PATH = HERE / "liboracle.so"
 _f = C.POINTER(C.c_float)
 _u = C.POINTER(C.c_uint32)
 _d = C.POINTER(C.c_double)
+_u64 = C.POINTER(C.c_uint64)
 
 
 class OracleScene(C.Structure):
@@ -63,11 +64,11 @@ def _load():
     lib.oracle_run.restype = C.c_int
     lib.oracle_run.argtypes = [C.POINTER(OracleScene), C.POINTER(OracleParams), C.c_int,
                                C.c_uint32, C.c_uint32, C.c_float, _f, C.c_int, C.c_int,
-                               C.POINTER(OracleOut)]
+                               C.POINTER(OracleOut), _u64, C.c_int]
     lib.oracle_run_f64_state.restype = C.c_int
     lib.oracle_run_f64_state.argtypes = [C.POINTER(OracleScene), C.POINTER(OracleParams),
                                          C.c_uint32, C.c_uint32, C.c_float, _f, _d, _d, _d, _d,
-                                         _d, C.POINTER(OracleOut)]
+                                         _d, C.c_int, C.POINTER(OracleOut), _u64, C.c_int]
     lib.oracle_morton.argtypes = [_f, C.c_uint32, _u, _f]
     lib.oracle_radix_sort.argtypes = [_u, C.c_uint32, _u, _u]
     lib.oracle_karras.argtypes = [_u, C.c_uint32, _u, _u, _u]
@@ -142,11 +143,39 @@ def _finish(out: dict, o: OracleOut, nv: int, max_pairs: int, max_contacts: int)
     return out
 
 
+LOCK_MODES = {None: 0, "record": 1, "replay": 2}
+
+
+def _sig(a: dict, on: bool):
+    """Per-scene branch-hash output array, or None."""
+    if not on:
+        return None
+    off = a.get("scene_body_offset")
+    ns = len(off) - 1 if off is not None and len(off) > 1 else 1
+    return np.zeros(ns, np.uint64)
+
+
+def _done(rc: int, name: str, out: dict, o, nv, max_pairs, max_contacts, sig) -> dict:
+    if rc == 3:
+        raise RuntimeError(f"{name}: the replayed run left its recorded branches")
+    if rc != 0:
+        raise RuntimeError(f"{name} failed ({rc})")
+    out = _finish(out, o, nv, max_pairs, max_contacts)
+    if sig is not None:
+        out["branch_sig"] = sig
+    return out
+
+
 def run(arrays: dict, *, frames=1, substeps=10, dt=1.0 / 60.0, gravity=(0.0, -9.81, 0.0),
         pgs_iterations=4, max_pairs=10000, max_contacts=4000, precision=32,
-        update_verts=True, threads=0, use_hull_range=True, **consts) -> dict:
+        update_verts=True, threads=0, use_hull_range=True, branches=False, lock=None,
+        **consts) -> dict:
     """Run `frames` Physics.step calls on a copy of the scene `arrays`
-    (Data.arrays()).  Returns final state and last-substep outputs (float64)."""
+    (Data.arrays()).  Returns final state and last-substep outputs (float64).
+    branches=True adds "branch_sig": per scene, a hash of the run's
+    structural decisions (support vertices chosen, pairs, contacts).
+    lock="record" records every branch decision of the run; lock="replay"
+    follows the last recording instead of deciding (same threads layout)."""
     a = {k: np.ascontiguousarray(v) for k, v in arrays.items()}
     nb = len(a["body_inv_mass"])
     nv = len(a["orig_vertices"]) if update_verts else 0
@@ -154,20 +183,21 @@ def run(arrays: dict, *, frames=1, substeps=10, dt=1.0 / 60.0, gravity=(0.0, -9.
     P = _params(pgs_iterations, max_pairs, max_contacts, consts)
     out, o = _outputs(nb, nv, max_pairs, max_contacts)
     g = (C.c_float * 3)(*gravity)
+    sig = _sig(a, branches)
     rc = lib.oracle_run(C.byref(s), C.byref(P), precision, frames, substeps, dt, g,
-                        1 if nv else 0, threads, C.byref(o))
-    if rc != 0:
-        raise RuntimeError(f"oracle_run failed ({rc})")
-    return _finish(out, o, nv, max_pairs, max_contacts)
+                        1 if nv else 0, threads, C.byref(o), _p(sig, _u64), LOCK_MODES[lock])
+    return _done(rc, "oracle_run", out, o, nv, max_pairs, max_contacts, sig)
 
 
 def run_f64_state(arrays: dict, *, pos=None, quat=None, vel=None, omega=None, friction=None,
                   frames=1, substeps=10, dt=1.0 / 60.0, gravity=(0.0, -9.81, 0.0),
                   pgs_iterations=4, max_pairs=10000, max_contacts=4000,
-                  use_hull_range=True, **consts) -> dict:
-    """FP64 run of the whole batch whose initial pos/quat/vel/omega and
-    friction come from float64 arrays (None: the scene's float values), for
-    finite differences finer than a float ulp."""
+                  use_hull_range=True, threads=0, branches=False, lock=None,
+                  **consts) -> dict:
+    """FP64 run whose initial pos/quat/vel/omega and friction come from
+    float64 arrays (None: the scene's float values), for finite differences
+    finer than a float ulp.  threads > 0: one instance per scene in
+    parallel.  branches and lock as run()."""
     a = {k: np.ascontiguousarray(v) for k, v in arrays.items()}
     nb = len(a["body_inv_mass"])
     s = _scene(a, False, use_hull_range)
@@ -176,11 +206,11 @@ def run_f64_state(arrays: dict, *, pos=None, quat=None, vel=None, omega=None, fr
     d = lambda x: None if x is None else np.ascontiguousarray(x, dtype=np.float64)
     keep = [d(pos), d(quat), d(vel), d(omega), d(friction)]
     g = (C.c_float * 3)(*gravity)
+    sig = _sig(a, branches)
     rc = lib.oracle_run_f64_state(C.byref(s), C.byref(P), frames, substeps, dt, g,
-                                  *[_p(x, _d) for x in keep], C.byref(o))
-    if rc != 0:
-        raise RuntimeError(f"oracle_run_f64_state failed ({rc})")
-    return _finish(out, o, 0, max_pairs, max_contacts)
+                                  *[_p(x, _d) for x in keep], threads, C.byref(o),
+                                  _p(sig, _u64), LOCK_MODES[lock])
+    return _done(rc, "oracle_run_f64_state", out, o, 0, max_pairs, max_contacts, sig)
 
 
 def morton(centroids: np.ndarray):

@@ -148,6 +148,38 @@ class Physics {
     std::vector<uint32_t> hull_start, hull_count, vert_start, geom_body, sup_off;
     const uint32_t* sup_lut = nullptr;  // shared lookup table (absolute offsets)
     std::vector<uint32_t> scene_of;  // body -> scene
+    // Test instrumentation (off while empty): per scene, a hash of the
+    // step's structural decisions (every support vertex chosen, every pair
+    // and whether it made a contact), so that two runs can be checked to
+    // have produced the same contact sets from the same MPR portals.
+    std::vector<uint64_t> branch;
+    void mix(uint32_t body, uint64_t v) {
+        if (branch.empty()) return;
+        uint64_t& h = branch[scene_of[body]];
+        h = (h ^ v) * 1099511628211ull;
+    }
+    // Test instrumentation: branch locking.  In Record mode every
+    // data-dependent decision of the step (each float comparison that picks
+    // a branch, each support vertex chosen) is appended to `lock`; in Replay
+    // mode the decisions are read back instead of computed, so that a run in
+    // another precision, or from perturbed inputs, follows exactly the
+    // recorded branches.  Finite differences of replayed FP64 runs are then
+    // the derivative of the recorded branch: what an adjoint computes.
+    enum class Lock { Off, Record, Replay };
+    Lock lock_mode = Lock::Off;
+    std::vector<uint32_t> lock;
+    size_t lock_pos = 0;
+    bool lock_error = false;  // replay ran past the recorded decisions
+    uint32_t decide(uint32_t v) {
+        if (lock_mode == Lock::Record) {
+            lock.push_back(v);
+        } else if (lock_mode == Lock::Replay) {
+            if (lock_pos < lock.size()) return lock[lock_pos++];
+            lock_error = true;
+        }
+        return v;
+    }
+    bool decide(bool b) { return decide(b ? 1u : 0u) != 0u; }
     std::vector<uint32_t> scene_end; // scene -> one past its last body
     uint32_t nb = 0, nv = 0, nhv = 0;
     Params P;
@@ -259,14 +291,19 @@ class Physics {
             ops.support_brute_verts += vc;
             R best = R(-1e10);
             V3<R> bv = {R(0), R(0), R(0)};
+            uint32_t chosen = 0xFFFFFFFFu;
             for (uint32_t i = 0; i < vc; ++i) {
                 const V3<R> v = get3(hull, vs + i);
                 const R dd = dot(v, ld);
                 if (dd > best) {
                     best = dd;
                     bv = v;
+                    chosen = i;
                 }
             }
+            chosen = decide(chosen);
+            bv = chosen < vc ? get3(hull, vs + chosen) : V3<R>{R(0), R(0), R(0)};
+            mix(bi, chosen);
             return p + mul(Rm, bv);
         }
         ops.support_lookup++;
@@ -274,6 +311,7 @@ class Physics {
         const R two_pi = R(6.2831853);
         R best = R(-1e10);
         V3<R> bv = {R(0), R(0), R(0)};
+        uint32_t chosen = 0xFFFFFFFFu;
         for (uint32_t ax = 0; ax < 3; ++ax) {
             R a = angles[ax];
             if (a < R(0)) a += two_pi;
@@ -285,14 +323,19 @@ class Physics {
             if (d0 > best) {
                 best = d0;
                 bv = v0;
+                chosen = sup_lut[lk + ax * 64 + b0];
             }
             const V3<R> v1 = get3(hull, vs + sup_lut[lk + ax * 64 + b1]);
             const R d1 = dot(v1, ld);
             if (d1 > best) {
                 best = d1;
                 bv = v1;
+                chosen = sup_lut[lk + ax * 64 + b1];
             }
         }
+        chosen = decide(chosen);
+        bv = chosen < vc ? get3(hull, vs + chosen) : V3<R>{R(0), R(0), R(0)};
+        mix(bi, chosen);
         return p + mul(Rm, bv);
     }
     void mink(uint32_t a, uint32_t b, V3<R> d, V3<R>& v, V3<R>& sa, V3<R>& sb) {  // 165-169
@@ -310,29 +353,29 @@ class Physics {
         const R dot1 = gmin(gmin(dv4 - dv1, dv4 - dv2), dv4 - dv3);
         return dot1 < R(P.tol) + eps() * gmax(R(1), dot1);
     }
-    static void expand(V3<R>& v0, V3<R>& v1, V3<R>& v2, V3<R>& v3, V3<R> v4, V3<R>& s1a,
-                       V3<R>& s2a, V3<R>& s3a, V3<R> s4a, V3<R>& s1b, V3<R>& s2b, V3<R>& s3b,
-                       V3<R> s4b) {  // 200-221
+    void expand(V3<R>& v0, V3<R>& v1, V3<R>& v2, V3<R>& v3, V3<R> v4, V3<R>& s1a,
+                V3<R>& s2a, V3<R>& s3a, V3<R> s4a, V3<R>& s1b, V3<R>& s2b, V3<R>& s3b,
+                V3<R> s4b) {  // 200-221
         const V3<R> v4v0 = cross(v4, v0);
         R d = dot(v1, v4v0);
-        if (d > R(0)) {
+        if (decide(d > R(0))) {
             d = dot(v2, v4v0);
-            if (d > R(0)) { v1 = v4; s1a = s4a; s1b = s4b; }
+            if (decide(d > R(0))) { v1 = v4; s1a = s4a; s1b = s4b; }
             else { v3 = v4; s3a = s4a; s3b = s4b; }
         } else {
             d = dot(v3, v4v0);
-            if (d > R(0)) { v2 = v4; s2a = s4a; s2b = s4b; }
+            if (decide(d > R(0))) { v2 = v4; s2a = s4a; s2b = s4b; }
             else { v1 = v4; s1a = s4a; s1b = s4b; }
         }
     }
     V3<R> find_pos(V3<R> v0, V3<R> v1, V3<R> v2, V3<R> v3, V3<R> s0a, V3<R> s1a, V3<R> s2a,
-                   V3<R> s3a, V3<R> s0b, V3<R> s1b, V3<R> s2b, V3<R> s3b) const {  // 224-247
+                   V3<R> s3a, V3<R> s0b, V3<R> s1b, V3<R> s2b, V3<R> s3b) {  // 224-247
         R b0 = dot(cross(v1, v2), v3);
         R b1 = -dot(cross(v0, v2), v3);
         R b2 = dot(cross(v0, v1), v3);
         R b3 = -dot(cross(v0, v1), v2);
         R sum = b0 + b1 + b2 + b3;
-        if (std::fabs(sum) < eps()) {
+        if (decide(std::fabs(sum) < eps())) {
             const V3<R> dir = portal_dir(v1, v2, v3);
             b0 = R(0);
             b1 = dot(cross(v2, v3), dir);
@@ -350,25 +393,25 @@ class Physics {
         s0a = get3(pos, a);
         s0b = get3(pos, b);
         v0 = s0a - s0b;
-        if (std::fabs(v0.x) < eps() && std::fabs(v0.y) < eps() && std::fabs(v0.z) < eps())
+        if (decide(std::fabs(v0.x) < eps() && std::fabs(v0.y) < eps() && std::fabs(v0.z) < eps()))
             v0.x += R(10) * eps();
         V3<R> dir = normalize(-v0);
         mink(a, b, dir, v1, s1a, s1b);
         R d = dot(v1, dir);
-        if (d < eps()) return -1;
+        if (decide(d < eps())) return -1;
         dir = cross(v0, v1);
-        if (dot(dir, dir) < eps()) {
-            if (std::fabs(v1.x) < eps() && std::fabs(v1.y) < eps() && std::fabs(v1.z) < eps())
+        if (decide(dot(dir, dir) < eps())) {
+            if (decide(std::fabs(v1.x) < eps() && std::fabs(v1.y) < eps() && std::fabs(v1.z) < eps()))
                 return 1;
             return 2;
         }
         dir = normalize(dir);
         mink(a, b, dir, v2, s2a, s2b);
         d = dot(v2, dir);
-        if (d < eps()) return -1;
+        if (decide(d < eps())) return -1;
         V3<R> va = v1 - v0, vb = v2 - v0;
         dir = normalize(cross(va, vb));
-        if (dot(dir, v0) > R(0)) {
+        if (decide(dot(dir, v0) > R(0))) {
             std::swap(v1, v2);
             std::swap(s1a, s2a);
             std::swap(s1b, s2b);
@@ -379,10 +422,10 @@ class Physics {
             V3<R> v3c, s3ca, s3cb;
             mink(a, b, dir, v3c, s3ca, s3cb);
             d = dot(v3c, dir);
-            if (d < eps()) return -1;
+            if (decide(d < eps())) return -1;
             va = cross(v1, v3c);
             d = dot(va, v0);
-            if (d < -eps()) {
+            if (decide(d < -eps())) {
                 v2 = v3c; s2a = s3ca; s2b = s3cb;
                 va = v1 - v0; vb = v2 - v0;
                 dir = normalize(cross(va, vb));
@@ -391,7 +434,7 @@ class Physics {
             }
             va = cross(v3c, v2);
             d = dot(va, v0);
-            if (d < -eps()) {
+            if (decide(d < -eps())) {
                 v1 = v3c; s1a = s3ca; s1b = s3cb;
                 va = v1 - v0; vb = v2 - v0;
                 dir = normalize(cross(va, vb));
@@ -424,10 +467,10 @@ class Physics {
         res = 1;
         for (uint32_t it = 0; it < P.mpr_iterations; ++it) {
             const V3<R> dir = portal_dir(v1, v2, v3);
-            if (dot(v1, dir) > -eps()) { res = 0; break; }
+            if (decide(dot(v1, dir) > -eps())) { res = 0; break; }
             V3<R> v4, s4a, s4b;
             mink(a, b, dir, v4, s4a, s4b);
-            if (!(dot(v4, dir) > -eps()) || reach_tol(v1, v2, v3, v4, dir)) { res = -1; break; }
+            if (decide(!(dot(v4, dir) > -eps()) || reach_tol(v1, v2, v3, v4, dir))) { res = -1; break; }
             expand(v0, v1, v2, v3, v4, s1a, s2a, s3a, s4a, s1b, s2b, s3b, s4b);
         }
         if (res < 0) return false;
@@ -437,7 +480,7 @@ class Physics {
             const V3<R> dir = portal_dir(v1, v2, v3);
             V3<R> v4, s4a, s4b;
             mink(a, b, dir, v4, s4a, s4b);
-            if (reach_tol(v1, v2, v3, v4, dir) || it >= P.mpr_iterations - 1) {
+            if (decide(reach_tol(v1, v2, v3, v4, dir) || it >= P.mpr_iterations - 1)) {
                 depth = dot(dir, v1);
                 normal = dir;
                 found = true;
@@ -502,8 +545,8 @@ class Physics {
                 ops.broad_tests++;
                 if (inv_mass[i] <= R(0) && inv_mass[j] <= R(0)) continue;
                 const V3<R> mnb = get3(aabb_min, j), mxb = get3(aabb_max, j);
-                if (!(mxa.x < mnb.x || mxb.x < mna.x || mxa.y < mnb.y || mxb.y < mna.y ||
-                      mxa.z < mnb.z || mxb.z < mna.z)) {
+                if (decide(!(mxa.x < mnb.x || mxb.x < mna.x || mxa.y < mnb.y || mxb.y < mna.y ||
+                             mxa.z < mnb.z || mxb.z < mna.z))) {
                     if (pairs_total < P.max_pairs) {
                         pairs.push_back(i);
                         pairs.push_back(j);
@@ -521,7 +564,10 @@ class Physics {
             const uint32_t a = pairs[pi * 2], b = pairs[pi * 2 + 1];
             V3<R> n{}, cp{};
             R depth = R(0);
-            if (mpr(a, b, n, depth, cp) && depth > R(0)) {
+            const bool found = mpr(a, b, n, depth, cp);
+            const bool hit = decide(found && depth > R(0));
+            mix(a, (uint64_t(b - a) << 8) ^ (hit ? 0x5Aull : 0ull));
+            if (hit) {
                 if (contacts_total < P.max_contacts) {
                     c_pos.insert(c_pos.end(), {cp.x, cp.y, cp.z});
                     c_normal.insert(c_normal.end(), {n.x, n.y, n.z});
@@ -548,7 +594,9 @@ class Physics {
             const R vn = dot(vb - va, n);
             const R pen = c_pen[ci];
             const R e = gmax(restitution[ga], restitution[gb]);
-            bias[ci] = baum * gmax(pen - slop, R(0)) / dt + e * gmax(-vn, R(0));
+            const R over = decide(pen - slop < R(0)) ? R(0) : pen - slop;  // gmax(pen - slop, 0)
+            const R sep = decide(-vn < R(0)) ? R(0) : -vn;                  // gmax(-vn, 0)
+            bias[ci] = baum * over / dt + e * sep;
         }
         for (uint32_t it = 0; it < P.pgs_iterations; ++it) {
             for (uint32_t ci = 0; ci < nc; ++ci) {
@@ -566,7 +614,7 @@ class Physics {
                 const R k = ima + imb + dot(ran, apply_inv_I(a, ran)) + dot(rbn, apply_inv_I(b, rbn));
                 R d_ln = (-vn + bias[ci]) / k;
                 const R old_ln = lambda[ci];
-                const R new_ln = gmax(old_ln + d_ln, R(0));
+                const R new_ln = decide(old_ln + d_ln < R(0)) ? R(0) : old_ln + d_ln;  // gmax(., 0)
                 d_ln = new_ln - old_ln;
                 lambda[ci] = new_ln;
                 const V3<R> imp = d_ln * n;
@@ -580,12 +628,13 @@ class Physics {
                 const V3<R> dv = vb - va;
                 const V3<R> vt = dv - dot(dv, n) * n;
                 const R vt_len = length(vt);
-                if (vt_len > R(1e-6)) {
+                if (decide(vt_len > R(1e-6))) {
                     ops.pgs_friction_iters++;
                     const V3<R> td = divs(vt, vt_len);
                     const V3<R> rat = cross(ra, td), rbt = cross(rb, td);
                     const R kt = ima + imb + dot(rat, apply_inv_I(a, rat)) + dot(rbt, apply_inv_I(b, rbt));
-                    const R d_lt = gmin(vt_len / kt, mu * lambda[ci]);
+                    const R q1 = vt_len / kt, q2 = mu * lambda[ci];
+                    const R d_lt = decide(q2 < q1) ? q2 : q1;  // gmin(q1, q2)
                     const V3<R> imp_t = d_lt * td;
                     set3(vel, a, get3(vel, a) + ima * imp_t);
                     set3(vel, b, get3(vel, b) - imb * imp_t);
@@ -611,7 +660,7 @@ class Physics {
             qz += h * dz * dt;
             qw += h * dw * dt;
             const R l = std::sqrt(qx * qx + qy * qy + qz * qz + qw * qw);
-            if (l > R(1e-8)) {
+            if (decide(l > R(1e-8))) {
                 qx /= l;
                 qy /= l;
                 qz /= l;

@@ -25,6 +25,9 @@ OK, ERR_INVALID_ARGUMENT, ERR_CAPACITY, ERR_CUDA, ERR_TIMEOUT, ERR_NO_DEVICE, \
 BROADPHASE_N2, BROADPHASE_LBVH = 0, 1
 SOLVER_SEQUENTIAL, SOLVER_WAVEFRONT, SOLVER_COLORED = 0, 1, 2
 FLAG_NO_SYNC, FLAG_CUDA_GRAPH, FLAG_SKIP_RENDER_VERTS = 1, 2, 4
+# bits of seevr_physics_read_flags
+DEVICE_FLAG_PAIR_OVERFLOW, DEVICE_FLAG_CONTACT_OVERFLOW, DEVICE_FLAG_TIMEOUT, \
+    DEVICE_FLAG_SOLVER_GLOBAL = 1, 2, 4, 8
 
 # binding indices (physics.comp:16-57 + extension 30)
 (B_BODY_POS, B_BODY_QUAT, B_BODY_VEL, B_BODY_OMEGA, B_BODY_INV_MASS, B_BODY_INV_INERTIA,

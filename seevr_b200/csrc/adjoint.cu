@@ -1,6 +1,6 @@
 // adjoint.cu — reverse mode of one physics substep, for gradients of a
-// rollout with respect to initial velocities, angular velocities and
-// friction coefficients.
+// rollout with respect to initial positions, orientations, velocities,
+// angular velocities and friction coefficients.
 //
 // The substep is gravity (physics.comp:418-428), contacts from MPR
 // (physics.comp:171-399, 475-491), the PGS solve (500-583) and integration
@@ -18,55 +18,93 @@
 // Contact selection (AABBs, broadphase, which pairs touch, MPR's discrete
 // portal choices) and the clamps max(., 0), min(., .) and the friction test
 // are piecewise constant: the adjoint follows the branches the forward took.
-// The sequential parts run on lane 0 of the bundle's warp, so every sum is
-// accumulated in a fixed order and the gradients are deterministic.
+//
+// Precision: every forward quantity is recomputed in FP32 with the forward's
+// arithmetic, so branch decisions and values are the forward's own; the
+// reverse-mode arithmetic on them runs in FP64 (type d3 below).  The PGS
+// sweep's per-iteration sensitivities nearly cancel (later iterations undo
+// most of an earlier impulse), so FP32 accumulation loses digits, most
+// visibly in the friction gradient, while FP64 keeps the result to the
+// FP32 forward's own accuracy.  The sequential parts run on lane 0 of the
+// bundle's warp, so every sum is accumulated in a fixed order and the
+// gradients are deterministic.
 #include "adjoint.cuh"
 
 namespace seevr {
 namespace {
 
-__device__ __forceinline__ f3 z3() { return mk(0.f, 0.f, 0.f); }
-__device__ __forceinline__ void acc(f3& a, f3 b) { a = add(a, b); }
-__device__ __forceinline__ void acc_s(f3& a, float s, f3 b) { a = add(a, scale(s, b)); }
-__device__ __forceinline__ void add3(float* p, uint32_t i, f3 v) {
+// ---- FP64 vectors for the reverse pass (operators only on d3, so an FP32
+// f3 can never enter a derivative expression without an explicit D()) ----
+struct d3 {
+    double x, y, z;
+};
+struct dm3 {
+    d3 c0, c1, c2;
+};
+__device__ __forceinline__ d3 D(f3 a) { return d3{a.x, a.y, a.z}; }
+__device__ __forceinline__ dm3 DM(const m3& m) { return dm3{D(m.c0), D(m.c1), D(m.c2)}; }
+__device__ __forceinline__ d3 dz() { return d3{0.0, 0.0, 0.0}; }
+__device__ __forceinline__ d3 operator+(d3 a, d3 b) { return d3{a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ d3 operator-(d3 a, d3 b) { return d3{a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ d3 operator-(d3 a) { return d3{-a.x, -a.y, -a.z}; }
+__device__ __forceinline__ d3 operator*(double s, d3 a) { return d3{s * a.x, s * a.y, s * a.z}; }
+__device__ __forceinline__ d3& operator+=(d3& a, d3 b) {
+    a = a + b;
+    return a;
+}
+__device__ __forceinline__ double ddot(d3 a, d3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ d3 dcross(d3 a, d3 b) {
+    return d3{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+__device__ __forceinline__ d3 dhad(d3 a, d3 b) { return d3{a.x * b.x, a.y * b.y, a.z * b.z}; }
+__device__ __forceinline__ d3 dmul(const dm3& m, d3 v) { return v.x * m.c0 + v.y * m.c1 + v.z * m.c2; }
+__device__ __forceinline__ d3 dmulT(const dm3& m, d3 v) {
+    return d3{ddot(m.c0, v), ddot(m.c1, v), ddot(m.c2, v)};
+}
+// R (I ⊙ (Rᵀ v)) (apply_inv_I, physics.comp:90-94) in FP64
+__device__ __forceinline__ d3 dapply(const dm3& R, d3 I, d3 v) { return dmul(R, dhad(I, dmulT(R, v))); }
+__device__ __forceinline__ dm3 dm3zero() { return dm3{dz(), dz(), dz()}; }
+__device__ __forceinline__ void addd3(double* p, uint32_t i, d3 v) {
     p[size_t(i) * 3] += v.x;
     p[size_t(i) * 3 + 1] += v.y;
     p[size_t(i) * 3 + 2] += v.z;
 }
-__device__ __forceinline__ m3 m3zero() {
-    m3 m;
-    m.c0 = m.c1 = m.c2 = z3();
-    return m;
+__device__ __forceinline__ d3 ldd3(const double* p, uint32_t i) {
+    return d3{p[size_t(i) * 3], p[size_t(i) * 3 + 1], p[size_t(i) * 3 + 2]};
 }
-__device__ __forceinline__ void add_m3(float* p, uint32_t i, const m3& g) {
-    float* q = p + size_t(i) * 9;
+__device__ __forceinline__ void std3(double* p, uint32_t i, d3 v) {
+    p[size_t(i) * 3] = v.x;
+    p[size_t(i) * 3 + 1] = v.y;
+    p[size_t(i) * 3 + 2] = v.z;
+}
+__device__ __forceinline__ void add_dm3(double* p, uint32_t i, const dm3& g) {
+    double* q = p + size_t(i) * 9;
     q[0] += g.c0.x; q[1] += g.c0.y; q[2] += g.c0.z;
     q[3] += g.c1.x; q[4] += g.c1.y; q[5] += g.c1.z;
     q[6] += g.c2.x; q[7] += g.c2.y; q[8] += g.c2.z;
 }
 
-// y = R (I ⊙ (Rᵀ x)) (apply_inv_I, physics.comp:90-94): accumulates dL/dR
-// into gR (columns) and returns dL/dx (the map is symmetric in x).
-__device__ __forceinline__ f3 inv_I_bwd(const m3& R, f3 I, f3 x, f3 gy, m3& gR) {
-    const f3 w = mulT(R, x);
-    const f3 u = hadamard(I, w);
-    const f3 gw = hadamard(I, mulT(R, gy));
-    gR.c0 = add(gR.c0, add(scale(u.x, gy), scale(gw.x, x)));
-    gR.c1 = add(gR.c1, add(scale(u.y, gy), scale(gw.y, x)));
-    gR.c2 = add(gR.c2, add(scale(u.z, gy), scale(gw.z, x)));
-    return mul(R, gw);
+// y = R (I ⊙ (Rᵀ x)): accumulates dL/dR into gR (columns) and returns dL/dx
+// (the map is symmetric in x).
+__device__ __forceinline__ d3 inv_I_bwd(const dm3& R, d3 I, d3 x, d3 gy, dm3& gR) {
+    const d3 u = dhad(I, dmulT(R, x));
+    const d3 gw = dhad(I, dmulT(R, gy));
+    gR.c0 += u.x * gy + gw.x * x;
+    gR.c1 += u.y * gy + gw.y * x;
+    gR.c2 += u.z * gy + gw.z * x;
+    return dmul(R, gw);
 }
 
 // dL/d(x,y,z,w) of quat_to_mat (physics.comp:74-81) from dL/dR by columns
-__device__ __forceinline__ void quat_bwd(float x, float y, float z, float w, const float* g,
-                                         float out[4]) {
-    out[0] = 2.f * (g[1] * y + g[2] * z + g[3] * y - 2.f * g[4] * x + g[5] * w + g[6] * z -
-                    g[7] * w - 2.f * g[8] * x);
-    out[1] = 2.f * (-2.f * g[0] * y + g[1] * x - g[2] * w + g[3] * x + g[5] * z + g[6] * w +
-                    g[7] * z - 2.f * g[8] * y);
-    out[2] = 2.f * (-2.f * g[0] * z + g[1] * w + g[2] * x - g[3] * w - 2.f * g[4] * z + g[5] * y +
+__device__ __forceinline__ void quat_bwd(double x, double y, double z, double w, const double* g,
+                                         double out[4]) {
+    out[0] = 2.0 * (g[1] * y + g[2] * z + g[3] * y - 2.0 * g[4] * x + g[5] * w + g[6] * z -
+                    g[7] * w - 2.0 * g[8] * x);
+    out[1] = 2.0 * (-2.0 * g[0] * y + g[1] * x - g[2] * w + g[3] * x + g[5] * z + g[6] * w +
+                    g[7] * z - 2.0 * g[8] * y);
+    out[2] = 2.0 * (-2.0 * g[0] * z + g[1] * w + g[2] * x - g[3] * w - 2.0 * g[4] * z + g[5] * y +
                     g[6] * x + g[7] * y);
-    out[3] = 2.f * (g[1] * z - g[2] * y - g[3] * z + g[5] * x + g[6] * y - g[7] * x);
+    out[3] = 2.0 * (g[1] * z - g[2] * y - g[3] * z + g[5] * x + g[6] * y - g[7] * x);
 }
 
 struct Body {
@@ -84,13 +122,14 @@ __device__ __forceinline__ Body load_body(const World& w, uint32_t b) {
     return o;
 }
 
+// Contact constants (FP32, the forward's values) and their gradients (FP64).
 struct CParams {
     f3 n, ra, rb;
     float bias, kn, mu;
 };
 struct CGrad {
-    f3 n, ra, rb;
-    float bias, kn, mu;
+    d3 n, ra, rb;
+    double bias, kn, mu;
 };
 __device__ __forceinline__ CParams ld_par(const float* p, uint32_t c) {
     const float* q = p + size_t(c) * 12;
@@ -104,13 +143,13 @@ __device__ __forceinline__ void st_par(float* p, uint32_t c, const CParams& v) {
     q[6] = v.rb.x; q[7] = v.rb.y; q[8] = v.rb.z;
     q[9] = v.bias; q[10] = v.kn; q[11] = v.mu;
 }
-__device__ __forceinline__ CGrad ld_grad(const float* p, uint32_t c) {
-    const float* q = p + size_t(c) * 12;
-    return CGrad{mk(q[0], q[1], q[2]), mk(q[3], q[4], q[5]), mk(q[6], q[7], q[8]), q[9], q[10],
+__device__ __forceinline__ CGrad ld_grad(const double* p, uint32_t c) {
+    const double* q = p + size_t(c) * 12;
+    return CGrad{d3{q[0], q[1], q[2]}, d3{q[3], q[4], q[5]}, d3{q[6], q[7], q[8]}, q[9], q[10],
                  q[11]};
 }
-__device__ __forceinline__ void st_grad(float* p, uint32_t c, const CGrad& v) {
-    float* q = p + size_t(c) * 12;
+__device__ __forceinline__ void st_grad(double* p, uint32_t c, const CGrad& v) {
+    double* q = p + size_t(c) * 12;
     q[0] = v.n.x; q[1] = v.n.y; q[2] = v.n.z;
     q[3] = v.ra.x; q[4] = v.ra.y; q[5] = v.ra.z;
     q[6] = v.rb.x; q[7] = v.rb.y; q[8] = v.rb.z;
@@ -161,9 +200,9 @@ __device__ __forceinline__ void update_fwd(const Body& A, const Body& B, const C
 // after the update) and glam dL/d(λ after); on return dL/d(before).
 // Parameter gradients accumulate into gc, gRa, gRb.
 __device__ void update_bwd(const Body& A, const Body& B, const CParams& c, f3 va, f3 wa, f3 vb,
-                           f3 wb, float lam, f3& Gva, f3& Gwa, f3& Gvb, f3& Gwb, float& glam,
-                           CGrad& gc, m3& gRa, m3& gRb) {
-    // forward intermediates
+                           f3 wb, float lam, d3& Gva, d3& Gwa, d3& Gvb, d3& Gwb, double& glam,
+                           CGrad& gc, dm3& gRa, dm3& gRb) {
+    // forward intermediates, FP32 as in the forward: the same values and branches
     const f3 ua = add(va, cross(wa, c.ra)), ub = add(vb, cross(wb, c.rb));
     const f3 dvn = sub(ub, ua);
     const float vn = dot(dvn, c.n);
@@ -181,240 +220,261 @@ __device__ void update_bwd(const Body& A, const Body& B, const CParams& c, f3 va
     const float dn = dot(dv, c.n);
     const f3 vt = sub(dv, scale(dn, c.n));
     const float s = length(vt);
+    // the reverse pass, FP64
+    const dm3 RA = DM(A.R), RB = DM(B.R);
+    const d3 IA = D(A.I), IB = D(B.I);
+    const double ima = A.ima, imb = B.ima;
+    const d3 n = D(c.n), ra = D(c.ra), rb = D(c.rb);
     // gradients of the outputs: a fixed body's outputs are discarded
-    const f3 gva2 = A.fixed ? z3() : Gva, gwa2 = A.fixed ? z3() : Gwa;
-    const f3 gvb2 = B.fixed ? z3() : Gvb, gwb2 = B.fixed ? z3() : Gwb;
-    f3 gva1 = gva2, gwa1 = gwa2, gvb1 = gvb2, gwb1 = gwb2;
-    float g_l1 = glam;
-    f3 g_vt = z3();
-    float g_s = 0.f;
+    const d3 gva2 = A.fixed ? dz() : Gva, gwa2 = A.fixed ? dz() : Gwa;
+    const d3 gvb2 = B.fixed ? dz() : Gvb, gwb2 = B.fixed ? dz() : Gwb;
+    d3 gva1 = gva2, gwa1 = gwa2, gvb1 = gvb2, gwb1 = gwb2;
+    double g_l1 = glam;
+    d3 g_vt = dz();
+    double g_s = 0.0;
     if (s > 1e-6f) {
-        const f3 td = divs(vt, s);
-        const f3 rat = cross(c.ra, td), rbt = cross(c.rb, td);
-        const f3 pa = apply_inv_I(A.R, A.I, rat), pb = apply_inv_I(B.R, B.I, rbt);
-        const float kt = A.ima + B.ima + dot(rat, pa) + dot(rbt, pb);
+        const f3 tdf = divs(vt, s);
+        const f3 ratf = cross(c.ra, tdf), rbtf = cross(c.rb, tdf);
+        const float kt = A.ima + B.ima + dot(ratf, apply_inv_I(A.R, A.I, ratf)) +
+                         dot(rbtf, apply_inv_I(B.R, B.I, rbtf));
         const float q1 = s / kt, q2 = c.mu * l1;
         const bool take2 = q2 < q1;  // GLSL min(q1, q2)
-        const float dt_ = take2 ? q2 : q1;
-        const f3 it = scale(dt_, td);
-        const f3 xa2 = cross(c.ra, it), xb2 = cross(c.rb, it);
-        f3 g_it = z3();
-        // wa2 = wa1 + A(xa2); wb2 = wb1 - A(xb2)
-        const f3 g_xa2 = inv_I_bwd(A.R, A.I, xa2, gwa2, gRa);
-        const f3 g_xb2 = inv_I_bwd(B.R, B.I, xb2, neg(gwb2), gRb);
-        acc(gc.ra, cross(it, g_xa2));
-        acc(g_it, cross(g_xa2, c.ra));
-        acc(gc.rb, cross(it, g_xb2));
-        acc(g_it, cross(g_xb2, c.rb));
+        const float dtf = take2 ? q2 : q1;
+        const f3 itf = scale(dtf, tdf);
+        const d3 td = D(tdf), it = D(itf), rat = D(ratf), rbt = D(rbtf);
+        const double ktd = kt, sd = s, dtd = dtf;
+        d3 g_it = dz();
+        // wa2 = wa1 + A(ra x it); wb2 = wb1 - B(rb x it)
+        const d3 g_xa2 = inv_I_bwd(RA, IA, D(cross(c.ra, itf)), gwa2, gRa);
+        const d3 g_xb2 = inv_I_bwd(RB, IB, D(cross(c.rb, itf)), -gwb2, gRb);
+        gc.ra += dcross(it, g_xa2);
+        g_it += dcross(g_xa2, ra);
+        gc.rb += dcross(it, g_xb2);
+        g_it += dcross(g_xb2, rb);
         // va2 = va1 + ima it; vb2 = vb1 - imb it
-        acc_s(g_it, A.ima, gva2);
-        acc_s(g_it, -B.ima, gvb2);
+        g_it += ima * gva2;
+        g_it += (-imb) * gvb2;
         // it = dt_ td
-        const float g_dt = dot(g_it, td);
-        f3 g_td = scale(dt_, g_it);
-        float g_kt = 0.f;
+        const double g_dt = ddot(g_it, td);
+        d3 g_td = dtd * g_it;
+        double g_kt = 0.0;
         if (take2) {
-            gc.mu += g_dt * l1;
-            g_l1 += g_dt * c.mu;
+            gc.mu += g_dt * double(l1);
+            g_l1 += g_dt * double(c.mu);
         } else {
-            g_s += g_dt / kt;
-            g_kt = -g_dt * s / (kt * kt);
+            g_s += g_dt / ktd;
+            g_kt = -g_dt * sd / (ktd * ktd);
         }
-        // kt = ... + rat·A(rat) + rbt·A(rbt): d/drat = 2 A(rat)
-        const f3 g_rat = scale(2.f * g_kt, pa), g_rbt = scale(2.f * g_kt, pb);
-        inv_I_bwd(A.R, A.I, rat, scale(g_kt, rat), gRa);
-        inv_I_bwd(B.R, B.I, rbt, scale(g_kt, rbt), gRb);
+        // kt = ... + rat·A(rat) + rbt·B(rbt): d/drat = 2 A(rat)
+        const d3 g_rat = (2.0 * g_kt) * dapply(RA, IA, rat);
+        const d3 g_rbt = (2.0 * g_kt) * dapply(RB, IB, rbt);
+        inv_I_bwd(RA, IA, rat, g_kt * rat, gRa);
+        inv_I_bwd(RB, IB, rbt, g_kt * rbt, gRb);
         // rat = ra x td
-        acc(gc.ra, cross(td, g_rat));
-        acc(g_td, cross(g_rat, c.ra));
-        acc(gc.rb, cross(td, g_rbt));
-        acc(g_td, cross(g_rbt, c.rb));
+        gc.ra += dcross(td, g_rat);
+        g_td += dcross(g_rat, ra);
+        gc.rb += dcross(td, g_rbt);
+        g_td += dcross(g_rbt, rb);
         // td = vt / s
-        acc_s(g_vt, 1.f / s, g_td);
-        g_s += -dot(g_td, vt) / (s * s);
+        g_vt += (1.0 / sd) * g_td;
+        g_s += -ddot(g_td, D(vt)) / (sd * sd);
     }
-    if (s > 0.f) acc_s(g_vt, g_s / s, vt);
+    if (s > 0.f) g_vt += (g_s / double(s)) * D(vt);
     // vt = dv - dn n; dn = dv·n
-    f3 g_dv = g_vt;
-    const float g_dn = -dot(g_vt, c.n);
-    acc_s(gc.n, -dn, g_vt);
-    acc_s(g_dv, g_dn, c.n);
-    acc_s(gc.n, g_dn, dv);
+    d3 g_dv = g_vt;
+    const double g_dn = -ddot(g_vt, n);
+    gc.n += (-double(dn)) * g_vt;
+    g_dv += g_dn * n;
+    gc.n += g_dn * D(dv);
     // dv = ub1 - ua1; ua1 = va1 + wa1 x ra
-    const f3 g_ua1 = neg(g_dv), g_ub1 = g_dv;
-    acc(gva1, g_ua1);
-    acc(gwa1, cross(c.ra, g_ua1));
-    acc(gc.ra, cross(g_ua1, wa1));
-    acc(gvb1, g_ub1);
-    acc(gwb1, cross(c.rb, g_ub1));
-    acc(gc.rb, cross(g_ub1, wb1));
-    // wa1 = wa - A(xa); wb1 = wb + A(xb); xa = ra x imp
-    f3 gi_va = gva1, gi_wa = gwa1, gi_vb = gvb1, gi_wb = gwb1, g_imp = z3();
-    const f3 g_xa = inv_I_bwd(A.R, A.I, xa, neg(gwa1), gRa);
-    const f3 g_xb = inv_I_bwd(B.R, B.I, xb, gwb1, gRb);
-    acc(gc.ra, cross(imp, g_xa));
-    acc(g_imp, cross(g_xa, c.ra));
-    acc(gc.rb, cross(imp, g_xb));
-    acc(g_imp, cross(g_xb, c.rb));
+    const d3 g_ua1 = -g_dv, g_ub1 = g_dv;
+    gva1 += g_ua1;
+    gwa1 += dcross(ra, g_ua1);
+    gc.ra += dcross(g_ua1, D(wa1));
+    gvb1 += g_ub1;
+    gwb1 += dcross(rb, g_ub1);
+    gc.rb += dcross(g_ub1, D(wb1));
+    // wa1 = wa - A(xa); wb1 = wb + B(xb); xa = ra x imp
+    d3 gi_va = gva1, gi_wa = gwa1, gi_vb = gvb1, gi_wb = gwb1, g_imp = dz();
+    const d3 g_xa = inv_I_bwd(RA, IA, D(xa), -gwa1, gRa);
+    const d3 g_xb = inv_I_bwd(RB, IB, D(xb), gwb1, gRb);
+    const d3 impd = D(imp);
+    gc.ra += dcross(impd, g_xa);
+    g_imp += dcross(g_xa, ra);
+    gc.rb += dcross(impd, g_xb);
+    g_imp += dcross(g_xb, rb);
     // va1 = va - ima imp; vb1 = vb + imb imp
-    acc_s(g_imp, -A.ima, gva1);
-    acc_s(g_imp, B.ima, gvb1);
+    g_imp += (-ima) * gva1;
+    g_imp += imb * gvb1;
     // imp = d n
-    const float g_d = dot(g_imp, c.n);
-    acc_s(gc.n, d, g_imp);
+    const double g_d = ddot(g_imp, n);
+    gc.n += double(d) * g_imp;
     // d = l1 - lam; l1 = max(s1, 0); s1 = lam + d0
     g_l1 += g_d;
-    float gi_lam = -g_d;
-    const float g_s1 = s1 < 0.f ? 0.f : g_l1;
+    double gi_lam = -g_d;
+    const double g_s1 = s1 < 0.f ? 0.0 : g_l1;
     gi_lam += g_s1;
     // d0 = (-vn + bias) / kn
-    const float g_vn = -g_s1 / c.kn;
-    gc.bias += g_s1 / c.kn;
-    gc.kn += -g_s1 * d0 / c.kn;
+    const double knd = c.kn;
+    const double g_vn = -g_s1 / knd;
+    gc.bias += g_s1 / knd;
+    gc.kn += -g_s1 * double(d0) / knd;
     // vn = dvn·n; dvn = ub - ua; ua = va + wa x ra
-    acc_s(gc.n, g_vn, dvn);
-    const f3 g_ub = scale(g_vn, c.n), g_ua = neg(g_ub);
-    acc(gi_va, g_ua);
-    acc(gi_wa, cross(c.ra, g_ua));
-    acc(gc.ra, cross(g_ua, wa));
-    acc(gi_vb, g_ub);
-    acc(gi_wb, cross(c.rb, g_ub));
-    acc(gc.rb, cross(g_ub, wb));
+    gc.n += g_vn * D(dvn);
+    const d3 g_ub = g_vn * n, g_ua = -g_ub;
+    gi_va += g_ua;
+    gi_wa += dcross(ra, g_ua);
+    gc.ra += dcross(g_ua, D(wa));
+    gi_vb += g_ub;
+    gi_wb += dcross(rb, g_ub);
+    gc.rb += dcross(g_ub, D(wb));
     // a fixed body's state persists: its incoming gradient passes through
-    Gva = A.fixed ? add(Gva, gi_va) : gi_va;
-    Gwa = A.fixed ? add(Gwa, gi_wa) : gi_wa;
-    Gvb = B.fixed ? add(Gvb, gi_vb) : gi_vb;
-    Gwb = B.fixed ? add(Gwb, gi_wb) : gi_wb;
+    Gva = A.fixed ? Gva + gi_va : gi_va;
+    Gwa = A.fixed ? Gwa + gi_wa : gi_wa;
+    Gvb = B.fixed ? Gvb + gi_vb : gi_vb;
+    Gwb = B.fixed ? Gwb + gi_wb : gi_wb;
     glam = gi_lam;
 }
 
 __device__ __forceinline__ f3 hull_vert(const World& w, uint32_t vs, uint32_t i) {
-    return i == kNone ? z3() : ld3(w.hull, vs + i);
+    return i == kNone ? mk(0.f, 0.f, 0.f) : ld3(w.hull, vs + i);
 }
 
 // dL/d (positions, rotations) of one contact's normal, depth and point,
 // through the taped supporting vertices (physics.comp:224-247, 346-365,
-// 376-387).
+// 376-387).  The support points are recomputed in FP32 as the narrowphase
+// computed them; the derivatives are FP64.
 __device__ void contact_geom_bwd(const World& w, const Consts& k, const AdjScratch& a, uint32_t c,
-                                 uint32_t ba, uint32_t bb, f3 g_n, float g_pen, f3 g_cp) {
+                                 uint32_t ba, uint32_t bb, d3 g_n, double g_pen, d3 g_cp) {
     const uint4 t0 = a.ctape[size_t(c) * 2], t1 = a.ctape[size_t(c) * 2 + 1];
-    const f3 pA = ld3(w.pos, ba), pB = ld3(w.pos, bb);
-    const m3 RA = quat_to_mat(w.quat, ba), RB = quat_to_mat(w.quat, bb);
+    const f3 pAf = ld3(w.pos, ba), pBf = ld3(w.pos, bb);
+    const m3 RAf = quat_to_mat(w.quat, ba), RBf = quat_to_mat(w.quat, bb);
     const uint32_t vsA = w.hull_range[size_t(ba) * 2], vsB = w.hull_range[size_t(bb) * 2];
-    f3 hA[4], hB[4], sa[4], sb[4], gsa[4], gsb[4], v[4], gv[4];
+    f3 hA[4], hB[4], saf[4], sbf[4], vf[4];
+    d3 gsa[4], gsb[4], gv[4];
     const uint32_t ia[4] = {kNone, t0.y, t0.w, t1.y};
     const uint32_t ib[4] = {kNone, t0.z, t1.x, t1.z};
     for (int i = 0; i < 4; ++i) {
         hA[i] = hull_vert(w, vsA, ia[i]);
         hB[i] = hull_vert(w, vsB, ib[i]);
-        sa[i] = add(pA, mul(RA, hA[i]));
-        sb[i] = add(pB, mul(RB, hB[i]));
-        v[i] = sub(sa[i], sb[i]);
-        gsa[i] = gsb[i] = gv[i] = z3();
+        saf[i] = add(pAf, mul(RAf, hA[i]));
+        sbf[i] = add(pBf, mul(RBf, hB[i]));
+        vf[i] = sub(saf[i], sbf[i]);
+        gsa[i] = gsb[i] = gv[i] = dz();
     }
-    f3 gpA = z3(), gpB = z3();
+    d3 gpA = dz(), gpB = dz();
     if (t0.x == 2u) {  // segment case: depth = |v1|, n = v1/|v1|, cp = (s1a + s1b)/2
-        const float l = length(v[1]);
-        const f3 n = divs(v[1], l);
-        f3 g1 = scale(g_pen, n);
-        acc_s(g1, 1.f / l, sub(g_n, scale(dot(n, g_n), n)));
-        gsa[1] = add(scale(0.5f, g_cp), g1);
-        gsb[1] = sub(scale(0.5f, g_cp), g1);
+        const d3 v1 = D(vf[1]);
+        const double l = sqrt(ddot(v1, v1));
+        const d3 n = (1.0 / l) * v1;
+        d3 g1 = g_pen * n;
+        g1 += (1.0 / l) * (g_n - ddot(n, g_n) * n);
+        gsa[1] = 0.5 * g_cp + g1;
+        gsb[1] = 0.5 * g_cp - g1;
     } else {  // portal: n = normalize((v2-v1)x(v3-v1)), depth = n·v1, cp = find_pos
-        f3 v0 = sub(pA, pB);
-        if (fabsf(v0.x) < k.eps && fabsf(v0.y) < k.eps && fabsf(v0.z) < k.eps) v0.x += 10.0f * k.eps;
-        v[0] = v0;
-        sa[0] = pA;
-        sb[0] = pB;
-        const f3 e1 = sub(v[2], v[1]), e2 = sub(v[3], v[1]);
-        const f3 cr = cross(e1, e2);
-        const float cl = length(cr);
-        const f3 n = divs(cr, cl);
-        f3 g_nn = g_n;
-        acc_s(g_nn, g_pen, v[1]);
-        acc_s(gv[1], g_pen, n);
-        // contact point
-        float b[4];
-        b[0] = dot(cross(v[1], v[2]), v[3]);
-        b[1] = -dot(cross(v[0], v[2]), v[3]);
-        b[2] = dot(cross(v[0], v[1]), v[3]);
-        b[3] = -dot(cross(v[0], v[1]), v[2]);
-        float sum = b[0] + b[1] + b[2] + b[3];
-        const bool fallback = fabsf(sum) < k.eps;
-        if (fallback) {
-            b[0] = 0.f;
-            b[1] = dot(cross(v[2], v[3]), n);
-            b[2] = dot(cross(v[3], v[1]), n);
-            b[3] = dot(cross(v[1], v[2]), n);
-            sum = b[0] + b[1] + b[2] + b[3];
-        }
-        f3 P = z3();
-        for (int i = 0; i < 4; ++i) P = add(P, scale(b[i], add(sa[i], sb[i])));
-        const float kk = 0.5f / sum;
-        const f3 gP = scale(kk, g_cp);
-        const float g_sum = -0.5f / (sum * sum) * dot(g_cp, P);
-        float gb[4];
+        f3 v0f = sub(pAf, pBf);
+        if (fabsf(v0f.x) < k.eps && fabsf(v0f.y) < k.eps && fabsf(v0f.z) < k.eps)
+            v0f.x += 10.0f * k.eps;
+        vf[0] = v0f;
+        saf[0] = pAf;
+        sbf[0] = pBf;
+        d3 v[4], sa[4], sb[4];
         for (int i = 0; i < 4; ++i) {
-            gb[i] = dot(gP, sa[i]) + dot(gP, sb[i]) + g_sum;
-            acc_s(gsa[i], b[i], gP);
-            acc_s(gsb[i], b[i], gP);
+            v[i] = D(vf[i]);
+            sa[i] = D(saf[i]);
+            sb[i] = D(sbf[i]);
+        }
+        const d3 e1 = v[2] - v[1], e2 = v[3] - v[1];
+        const d3 cr = dcross(e1, e2);
+        const double cl = sqrt(ddot(cr, cr));
+        const d3 n = (1.0 / cl) * cr;
+        d3 g_nn = g_n;
+        g_nn += g_pen * v[1];
+        gv[1] += g_pen * n;
+        // contact point: the forward's fallback test (FP32, find_pos)
+        const float fsum = dot(cross(vf[1], vf[2]), vf[3]) + -dot(cross(vf[0], vf[2]), vf[3]) +
+                           dot(cross(vf[0], vf[1]), vf[3]) + -dot(cross(vf[0], vf[1]), vf[2]);
+        const bool fallback = fabsf(fsum) < k.eps;
+        double b[4];
+        if (!fallback) {
+            b[0] = ddot(dcross(v[1], v[2]), v[3]);
+            b[1] = -ddot(dcross(v[0], v[2]), v[3]);
+            b[2] = ddot(dcross(v[0], v[1]), v[3]);
+            b[3] = -ddot(dcross(v[0], v[1]), v[2]);
+        } else {
+            b[0] = 0.0;
+            b[1] = ddot(dcross(v[2], v[3]), n);
+            b[2] = ddot(dcross(v[3], v[1]), n);
+            b[3] = ddot(dcross(v[1], v[2]), n);
+        }
+        const double sum = b[0] + b[1] + b[2] + b[3];
+        d3 P = dz();
+        for (int i = 0; i < 4; ++i) P += b[i] * (sa[i] + sb[i]);
+        const d3 gP = (0.5 / sum) * g_cp;
+        const double g_sum = -0.5 / (sum * sum) * ddot(g_cp, P);
+        double gb[4];
+        for (int i = 0; i < 4; ++i) {
+            gb[i] = ddot(gP, sa[i]) + ddot(gP, sb[i]) + g_sum;
+            gsa[i] += b[i] * gP;
+            gsb[i] += b[i] * gP;
         }
         if (!fallback) {
             // triple products [a,b,c] = (a x b)·c: d/da = b x c, d/db = c x a, d/dc = a x b
-            acc_s(gv[1], gb[0], cross(v[2], v[3]));
-            acc_s(gv[2], gb[0], cross(v[3], v[1]));
-            acc_s(gv[3], gb[0], cross(v[1], v[2]));
-            acc_s(gv[0], -gb[1], cross(v[2], v[3]));
-            acc_s(gv[2], -gb[1], cross(v[3], v[0]));
-            acc_s(gv[3], -gb[1], cross(v[0], v[2]));
-            acc_s(gv[0], gb[2], cross(v[1], v[3]));
-            acc_s(gv[1], gb[2], cross(v[3], v[0]));
-            acc_s(gv[3], gb[2], cross(v[0], v[1]));
-            acc_s(gv[0], -gb[3], cross(v[1], v[2]));
-            acc_s(gv[1], -gb[3], cross(v[2], v[0]));
-            acc_s(gv[2], -gb[3], cross(v[0], v[1]));
+            gv[1] += gb[0] * dcross(v[2], v[3]);
+            gv[2] += gb[0] * dcross(v[3], v[1]);
+            gv[3] += gb[0] * dcross(v[1], v[2]);
+            gv[0] += (-gb[1]) * dcross(v[2], v[3]);
+            gv[2] += (-gb[1]) * dcross(v[3], v[0]);
+            gv[3] += (-gb[1]) * dcross(v[0], v[2]);
+            gv[0] += gb[2] * dcross(v[1], v[3]);
+            gv[1] += gb[2] * dcross(v[3], v[0]);
+            gv[3] += gb[2] * dcross(v[0], v[1]);
+            gv[0] += (-gb[3]) * dcross(v[1], v[2]);
+            gv[1] += (-gb[3]) * dcross(v[2], v[0]);
+            gv[2] += (-gb[3]) * dcross(v[0], v[1]);
         } else {
             // b1 = (v2 x v3)·n, b2 = (v3 x v1)·n, b3 = (v1 x v2)·n
-            acc_s(gv[2], gb[1], cross(v[3], n));
-            acc_s(gv[3], gb[1], cross(n, v[2]));
-            acc_s(g_nn, gb[1], cross(v[2], v[3]));
-            acc_s(gv[3], gb[2], cross(v[1], n));
-            acc_s(gv[1], gb[2], cross(n, v[3]));
-            acc_s(g_nn, gb[2], cross(v[3], v[1]));
-            acc_s(gv[1], gb[3], cross(v[2], n));
-            acc_s(gv[2], gb[3], cross(n, v[1]));
-            acc_s(g_nn, gb[3], cross(v[1], v[2]));
+            gv[2] += gb[1] * dcross(v[3], n);
+            gv[3] += gb[1] * dcross(n, v[2]);
+            g_nn += gb[1] * dcross(v[2], v[3]);
+            gv[3] += gb[2] * dcross(v[1], n);
+            gv[1] += gb[2] * dcross(n, v[3]);
+            g_nn += gb[2] * dcross(v[3], v[1]);
+            gv[1] += gb[3] * dcross(v[2], n);
+            gv[2] += gb[3] * dcross(n, v[1]);
+            g_nn += gb[3] * dcross(v[1], v[2]);
         }
         // n = cr / |cr|; cr = e1 x e2
-        const f3 g_cr = scale(1.f / cl, sub(g_nn, scale(dot(n, g_nn), n)));
-        const f3 g_e1 = cross(e2, g_cr), g_e2 = cross(g_cr, e1);
-        acc(gv[2], g_e1);
-        acc(gv[3], g_e2);
-        gv[1] = sub(gv[1], add(g_e1, g_e2));
+        const d3 g_cr = (1.0 / cl) * (g_nn - ddot(n, g_nn) * n);
+        const d3 g_e1 = dcross(e2, g_cr), g_e2 = dcross(g_cr, e1);
+        gv[2] += g_e1;
+        gv[3] += g_e2;
+        gv[1] = gv[1] - (g_e1 + g_e2);
         // v0 = pA - pB; s0a = pA; s0b = pB
-        acc(gpA, add(gv[0], gsa[0]));
-        acc(gpB, sub(gsb[0], gv[0]));
+        gpA += gv[0] + gsa[0];
+        gpB += gsb[0] - gv[0];
         for (int i = 1; i < 4; ++i) {
-            acc(gsa[i], gv[i]);
-            gsb[i] = sub(gsb[i], gv[i]);
+            gsa[i] += gv[i];
+            gsb[i] = gsb[i] - gv[i];
         }
     }
     // s_ia = pA + RA h_ia; s_ib = pB + RB h_ib (i = 1..3)
-    m3 gRA = m3zero(), gRB = m3zero();
+    dm3 gRA = dm3zero(), gRB = dm3zero();
     for (int i = 1; i < 4; ++i) {
-        acc(gpA, gsa[i]);
-        acc(gpB, gsb[i]);
-        gRA.c0 = add(gRA.c0, scale(hA[i].x, gsa[i]));
-        gRA.c1 = add(gRA.c1, scale(hA[i].y, gsa[i]));
-        gRA.c2 = add(gRA.c2, scale(hA[i].z, gsa[i]));
-        gRB.c0 = add(gRB.c0, scale(hB[i].x, gsb[i]));
-        gRB.c1 = add(gRB.c1, scale(hB[i].y, gsb[i]));
-        gRB.c2 = add(gRB.c2, scale(hB[i].z, gsb[i]));
+        gpA += gsa[i];
+        gpB += gsb[i];
+        const d3 ha = D(hA[i]), hb = D(hB[i]);
+        gRA.c0 += ha.x * gsa[i];
+        gRA.c1 += ha.y * gsa[i];
+        gRA.c2 += ha.z * gsa[i];
+        gRB.c0 += hb.x * gsb[i];
+        gRB.c1 += hb.y * gsb[i];
+        gRB.c2 += hb.z * gsb[i];
     }
-    add3(a.gp, ba, gpA);
-    add3(a.gp, bb, gpB);
-    add_m3(a.gR, ba, gRA);
-    add_m3(a.gR, bb, gRB);
+    addd3(a.gp, ba, gpA);
+    addd3(a.gp, bb, gpB);
+    add_dm3(a.gR, ba, gRA);
+    add_dm3(a.gR, bb, gRB);
 }
 
 constexpr uint32_t kAdjWarps = 4;
@@ -434,9 +494,9 @@ __global__ void __launch_bounds__(kAdjWarps * 32)
         for (int j = 0; j < 3; ++j) {
             a.vw[size_t(b) * 6 + j] = w.vel[size_t(b) * 3 + j];
             a.vw[size_t(b) * 6 + 3 + j] = w.omega[size_t(b) * 3 + j];
-            a.gp[size_t(b) * 3 + j] = 0.f;
+            a.gp[size_t(b) * 3 + j] = 0.0;
         }
-        for (int j = 0; j < 9; ++j) a.gR[size_t(b) * 9 + j] = 0.f;
+        for (int j = 0; j < 9; ++j) a.gR[size_t(b) * 9 + j] = 0.0;
     }
     // ---- contact constants (physics.comp:504-521, 533-546) ----
     for (uint32_t c = c0 + lane; c < c1; c += 32) {
@@ -458,8 +518,8 @@ __global__ void __launch_bounds__(kAdjWarps * 32)
         p.mu = sqrtf(w.friction[ga] * w.friction[gb]);
         st_par(a.par, c, p);
         a.lam[c] = 0.f;
-        a.glam[c] = 0.f;
-        st_grad(a.gc, c, CGrad{z3(), z3(), z3(), 0.f, 0.f, 0.f});
+        a.glam[c] = 0.0;
+        st_grad(a.gc, c, CGrad{dz(), dz(), dz(), 0.0, 0.0, 0.0});
     }
     __syncwarp();
 
@@ -495,44 +555,46 @@ __global__ void __launch_bounds__(kAdjWarps * 32)
 
     // ---- integration (physics.comp:586-604), reversed ----
     for (uint32_t b = b0 + lane; b < b1; b += 32) {
-        const f3 Gp1 = ld3(g.pos, b), Gv1 = ld3(g.vel, b), Gw1 = ld3(g.omega, b);
-        float Gq1[4] = {g.quat[size_t(b) * 4], g.quat[size_t(b) * 4 + 1], g.quat[size_t(b) * 4 + 2],
-                        g.quat[size_t(b) * 4 + 3]};
-        f3 Gv = Gv1, Gw = Gw1;
-        float Gq[4] = {Gq1[0], Gq1[1], Gq1[2], Gq1[3]};
+        const d3 Gp1 = ldd3(g.pos, b), Gv1 = ldd3(g.vel, b), Gw1 = ldd3(g.omega, b);
+        const double Gq1[4] = {g.quat[size_t(b) * 4], g.quat[size_t(b) * 4 + 1],
+                               g.quat[size_t(b) * 4 + 2], g.quat[size_t(b) * 4 + 3]};
+        d3 Gv = Gv1, Gw = Gw1;
+        double Gq[4] = {Gq1[0], Gq1[1], Gq1[2], Gq1[3]};
         if (w.inv_mass[b] > 0.0f) {
-            acc_s(Gv, dt, Gp1);  // pos += vel dt
+            Gv += double(dt) * Gp1;  // pos += vel dt
             const float ox = a.vw[size_t(b) * 6 + 3], oy = a.vw[size_t(b) * 6 + 4],
                         oz = a.vw[size_t(b) * 6 + 5];
             const float qx = w.quat[size_t(b) * 4], qy = w.quat[size_t(b) * 4 + 1],
                         qz = w.quat[size_t(b) * 4 + 2], qw = w.quat[size_t(b) * 4 + 3];
             const float dx = ox * qw + oy * qz - oz * qy;
             const float dy = -ox * qz + oy * qw + oz * qx;
-            const float dz = ox * qy - oy * qx + oz * qw;
+            const float dzq = ox * qy - oy * qx + oz * qw;
             const float dw = -ox * qx - oy * qy - oz * qz;
-            const float ux = qx + 0.5f * dx * dt, uy = qy + 0.5f * dy * dt, uz = qz + 0.5f * dz * dt,
-                        uw = qw + 0.5f * dw * dt;
+            const float ux = qx + 0.5f * dx * dt, uy = qy + 0.5f * dy * dt,
+                        uz = qz + 0.5f * dzq * dt, uw = qw + 0.5f * dw * dt;
             const float l = sqrtf(ux * ux + uy * uy + uz * uz + uw * uw);
-            float gu[4] = {Gq1[0], Gq1[1], Gq1[2], Gq1[3]};
+            double gu[4] = {Gq1[0], Gq1[1], Gq1[2], Gq1[3]};
             if (l > 1e-8f) {  // q' = u / |u|
-                const float nq[4] = {ux / l, uy / l, uz / l, uw / l};
-                const float dp = nq[0] * Gq1[0] + nq[1] * Gq1[1] + nq[2] * Gq1[2] + nq[3] * Gq1[3];
-                for (int j = 0; j < 4; ++j) gu[j] = (Gq1[j] - nq[j] * dp) / l;
+                const double ld = l;
+                const double nq[4] = {ux / ld, uy / ld, uz / ld, uw / ld};
+                const double dp = nq[0] * Gq1[0] + nq[1] * Gq1[1] + nq[2] * Gq1[2] + nq[3] * Gq1[3];
+                for (int j = 0; j < 4; ++j) gu[j] = (Gq1[j] - nq[j] * dp) / ld;
             }
-            const float h = 0.5f * dt;
-            const float gdx = h * gu[0], gdy = h * gu[1], gdz = h * gu[2], gdw = h * gu[3];
-            Gq[0] = gu[0] + gdy * oz - gdz * oy - gdw * ox;
-            Gq[1] = gu[1] - gdx * oz + gdz * ox - gdw * oy;
-            Gq[2] = gu[2] + gdx * oy - gdy * ox - gdw * oz;
-            Gq[3] = gu[3] + gdx * ox + gdy * oy + gdz * oz;
-            Gw.x += gdx * qw - gdy * qz + gdz * qy - gdw * qx;
-            Gw.y += gdx * qz + gdy * qw - gdz * qx - gdw * qy;
-            Gw.z += -gdx * qy + gdy * qx + gdz * qw - gdw * qz;
+            const double h = 0.5 * double(dt);
+            const double gdx = h * gu[0], gdy = h * gu[1], gdz = h * gu[2], gdw = h * gu[3];
+            const double Ox = ox, Oy = oy, Oz = oz, Qx = qx, Qy = qy, Qz = qz, Qw = qw;
+            Gq[0] = gu[0] + gdy * Oz - gdz * Oy - gdw * Ox;
+            Gq[1] = gu[1] - gdx * Oz + gdz * Ox - gdw * Oy;
+            Gq[2] = gu[2] + gdx * Oy - gdy * Ox - gdw * Oz;
+            Gq[3] = gu[3] + gdx * Ox + gdy * Oy + gdz * Oz;
+            Gw.x += gdx * Qw - gdy * Qz + gdz * Qy - gdw * Qx;
+            Gw.y += gdx * Qz + gdy * Qw - gdz * Qx - gdw * Qy;
+            Gw.z += -gdx * Qy + gdy * Qx + gdz * Qw - gdw * Qz;
         }
-        st3(a.gv, b, Gv);
-        st3(a.gw, b, Gw);
+        std3(a.gv, b, Gv);
+        std3(a.gw, b, Gw);
         for (int j = 0; j < 4; ++j) a.gq[size_t(b) * 4 + j] = Gq[j];
-        for (int j = 0; j < 3; ++j) a.gp[size_t(b) * 3 + j] = (&Gp1.x)[j];
+        std3(a.gp, b, Gp1);
     }
     __syncwarp();
 
@@ -544,21 +606,22 @@ __global__ void __launch_bounds__(kAdjWarps * 32)
                 const Body A = load_body(w, ba), B = load_body(w, bb);
                 if (A.ima == 0.0f && B.ima == 0.0f) continue;
                 const float* t = a.tape + (size_t(c0) * iters + size_t(it) * ncb + (c - c0)) * 13;
-                f3 Gva = ld3(a.gv, ba), Gwa = ld3(a.gw, ba), Gvb = ld3(a.gv, bb), Gwb = ld3(a.gw, bb);
-                float glam = a.glam[c];
+                d3 Gva = ldd3(a.gv, ba), Gwa = ldd3(a.gw, ba), Gvb = ldd3(a.gv, bb),
+                   Gwb = ldd3(a.gw, bb);
+                double glam = a.glam[c];
                 CGrad gc = ld_grad(a.gc, c);
-                m3 gRa = m3zero(), gRb = m3zero();
+                dm3 gRa = dm3zero(), gRb = dm3zero();
                 update_bwd(A, B, ld_par(a.par, c), mk(t[0], t[1], t[2]), mk(t[3], t[4], t[5]),
                            mk(t[6], t[7], t[8]), mk(t[9], t[10], t[11]), t[12], Gva, Gwa, Gvb, Gwb,
                            glam, gc, gRa, gRb);
-                st3(a.gv, ba, Gva);
-                st3(a.gw, ba, Gwa);
-                st3(a.gv, bb, Gvb);
-                st3(a.gw, bb, Gwb);
+                std3(a.gv, ba, Gva);
+                std3(a.gw, ba, Gwa);
+                std3(a.gv, bb, Gvb);
+                std3(a.gw, bb, Gwb);
                 a.glam[c] = glam;
                 st_grad(a.gc, c, gc);
-                add_m3(a.gR, ba, gRa);
-                add_m3(a.gR, bb, gRb);
+                add_dm3(a.gR, ba, gRa);
+                add_dm3(a.gR, bb, gRb);
             }
         // ---- contact constants and contact geometry, reversed ----
         for (uint32_t c = c0; c < c1; ++c) {
@@ -567,45 +630,48 @@ __global__ void __launch_bounds__(kAdjWarps * 32)
             const Body A = load_body(w, ba), B = load_body(w, bb);
             const CParams p = ld_par(a.par, c);
             CGrad gc = ld_grad(a.gc, c);
-            m3 gRa = m3zero(), gRb = m3zero();
-            // kn = ima + imb + ran·A(ran) + rbn·A(rbn); ran = ra x n
-            const f3 ran = cross(p.ra, p.n), rbn = cross(p.rb, p.n);
-            const f3 g_ran = scale(2.f * gc.kn, apply_inv_I(A.R, A.I, ran));
-            const f3 g_rbn = scale(2.f * gc.kn, apply_inv_I(B.R, B.I, rbn));
-            inv_I_bwd(A.R, A.I, ran, scale(gc.kn, ran), gRa);
-            inv_I_bwd(B.R, B.I, rbn, scale(gc.kn, rbn), gRb);
-            acc(gc.ra, cross(p.n, g_ran));
-            acc(gc.n, cross(g_ran, p.ra));
-            acc(gc.rb, cross(p.n, g_rbn));
-            acc(gc.n, cross(g_rbn, p.rb));
+            dm3 gRa = dm3zero(), gRb = dm3zero();
+            const dm3 RA = DM(A.R), RB = DM(B.R);
+            const d3 IA = D(A.I), IB = D(B.I), n = D(p.n), ra = D(p.ra), rb = D(p.rb);
+            // kn = ima + imb + ran·A(ran) + rbn·B(rbn); ran = ra x n
+            const d3 ran = D(cross(p.ra, p.n)), rbn = D(cross(p.rb, p.n));
+            const d3 g_ran = (2.0 * gc.kn) * dapply(RA, IA, ran);
+            const d3 g_rbn = (2.0 * gc.kn) * dapply(RB, IB, rbn);
+            inv_I_bwd(RA, IA, ran, gc.kn * ran, gRa);
+            inv_I_bwd(RB, IB, rbn, gc.kn * rbn, gRb);
+            gc.ra += dcross(n, g_ran);
+            gc.n += dcross(g_ran, ra);
+            gc.rb += dcross(n, g_rbn);
+            gc.n += dcross(g_rbn, rb);
             // bias = baum max(pen - slop, 0)/dt + e max(-vn0, 0)
             const float pen = w.c_pen[c];
-            const float g_pen = (pen - k.slop < 0.f) ? 0.f : gc.bias * k.baumgarte / dt;
+            const double g_pen =
+                (pen - k.slop < 0.f) ? 0.0 : gc.bias * double(k.baumgarte) / double(dt);
             const float e = gmax(w.restitution[ga], w.restitution[gb]);
             const f3 va0 = add(ld3(w.vel, ba), cross(ld3(w.omega, ba), p.ra));
             const f3 vb0 = add(ld3(w.vel, bb), cross(ld3(w.omega, bb), p.rb));
             const float vn0 = dot(sub(vb0, va0), p.n);
-            const float g_vn0 = (-vn0 < 0.f) ? 0.f : -e * gc.bias;
-            acc_s(gc.n, g_vn0, sub(vb0, va0));
-            const f3 g_ub0 = scale(g_vn0, p.n), g_ua0 = neg(g_ub0);
-            add3(a.gv, ba, g_ua0);
-            add3(a.gw, ba, cross(p.ra, g_ua0));
-            acc(gc.ra, cross(g_ua0, ld3(w.omega, ba)));
-            add3(a.gv, bb, g_ub0);
-            add3(a.gw, bb, cross(p.rb, g_ub0));
-            acc(gc.rb, cross(g_ub0, ld3(w.omega, bb)));
+            const double g_vn0 = (-vn0 < 0.f) ? 0.0 : -double(e) * gc.bias;
+            gc.n += g_vn0 * D(sub(vb0, va0));
+            const d3 g_ub0 = g_vn0 * n, g_ua0 = -g_ub0;
+            addd3(a.gv, ba, g_ua0);
+            addd3(a.gw, ba, dcross(ra, g_ua0));
+            gc.ra += dcross(g_ua0, D(ld3(w.omega, ba)));
+            addd3(a.gv, bb, g_ub0);
+            addd3(a.gw, bb, dcross(rb, g_ub0));
+            gc.rb += dcross(g_ub0, D(ld3(w.omega, bb)));
             // mu = sqrt(fa fb)
             if (p.mu > 0.f) {
-                const float fa = w.friction[ga], fb = w.friction[gb];
-                g.friction[ga] += gc.mu * fb / (2.f * p.mu);
-                g.friction[gb] += gc.mu * fa / (2.f * p.mu);
+                const double fa = w.friction[ga], fb = w.friction[gb], mu = p.mu;
+                g.friction[ga] += gc.mu * fb / (2.0 * mu);
+                g.friction[gb] += gc.mu * fa / (2.0 * mu);
             }
             // ra = cp - pos_a; rb = cp - pos_b
-            const f3 g_cp = add(gc.ra, gc.rb);
-            add3(a.gp, ba, neg(gc.ra));
-            add3(a.gp, bb, neg(gc.rb));
-            add_m3(a.gR, ba, gRa);
-            add_m3(a.gR, bb, gRb);
+            const d3 g_cp = gc.ra + gc.rb;
+            addd3(a.gp, ba, -gc.ra);
+            addd3(a.gp, bb, -gc.rb);
+            add_dm3(a.gR, ba, gRa);
+            add_dm3(a.gR, bb, gRb);
             contact_geom_bwd(w, k, a, c, ba, bb, gc.n, g_pen, g_cp);
         }
     }
@@ -613,18 +679,18 @@ __global__ void __launch_bounds__(kAdjWarps * 32)
 
     // ---- rotations -> quaternions, gravity (physics.comp:418-428), reversed
     for (uint32_t b = b0 + lane; b < b1; b += 32) {
-        float gq[4];
+        double gq[4];
         quat_bwd(w.quat[size_t(b) * 4], w.quat[size_t(b) * 4 + 1], w.quat[size_t(b) * 4 + 2],
                  w.quat[size_t(b) * 4 + 3], a.gR + size_t(b) * 9, gq);
         for (int j = 0; j < 4; ++j) g.quat[size_t(b) * 4 + j] = a.gq[size_t(b) * 4 + j] + gq[j];
-        f3 Gv = ld3(a.gv, b), Gw = ld3(a.gw, b);
+        d3 Gv = ldd3(a.gv, b), Gw = ldd3(a.gw, b);
         if (w.inv_mass[b] > 0.0f) {
-            Gv = scale(k.lin_damp, Gv);
-            Gw = scale(k.ang_damp, Gw);
+            Gv = double(k.lin_damp) * Gv;
+            Gw = double(k.ang_damp) * Gw;
         }
-        st3(g.vel, b, Gv);
-        st3(g.omega, b, Gw);
-        st3(g.pos, b, ld3(a.gp, b));
+        std3(g.vel, b, Gv);
+        std3(g.omega, b, Gw);
+        std3(g.pos, b, ldd3(a.gp, b));
     }
 }
 

@@ -1,14 +1,16 @@
 """Differentiable rollouts of the physics step (reverse mode).
 
-    buf = Data.rollout(n=32, seed=0).upload("cuda:0")
+    buf = Data.rollout(num_scenes=32, bodies=64).upload("cuda:0")
     ph = Physics(buf, make_params(pgs_iterations=30))
-    vel0 = buf.tensors["body_vel"][: 3 * n].clone().requires_grad_()
+    n = buf.num_bodies
+    vel0 = buf.tensors["body_vel"][: 3 * n].clone().reshape(n, 3).requires_grad_()
     pos, quat, vel, omega = rollout(ph, vel0=vel0, frames=4)
     loss(pos).backward()          # vel0.grad: dL/d initial velocities
 
 The forward runs the regular step one substep at a time (a frame of k
-substeps is exactly k calls of one substep with dt / k) and keeps a
-checkpoint of (pos, quat, vel, omega) before each.  The backward restores
+substeps is exactly k calls of one substep with dt / k), ordered on the
+current stream, and keeps a checkpoint of (pos, quat, vel, omega) before
+each.  The backward restores
 each checkpoint in reverse order and calls seevr_physics_adjoint_substep,
 which recomputes that substep's contacts and PGS sweep on the GPU and
 propagates dL/d(state) back through it, accumulating dL/d friction.
@@ -53,12 +55,18 @@ class _Rollout:
                     for v, x in zip(views, ins):
                         v.copy_(x.detach().reshape(-1))
                     t["geom_friction"][:nb].copy_(friction.detach().reshape(-1))
+                    # checkpoints and substeps stay ordered on one stream,
+                    # with no host round trip until the end
+                    stream = torch.cuda.current_stream(ph.buffers.device)
                     ckpt = []
                     for _ in range(steps):
                         ckpt.append(torch.cat([v.clone() for v in views]))
-                        torch.cuda.current_stream(ph.buffers.device).synchronize()
-                        ph.step(nb, 0, nhv, 1, sub_dt, gravity)
+                        ph.step_async(nb, 0, nhv, 1, sub_dt, gravity, frames=1, stream=stream)
                     outs = [v.clone().reshape(x.shape) for v, x in zip(views, ins)]
+                    torch.cuda.synchronize(ph.buffers.device)
+                    if ph.read_flags() & (L.DEVICE_FLAG_PAIR_OVERFLOW | L.DEVICE_FLAG_CONTACT_OVERFLOW):
+                        raise L.SeevrError(L.ERR_CAPACITY,
+                                           "pairs or contacts exceeded the caps during the rollout")
                 ctx.ph, ctx.cfg, ctx.ckpt = ph, cfg, ckpt
                 ctx.shapes = [x.shape for x in ins] + [friction.shape]
                 return tuple(outs)
@@ -69,11 +77,12 @@ class _Rollout:
                 nb, nhv, steps, sub_dt, gravity = ctx.cfg
                 t = ph.buffers.tensors
                 dev = ph.buffers.device
+                # the reverse pass carries FP64 gradients from substep to substep
                 g = []
                 for gx, (name, k) in zip((gpos, gquat, gvel, gomega), _names()):
-                    g.append(torch.zeros(nb * k, dtype=torch.float32, device=dev) if gx is None
-                             else gx.detach().reshape(-1).to(torch.float32).contiguous().clone())
-                gf = torch.zeros(max(nb, 1), dtype=torch.float32, device=dev)
+                    g.append(torch.zeros(nb * k, dtype=torch.float64, device=dev) if gx is None
+                             else gx.detach().reshape(-1).to(torch.float64).contiguous().clone())
+                gf = torch.zeros(max(nb, 1), dtype=torch.float64, device=dev)
                 gr = L.AdjointGrads(g[0].data_ptr(), g[1].data_ptr(), g[2].data_ptr(),
                                     g[3].data_ptr(), gf.data_ptr())
                 views = [t[name][: nb * k] for name, k in _names()]
@@ -87,8 +96,9 @@ class _Rollout:
                             ph._h, nb, nhv, sub_dt, L.fptr(gravity, 3), C.byref(gr)))
                 ctx.ckpt = None
                 sh = ctx.shapes
-                return (None, None, g[0].reshape(sh[0]), g[1].reshape(sh[1]),
-                        g[2].reshape(sh[2]), g[3].reshape(sh[3]), gf[:nb].reshape(sh[4]))
+                f = lambda x, shape: x.reshape(shape).to(torch.float32)
+                return (None, None, f(g[0], sh[0]), f(g[1], sh[1]), f(g[2], sh[2]),
+                        f(g[3], sh[3]), f(gf[:nb], sh[4]))
 
         cls.fn = Fn
         return Fn
@@ -105,12 +115,10 @@ def rollout(ph: Physics, pos0=None, quat0=None, vel0=None, omega0=None, friction
     """Run `frames` frames of `substeps` substeps from the given initial state
     (torch tensors on the handle's device; None = the bound buffers' current
     values) and return the final (pos, quat, vel, omega), differentiable
-    with respect to all five inputs.  The handle must run synchronously
-    (no FLAG_NO_SYNC)."""
+    with respect to all five inputs.  Raises SeevrError (ERR_CAPACITY) when
+    pairs or contacts exceeded the caps in any substep."""
     import torch
 
-    if ph.params.flags & L.FLAG_NO_SYNC:
-        raise ValueError("rollout needs a handle without FLAG_NO_SYNC")
     b = ph.buffers
     nb = b.num_bodies
     t = b.tensors

@@ -64,8 +64,11 @@ class Physics:
 
     def step_async(self, num_bodies: int, num_vertices: int, num_hull_verts: int, substeps: int,
                    dt: float, gravity=(0.0, -9.81, 0.0), frames: int = 1, stream=None) -> None:
-        """`frames` steps ordered on `stream` (torch.cuda.Stream or raw handle)."""
+        """`frames` steps ordered on `stream` (torch.cuda.Stream or raw handle;
+        None: the handle's own stream)."""
         s = getattr(stream, "cuda_stream", stream)
+        if stream is not None and not s:
+            s = 1  # torch's default stream is CUDA's legacy default stream (cudaStreamLegacy)
         L.check(L.lib.seevr_physics_step_async(self._h, num_bodies, num_vertices, num_hull_verts,
                                                substeps, dt, L.fptr(gravity, 3), frames,
                                                C.c_void_p(s) if s else None))

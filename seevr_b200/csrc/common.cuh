@@ -70,6 +70,24 @@ struct Consts {
     uint32_t pgs_iterations, mpr_iterations, discover_trials;
 };
 
+// Island solver work arrays (islands.cu); parent == NULL: not allocated.
+struct IslandScratch {
+    uint32_t* parent;       // [max_bodies] union-find links
+    uint32_t* keys_in;      // [max_contacts] island root per contact (or none)
+    uint32_t* vals_in;      // [max_contacts] contact index
+    uint32_t* keys_tmp;     // [max_contacts] sort ping-pong
+    uint32_t* vals_tmp;     // [max_contacts]
+    uint32_t* keys_out;     // [max_contacts] sorted roots
+    uint32_t* perm;         // [max_contacts] contact of each sorted slot
+    uint32_t* head;         // [max_contacts] 1 at an island's first slot
+    uint32_t* idx;          // [max_contacts] exclusive scan of head
+    uint32_t* start;        // [max_contacts + 1] first slot of each island
+    uint32_t* count;        // [1] islands
+    uint32_t* lvl;          // [2 * max_contacts + 2] level boundaries per island
+    uint32_t* sort_hist;    // [4 * 256]
+    uint32_t* sort_status;  // look-back words of the sort
+};
+
 // Library-owned scratch (device).
 struct Scratch {
     uint32_t* status;       // [4]: flags, scratch counters
@@ -103,6 +121,7 @@ struct Scratch {
     // count pass (NULL: the write pass re-tests)
     uint32_t* bp_mask;      // [rows * bp_stride]
     uint32_t bp_stride;     // words per row
+    IslandScratch isl;
 };
 
 // ---- launchers (one translation unit each) ------------------------------
@@ -140,5 +159,11 @@ inline void set_last_error(const std::string& msg) { set_last_error(msg.c_str())
 // in shared memory by the warp solver (larger bundles solve in place)
 int launch_solver(const World& w, const Consts& k, const Scratch& s, uint32_t mode,
                   float dt, uint32_t max_scene_bodies, uint32_t smem_bodies, cudaStream_t st);
+// Island-parallel solve of the whole contact list (needs s.isl); mode 0
+// sequential, 1 wavefront, 2 coloured.
+int launch_solver_islands(const World& w, const Consts& k, const Scratch& s, uint32_t mode,
+                          float dt, cudaStream_t st);
+// Scenes above this many bodies are solved by islands (when allocated).
+constexpr uint32_t kWarpMaxBodies = 1024;
 
 }  // namespace seevr

@@ -263,7 +263,7 @@ extern "C" seevr_status seevr_physics_step_noalloc(
         launch_hull_range_from_geom_data(static_cast<const float*>(P(SEEVR_B_GEOM_DATA)),
                                          s.derived_hull_range, num_bodies, st);
     const float sub_dt = dt / float(substeps);
-    const uint32_t mode = p.solver == SEEVR_SOLVER_SEQUENTIAL ? 0u : 1u;
+    const uint32_t mode = p.solver;
     for (uint32_t sub = 0; sub < substeps; ++sub) {
         launch_body_stage(w, k, (sub > 0 ? kIntegrate : 0u) | kGravity | kAabb, sub_dt, gravity[0],
                           gravity[1], gravity[2], st);

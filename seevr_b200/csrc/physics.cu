@@ -294,7 +294,7 @@ uint64_t issue_frame(seevr_physics* h, uint32_t nb, uint32_t nv, uint32_t nhv, u
         cudaMemsetAsync(w.lambda, 0, sizeof(float) * w.max_contacts, st);  // step 4
         T.end(kStClear);
         T.begin();
-        n += launch_solver(w, h->k, h->s, h->params.solver == SEEVR_SOLVER_SEQUENTIAL ? 0u : 1u,
+        n += launch_solver(w, h->k, h->s, h->params.solver,
                            sub_dt, h->max_bundle_bodies, h->smem_bundle_bodies, st);
         T.end(kStSolve);
     }
@@ -432,8 +432,6 @@ seevr_status seevr_physics_create(const seevr_bindings* b, const seevr_caps* cap
     if (params) p = *params;
     if (p.broadphase > SEEVR_BROADPHASE_LBVH || p.solver > SEEVR_SOLVER_COLORED)
         return fail(SEEVR_ERR_INVALID_ARGUMENT, "unknown broadphase or solver");
-    if (p.solver == SEEVR_SOLVER_COLORED)
-        return fail(SEEVR_ERR_NOT_SUPPORTED, "coloured solver is not available in this build");
 
     auto* h = new seevr_physics();
     cudaGetDevice(&h->device);
@@ -443,7 +441,7 @@ seevr_status seevr_physics_create(const seevr_bindings* b, const seevr_caps* cap
     h->params = p;
     seevr_status st = SEEVR_OK;
     const seevr_caps& c = h->caps;
-    const uint32_t scan_n = std::max(std::max(c.max_bodies, c.max_pairs), 1u);
+    const uint32_t scan_n = std::max(std::max(std::max(c.max_bodies, c.max_pairs), c.max_contacts), 1u);
     h->s.scan_tiles_cap = (scan_n + 2047) / 2048 + 2;
 #define ALLOC(ptr, n)                                   \
     if (st == SEEVR_OK) st = dev_alloc(h, &(ptr), (n));
@@ -475,6 +473,24 @@ seevr_status seevr_physics_create(const seevr_bindings* b, const seevr_caps* cap
     ALLOC(h->body_scene, c.max_bodies);
     ALLOC(h->scene_off, size_t(c.max_scenes) + 1);
     ALLOC(h->bundle_off, size_t(c.max_scenes) + 1);
+    if (c.max_bodies > kWarpMaxBodies) {  // scenes large enough for the island solver
+        IslandScratch& is = h->s.isl;
+        const size_t nc = c.max_contacts;
+        ALLOC(is.parent, c.max_bodies);
+        ALLOC(is.keys_in, nc);
+        ALLOC(is.vals_in, nc);
+        ALLOC(is.keys_tmp, nc);
+        ALLOC(is.vals_tmp, nc);
+        ALLOC(is.keys_out, nc);
+        ALLOC(is.perm, nc);
+        ALLOC(is.head, nc);
+        ALLOC(is.idx, nc);
+        ALLOC(is.start, nc + 1);
+        ALLOC(is.count, 1);
+        ALLOC(is.lvl, 2 * nc + 2);
+        ALLOC(is.sort_hist, 4 * 256);
+        ALLOC(is.sort_status, lbvh_status_words(c.max_contacts));
+    }
     if (p.broadphase == SEEVR_BROADPHASE_LBVH) {
         LbvhScratch& lb = h->lb;
         const size_t n = c.max_bodies;

@@ -26,67 +26,9 @@
 // cannot change (the reference writes v - 0*impulse, the same value), so
 // fixed bodies create no ordering constraint and are never written.
 #include "common.cuh"
+#include "solver.cuh"
 
 namespace seevr {
-
-struct BodyView {
-    float* v;           // [n*3]
-    float* w;           // [n*3]
-    const float* R;     // [n*9]
-    const float* invI;  // [n*3]
-    const float* invm;  // [n]
-};
-
-__device__ __forceinline__ bool is_fixed(const BodyView& B, uint32_t i) {
-    return B.invm[i] == 0.0f && B.invI[i * 3] == 0.0f && B.invI[i * 3 + 1] == 0.0f &&
-           B.invI[i * 3 + 2] == 0.0f;
-}
-
-// One normal + friction update of contact c (physics.comp:525-580).
-__device__ __forceinline__ void solve_one(const BodyView& B, uint32_t la, uint32_t lb, f3 n, f3 ra,
-                                          f3 rb, float bias, float kn, float mu, float* lam) {
-    const float ima = B.invm[la], imb = B.invm[lb];
-    const m3 Ra = ld_m3(B.R, la), Rb = ld_m3(B.R, lb);
-    const f3 Ia = ld3(B.invI, la), Ib = ld3(B.invI, lb);
-    f3 va = ld3(B.v, la), wa = ld3(B.w, la), vb = ld3(B.v, lb), wb = ld3(B.w, lb);
-    f3 ua = add(va, cross(wa, ra)), ub = add(vb, cross(wb, rb));
-    const float vn = dot(sub(ub, ua), n);
-    float d_ln = (-vn + bias) / kn;
-    const float old_ln = *lam;
-    const float new_ln = gmax(old_ln + d_ln, 0.0f);
-    d_ln = new_ln - old_ln;
-    *lam = new_ln;
-    const f3 imp = scale(d_ln, n);
-    va = sub(va, scale(ima, imp));
-    vb = add(vb, scale(imb, imp));
-    wa = sub(wa, apply_inv_I(Ra, Ia, cross(ra, imp)));
-    wb = add(wb, apply_inv_I(Rb, Ib, cross(rb, imp)));
-    // Coulomb friction along the current slip direction
-    ua = add(va, cross(wa, ra));
-    ub = add(vb, cross(wb, rb));
-    const f3 dv = sub(ub, ua);
-    const f3 vt = sub(dv, scale(dot(dv, n), n));
-    const float vt_len = length(vt);
-    if (vt_len > 1e-6f) {
-        const f3 td = divs(vt, vt_len);
-        const f3 rat = cross(ra, td), rbt = cross(rb, td);
-        const float kt = ima + imb + dot(rat, apply_inv_I(Ra, Ia, rat)) + dot(rbt, apply_inv_I(Rb, Ib, rbt));
-        const float d_lt = gmin(vt_len / kt, mu * new_ln);
-        const f3 it = scale(d_lt, td);
-        va = add(va, scale(ima, it));
-        vb = sub(vb, scale(imb, it));
-        wa = add(wa, apply_inv_I(Ra, Ia, cross(ra, it)));
-        wb = sub(wb, apply_inv_I(Rb, Ib, cross(rb, it)));
-    }
-    if (!is_fixed(B, la)) {
-        st3(B.v, la, va);
-        st3(B.w, la, wa);
-    }
-    if (!is_fixed(B, lb)) {
-        st3(B.v, lb, vb);
-        st3(B.w, lb, wb);
-    }
-}
 
 constexpr uint32_t kSolverThreads = 128;
 constexpr uint32_t kBodySmemWords = 20;  // v3 w3 R9 invI3 invm1 last1
@@ -262,7 +204,6 @@ __global__ void k_bundle_ranges(World w, uint32_t* __restrict__ bundle_c0) {
 // assigned 32 contacts at a time: each lane starts from the latest level of
 // its bodies in earlier chunks, then lanes are visited in order and every
 // later lane sharing a dynamic body with lane j moves past lane j's level.
-constexpr uint32_t kWarpMaxBodies = 1024;
 constexpr uint32_t kWarpsPerBlock = 4;
 constexpr uint32_t kWarpLamCap = 1024;   // impulses per bundle held in smem
 constexpr uint32_t kWarpLevelCap = 128;  // level boundaries held in smem
@@ -314,9 +255,46 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
     }
     __syncwarp();
 
-    // ---- levels (WAVEFRONT) or one level in index order (SEQUENTIAL) ----
+    // ---- levels: colours (COLORED), wavefront levels (WAVEFRONT) or one
+    // level in index order (SEQUENTIAL)
     uint32_t maxl = 0;
-    for (uint32_t cb = c0; cb < c1; cb += 32) {
+    bool coloured = mode == 2;
+    if (coloured) {
+        // greedy colouring in contact order: the smallest colour not used by
+        // an earlier contact at either of its dynamic bodies (per-body colour
+        // masks in `last`); more than 32 colours at a body falls back to the
+        // wavefront levels
+        uint32_t ok = 1u, mx = 0u;
+        if (lane == 0) {
+            for (uint32_t c = c0; c < c1; ++c) {
+                const uint32_t la = s.s_ab[size_t(c) * 2], lb = s.s_ab[size_t(c) * 2 + 1];
+                if (la == kNone) {
+                    s.s_level[c] = kNone;
+                    continue;
+                }
+                const bool da = !is_fixed(B, la), db = !is_fixed(B, lb);
+                const uint32_t used = (da ? last[la] : 0u) | (db ? last[lb] : 0u);
+                if (used == 0xFFFFFFFFu) {
+                    ok = 0u;
+                    break;
+                }
+                const uint32_t col = uint32_t(__ffs(int(~used))) - 1u;
+                if (da) last[la] |= 1u << col;
+                if (db) last[lb] |= 1u << col;
+                s.s_level[c] = col;
+                mx = max(mx, col + 1u);
+            }
+        }
+        ok = __shfl_sync(full, ok, 0);
+        maxl = __shfl_sync(full, mx, 0);
+        if (!ok) {
+            coloured = false;
+            maxl = 0;
+            for (uint32_t i = lane; i < nbs; i += 32) last[i] = 0;
+        }
+        __syncwarp();
+    }
+    for (uint32_t cb = c0; !coloured && cb < c1; cb += 32) {
         const uint32_t c = cb + lane;
         const bool valid = c < c1;
         const uint32_t la = valid ? s.s_ab[size_t(c) * 2] : kNone;
@@ -458,6 +436,7 @@ int launch_solver(const World& w, const Consts& k, const Scratch& s, uint32_t mo
         k_solver_warp<<<blocks, kWarpsPerBlock * 32, smem, st>>>(w, k, s, mode, dt, nbmax);
         return 2;
     }
+    if (s.isl.parent) return 1 + launch_solver_islands(w, k, s, mode, dt, st);
     uint32_t cta_bodies = max_scene_bodies;
     if (cta_bodies * kBodySmemWords * 4 > kSolverMaxSmem)
         cta_bodies = kSolverMaxSmem / (kBodySmemWords * 4);

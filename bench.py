@@ -54,6 +54,10 @@ def parse():
     ap.add_argument("--adjoint-bodies", type=int, default=64)
     ap.add_argument("--adjoint-frames", type=int, default=60)
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--towers", type=int, default=1024)
+    ap.add_argument("--tower-height", type=int, default=256)
+    ap.add_argument("--tower-frames", type=int, default=20)
+    ap.add_argument("--no-towers", action="store_true")
     ap.add_argument("--prof-frames", type=int, default=3)
     ap.add_argument("--bundle-bodies", type=int, default=0,
                     help="solver bundle size in bodies (0: the library default)")
@@ -326,6 +330,7 @@ def ours(a, rank, world, local_rank):
         cpu = cpu_baseline(a, d, pre_state)
 
     adj = None if a.no_adjoint else adjoint_leg(a, rank, world, dev)
+    tow = None if a.no_towers or world > 1 else towers_leg(a, rank, world, dev)
 
     if rank == 0:
         line = {
@@ -342,6 +347,7 @@ def ours(a, rank, world, local_rank):
             "cpu_baseline": cpu,
             "plain": plain,
             "adjoint": adj,
+            "towers": tow,
             "stage_ms_per_frame": stage_ms,
             "last_substep": {"pairs": pairs, "contacts": contacts},
         }
@@ -422,6 +428,55 @@ def adjoint_leg(a, rank, world, dev):
         "wrt": "initial velocities, angular velocities, friction",
         "timing": "CUDA events around one forward + backward, max over ranks",
     }
+
+
+def towers_leg(a, rank, world, dev):
+    """Stacked boxes: --towers towers of --tower-height unit boxes (jitter
+    N(0, 0.01) m, friction 0.6, no restitution) on one static ground, one
+    scene, LBVH broadphase, island-parallel PGS, --tower-frames frames of 10
+    substeps x 30 iterations.  Coloured vs wavefront (= sequential) order:
+    throughput and the tower tops' drift at the end."""
+    import torch
+
+    from seevr_b200 import (BROADPHASE_LBVH, FLAG_CUDA_GRAPH, FLAG_SKIP_RENDER_VERTS, Caps, Data,
+                            Physics, SOLVER_COLORED, SOLVER_WAVEFRONT, make_params)
+
+    h = a.tower_height
+    d = Data.towers(seed=rank, towers=a.towers, height=h, spacing=2.0)
+    nb, nhv = d.num_bodies, d.num_hull_verts
+    caps = Caps.for_data(d, pairs_per_body=4.0, contacts_per_body=4.0)
+    buf = d.upload(dev, caps)
+    init = {k: buf.tensors[k].clone() for k in ("body_pos", "body_quat", "body_vel", "body_omega")}
+    tops = torch.arange(a.towers, device=dev) * h + h  # top box of each tower (body 0: ground)
+    top0 = init["body_pos"].reshape(-1, 3)[tops, 1].clone()
+    stream = torch.cuda.Stream(dev)
+    out = {}
+    for name, solver in (("coloured", SOLVER_COLORED), ("wavefront", SOLVER_WAVEFRONT)):
+        for k, v in init.items():
+            buf.tensors[k].copy_(v)
+        ph = Physics(buf, make_params(pgs_iterations=a.pgs, solver=solver,
+                                      broadphase=BROADPHASE_LBVH,
+                                      flags=FLAG_CUDA_GRAPH | FLAG_SKIP_RENDER_VERTS))
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            ph.step_async(nb, 0, nhv, a.substeps, DT, G, frames=a.tower_frames, stream=stream)
+            e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        flags = ph.read_flags()
+        top = buf.tensors["body_pos"][: nb * 3].reshape(-1, 3)[tops, 1]
+        drift = (top - top0).abs()
+        out[name] = {"value": (nb - 1) * a.substeps * a.tower_frames / (ms / 1e3),
+                     "ms_per_frame": ms / a.tower_frames,
+                     "top_drift_mean_m": float(drift.mean()), "top_drift_max_m": float(drift.max()),
+                     "finite": bool(torch.isfinite(buf.tensors["body_pos"][: nb * 3]).all()),
+                     "device_flags": flags}
+        ph.deinit()
+    return {"unit": UNIT, "bodies": nb, "towers": a.towers, "height": h,
+            "frames": a.tower_frames, "substeps": a.substeps, "pgs_iterations": a.pgs,
+            "broadphase": "LBVH", "solver_work": "islands (one per tower)", **out}
 
 
 def plain_dropin(a, d, pre_state, dev):

@@ -14,7 +14,9 @@
 // The body broadphase traverses the tree once per body to count and once
 // to write, emitting pairs (i, j>i) in canonical lexicographic order: the
 // same set as the all-pairs test of physics.comp:451-472 (node boxes are
-// exact unions of leaf boxes, so every overlapping leaf is reached).
+// exact unions of leaf boxes, so every overlapping leaf is reached).  Rows
+// of static bodies, which can hold thousands of partners (a ground box), are
+// traversed by whole blocks instead of one thread.
 #include "common.cuh"
 #include "lbvh.cuh"
 
@@ -403,12 +405,91 @@ __device__ __forceinline__ void traverse(const World& w, const LbvhView& t, uint
     }
 }
 
-__global__ void k_lbvh_count(World w, LbvhView t, uint32_t* __restrict__ row_count, uint32_t* err) {
+// Rows of dynamic bodies, one thread each; static bodies' rows (a ground
+// box overlapping thousands of bodies) are left to k_lbvh_static_rows and
+// listed here.
+__global__ void k_lbvh_count(World w, LbvhView t, uint32_t* __restrict__ row_count, uint32_t* err,
+                             uint32_t* static_list, uint32_t* static_count) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= w.nb) return;
+    if (w.inv_mass[i] <= 0.0f) {
+        static_list[atomicAdd(static_count, 1u)] = i;
+        return;
+    }
     uint32_t c = 0;
     if (w.nb >= 2) traverse(w, t, i, i, err, [&](uint32_t) { ++c; });
     row_count[i] = c;
+}
+
+// Rows of static bodies, one block each: a breadth-first traversal whose
+// frontier the block's threads expand together.  Count pass: the row's
+// length.  Write pass: the row's partners are collected unordered, then each
+// is written at its rank (the number of smaller partners), which gives the
+// ascending-j order of the canonical pair list.
+template <bool kWrite>
+__global__ void __launch_bounds__(256)
+    k_lbvh_static_rows(World w, LbvhView t, uint32_t* row_count, const uint32_t* row_off,
+                       const uint32_t* static_list, const uint32_t* static_count, uint32_t* bfs) {
+    __shared__ uint32_t sh_next, sh_found, sh_cur;
+    const uint32_t n = w.nb;
+    if (n < 2) return;
+    uint32_t* fa = bfs + size_t(blockIdx.x) * 3 * 2 * n;
+    uint32_t* fb = fa + 2 * n;
+    uint32_t* found = fb + 2 * n;
+    const uint32_t ns = *static_count;
+    for (uint32_t r = blockIdx.x; r < ns; r += gridDim.x) {
+        const uint32_t i = static_list[r];
+        const f3 mna = ld3(w.aabb_min, i), mxa = ld3(w.aabb_max, i);
+        if (threadIdx.x == 0) {
+            fa[0] = 0;  // root
+            sh_cur = 1;
+            sh_found = 0;
+        }
+        __syncthreads();
+        uint32_t* in = fa;
+        uint32_t* out = fb;
+        while (sh_cur > 0) {
+            const uint32_t cur = sh_cur;
+            if (threadIdx.x == 0) sh_next = 0;
+            __syncthreads();
+            for (uint32_t k = threadIdx.x; k < cur; k += blockDim.x) {
+                const uint32_t node = in[k];
+                if (!overlap_box(mna, mxa, ld3(t.node_min, node), ld3(t.node_max, node))) continue;
+                if (node >= n - 1) {
+                    const uint32_t j = t.vals[node - (n - 1)];
+                    // the row owner is static: only dynamic partners count
+                    if (j > i && w.inv_mass[j] > 0.0f) found[atomicAdd(&sh_found, 1u)] = j;
+                } else {
+                    const uint32_t o = atomicAdd(&sh_next, 2u);
+                    out[o] = t.left[node];
+                    out[o + 1] = t.right[node];
+                }
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) sh_cur = sh_next;
+            uint32_t* tmp = in;
+            in = out;
+            out = tmp;
+            __syncthreads();
+        }
+        const uint32_t cnt = sh_found;
+        if (!kWrite) {
+            if (threadIdx.x == 0) row_count[i] = cnt;
+        } else {
+            const uint32_t base = row_off[i];
+            for (uint32_t e = threadIdx.x; e < cnt; e += blockDim.x) {
+                const uint32_t j = found[e];
+                uint32_t rank = 0;
+                for (uint32_t q = 0; q < cnt; ++q) rank += found[q] < j ? 1u : 0u;
+                const uint32_t slot = base + rank;
+                if (slot < w.max_pairs) {
+                    w.pairs[size_t(slot) * 2] = i;
+                    w.pairs[size_t(slot) * 2 + 1] = j;
+                }
+            }
+        }
+        __syncthreads();
+    }
 }
 
 // Writes row i's pairs at row_off[i] in ascending j: rows are emitted in
@@ -416,7 +497,7 @@ __global__ void k_lbvh_count(World w, LbvhView t, uint32_t* __restrict__ row_cou
 __global__ void k_lbvh_write(World w, LbvhView t, const uint32_t* __restrict__ row_count,
                              const uint32_t* __restrict__ row_off, uint32_t* err) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= w.nb) return;
+    if (i >= w.nb || w.inv_mass[i] <= 0.0f) return;  // static rows: k_lbvh_static_rows
     uint32_t remaining = row_count[i];
     uint32_t slot = row_off[i];
     uint32_t lo = i;
@@ -500,11 +581,17 @@ int launch_broadphase_lbvh(const World& w, const Scratch& sc, const LbvhScratch&
     if (n == 0) return 0;
     int k = lbvh_build_bodies(w, s, &sc.status[0], st);
     LbvhView t{s.node_min, s.node_max, s.left, s.right, s.vals_sorted};
-    k_lbvh_count<<<blocks_for(n, 128), 128, 0, st>>>(w, t, sc.row_count, &sc.status[0]);
+    cudaMemsetAsync(s.static_count, 0, sizeof(uint32_t), st);
+    k_lbvh_count<<<blocks_for(n, 128), 128, 0, st>>>(w, t, sc.row_count, &sc.status[0],
+                                                     s.static_list, s.static_count);
+    k_lbvh_static_rows<false><<<kStaticBlocks, 256, 0, st>>>(w, t, sc.row_count, nullptr,
+                                                            s.static_list, s.static_count, s.bfs);
     launch_exclusive_scan(sc.row_count, sc.row_off, nullptr, n, &w.counters[0], w.max_pairs,
                           kFlagPairOverflow, sc, st);
     k_lbvh_write<<<blocks_for(n, 128), 128, 0, st>>>(w, t, sc.row_count, sc.row_off, &sc.status[0]);
-    return k + 3;
+    k_lbvh_static_rows<true><<<kStaticBlocks, 256, 0, st>>>(w, t, nullptr, sc.row_off,
+                                                           s.static_list, s.static_count, s.bfs);
+    return k + 5;
 }
 
 int lbvh_build_triangles(const float* verts, const uint32_t* idx, uint32_t n, const LbvhScratch& s,

@@ -24,7 +24,15 @@ struct LbvhScratch {
     uint32_t* flags;        // [cap]
     float* node_min;        // [2*cap*3]
     float* node_max;        // [2*cap*3]
+    // rows of static bodies (body broadphase): list, count and per-block
+    // breadth-first work areas (kStaticBlocks x 3 x 2*cap)
+    uint32_t* static_list;   // [cap]
+    uint32_t* static_count;  // [1]
+    uint32_t* bfs;
 };
+
+// Blocks that traverse static bodies' rows.
+constexpr uint32_t kStaticBlocks = 8;
 
 struct LbvhView {
     const float* node_min;

@@ -512,6 +512,9 @@ seevr_status seevr_physics_create(const seevr_bindings* b, const seevr_caps* cap
         ALLOC(lb.flags, n);
         ALLOC(lb.node_min, 6 * n);
         ALLOC(lb.node_max, 6 * n);
+        ALLOC(lb.static_list, n);
+        ALLOC(lb.static_count, 1);
+        ALLOC(lb.bfs, size_t(kStaticBlocks) * 3 * 2 * n);
     }
 #undef ALLOC
     if (st == SEEVR_OK && cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)

@@ -313,6 +313,56 @@ seevr_status seevr_physics_adjoint_substep(seevr_physics* h, uint32_t num_bodies
                                            const float gravity[3],
                                            const seevr_adjoint_grads* grads);
 
+/* ---- path tracer (raytracer.zig / raytrace.comp) ------------------------- */
+
+/* Binding indices of Raytracer.init (raytracer.zig:31-58), identical to
+ * raytrace.comp's `binding=` numbers (raytrace.comp:15-35).  Binding 0 is a
+ * storage image in the reference; here it is a headless device buffer of
+ * f32[width*height*4] RGBA, row-major.  Bindings 3-8 are the triangle BVH's
+ * node min/max, left, right, count and primitive indices as seevr_bvh_build
+ * writes them. */
+enum seevr_rt_binding {
+    SEEVR_RT_IMAGE = 0,          /* f32[W*H*4]   w */
+    SEEVR_RT_VERTICES = 1,       /* f32[V*3]     r */
+    SEEVR_RT_INDICES = 2,        /* u32[T*3]     r */
+    SEEVR_RT_NODE_MIN = 3,       /* f32[(2T-1)*3] r */
+    SEEVR_RT_NODE_MAX = 4,       /* f32[(2T-1)*3] r */
+    SEEVR_RT_LEFT = 5,           /* u32[2T-1]    r */
+    SEEVR_RT_RIGHT = 6,          /* u32[2T-1]    r */
+    SEEVR_RT_COUNT = 7,          /* u32[2T-1]    r */
+    SEEVR_RT_PRIM = 8,           /* u32[T]       r */
+    SEEVR_RT_TRI_GEOM = 9,       /* u32[T]       r */
+    SEEVR_RT_GEOM_MATERIAL = 10, /* u32[G]       r */
+    SEEVR_RT_MAT_ALBEDO = 11,    /* f32[M*3]     r */
+    SEEVR_RT_MAT_ROUGHNESS = 12, /* f32[M]       r */
+    SEEVR_RT_MAT_METALLIC = 13,  /* f32[M]       r */
+    SEEVR_RT_MAT_EMISSION = 14,  /* f32[M*3]     r */
+    SEEVR_RT_MAT_IOR = 15,       /* f32[M] 0 = opaque r */
+    SEEVR_RT_NUM_BINDINGS = 16
+};
+
+typedef struct seevr_rt_bindings {
+    void* ptr[SEEVR_RT_NUM_BINDINGS];
+} seevr_rt_bindings;
+
+/* The push constants of raytrace.comp:5-13 (PC, raytracer.zig:6-15). */
+typedef struct seevr_rt_params {
+    float cam_pos[3], cam_dir[3], cam_right[3], cam_up[3];
+    uint32_t width, height;
+    uint32_t frame_num;      /* seeds the per-pixel RNG (raytrace.comp:182) */
+    uint32_t num_triangles;
+} seevr_rt_params;
+
+/* Raytracer.render (raytracer.zig:159-200): one frame, 16 samples per pixel
+ * and up to 16 bounces per sample, written (not accumulated) to binding 0.
+ * Ordered on `stream` (a cudaStream_t, NULL = the default stream) and
+ * synchronous, as render() waits for its queue.  Where GLSL leaves precision
+ * to the implementation the library pins it: sin/cos of the hemisphere
+ * angle by its own polynomials, pow(x, 5) as a product, and tan(30 degrees)
+ * rounded from double (seevr_raytrace_fov_scale). */
+seevr_status seevr_raytrace(const seevr_rt_bindings* b, const seevr_rt_params* p, void* stream);
+float seevr_raytrace_fov_scale(void);
+
 /* ---- triangle LBVH (bvh.zig / bvh.comp) ---------------------------------- */
 
 /* Binding indices of BVH.init (bvh.zig:32-51), identical to bvh.comp's

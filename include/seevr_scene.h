@@ -47,7 +47,15 @@ enum seevr_scene_array_id {
     SEEVR_S_SCENE_BODY_OFFSET = 20,/* u32 num_scenes+1 */
     SEEVR_S_COLORS = 21,           /* f32 V*3 */
     SEEVR_S_HULL_RANGE = 22,       /* u32 G*2 exact (hull_start, hull_count) */
-    SEEVR_S_NUM_ARRAYS = 23
+    /* path-tracer inputs (raytrace.comp bindings 9-15, data.zig:72, 104) */
+    SEEVR_S_GEOM_MATERIAL = 23,    /* u32 G   material of each geom          */
+    SEEVR_S_TRI_GEOM = 24,         /* u32 T   geom of each render triangle   */
+    SEEVR_S_MAT_ALBEDO = 25,       /* f32 M*3 */
+    SEEVR_S_MAT_ROUGHNESS = 26,    /* f32 M   */
+    SEEVR_S_MAT_METALLIC = 27,     /* f32 M   */
+    SEEVR_S_MAT_EMISSION = 28,     /* f32 M*3 */
+    SEEVR_S_MAT_IOR = 29,          /* f32 M   0 = opaque, > 0 = glass        */
+    SEEVR_S_NUM_ARRAYS = 30
 };
 
 enum seevr_scene_count_id {

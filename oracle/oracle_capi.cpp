@@ -323,3 +323,259 @@ int oracle_num_threads(void) {
 }
 
 }  // extern "C"
+
+// ---- path tracer (raytrace.comp), test infrastructure ------------------------
+// A restatement of raytrace.comp:37-282 in the shader's evaluation order,
+// with the same pinned definitions as the library (its own sin/cos
+// polynomials, pow(x, 5) as a product, the float literal 4294967295.0 as
+// 2^32).  Images are float RGBA, row-major.
+namespace rt {
+
+struct V {
+    float x, y, z;
+};
+inline V mk(float x, float y, float z) { return V{x, y, z}; }
+inline V add(V a, V b) { return V{a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline V sub(V a, V b) { return V{a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline V neg(V a) { return V{-a.x, -a.y, -a.z}; }
+inline V scale(float s, V a) { return V{s * a.x, s * a.y, s * a.z}; }
+inline V mul(V a, V b) { return V{a.x * b.x, a.y * b.y, a.z * b.z}; }
+inline float dot(V a, V b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline V cross(V a, V b) {
+    return V{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+inline V normalize(V a) {
+    const float l = std::sqrt(dot(a, a));
+    return V{a.x / l, a.y / l, a.z / l};
+}
+inline float gmin(float x, float y) { return y < x ? y : x; }  // GLSL min
+inline float gmax(float x, float y) { return x < y ? y : x; }  // GLSL max
+inline V ld(const float* p, uint32_t i) { return V{p[size_t(i) * 3], p[size_t(i) * 3 + 1], p[size_t(i) * 3 + 2]}; }
+
+inline uint32_t pcg(uint32_t seed) {  // raytrace.comp:43-47
+    const uint32_t state = seed * 747796405u + 2891336453u;
+    const uint32_t word = ((state >> ((state >> 28) + 4u)) ^ state) * 277803737u;
+    return (word >> 22) ^ word;
+}
+inline float rand_f(uint32_t seed) { return float(pcg(seed)) / 4294967296.0f; }
+
+inline void sincos_pinned(float x, float& s, float& c) {
+    const float hi = 1.57079637050628662109375f, lo = -4.37113900018624283e-8f;
+    const float q = float(int(x * 0.636619772f + 0.5f));
+    const float r = (x - q * hi) - q * lo;
+    const float r2 = r * r;
+    const float sp = r * (1.0f + r2 * (-1.0f / 6.0f + r2 * (1.0f / 120.0f + r2 * (-1.0f / 5040.0f +
+                                                                                  r2 * (1.0f / 362880.0f)))));
+    const float cp = 1.0f + r2 * (-0.5f + r2 * (1.0f / 24.0f + r2 * (-1.0f / 720.0f +
+                                                                    r2 * (1.0f / 40320.0f +
+                                                                          r2 * (-1.0f / 3628800.0f)))));
+    switch (int(q) & 3) {
+        case 0: s = sp; c = cp; break;
+        case 1: s = cp; c = -sp; break;
+        case 2: s = -sp; c = -cp; break;
+        default: s = -cp; c = sp; break;
+    }
+}
+inline V mix3(V x, V y, float a) { return add(scale(1.0f - a, x), scale(a, y)); }
+inline V reflect3(V i, V n) { return sub(i, scale(2.0f * dot(n, i), n)); }
+inline V refract3(V i, V n, float eta) {
+    const float d = dot(n, i);
+    const float k = 1.0f - eta * eta * (1.0f - d * d);
+    if (k < 0.0f) return mk(0.f, 0.f, 0.f);
+    return sub(scale(eta, i), scale(eta * d + std::sqrt(k), n));
+}
+inline float schlick(float cos_theta, float r0) {
+    const float x = 1.0f - cos_theta;
+    return r0 + (1.0f - r0) * (((x * x) * (x * x)) * x);
+}
+
+struct Scene {
+    const float *verts, *node_min, *node_max, *albedo, *roughness, *metallic, *emission, *ior;
+    const uint32_t *idx, *left, *right, *count, *prim, *tri_geom, *geom_material;
+};
+
+inline float ray_tri(V ro, V rd, V v0, V v1, V v2) {  // raytrace.comp:55-69
+    const V e1 = sub(v1, v0), e2 = sub(v2, v0);
+    const V h = cross(rd, e2);
+    const float a = dot(e1, h);
+    if (std::fabs(a) < 1e-8f) return -1.0f;
+    const float f = 1.0f / a;
+    const V s = sub(ro, v0);
+    const float u = f * dot(s, h);
+    if (u < 0.0f || u > 1.0f) return -1.0f;
+    const V q = cross(s, e1);
+    const float v = f * dot(rd, q);
+    if (v < 0.0f || u + v > 1.0f) return -1.0f;
+    const float t = f * dot(e2, q);
+    return t > 0.001f ? t : -1.0f;
+}
+
+inline bool ray_aabb(V ro, V inv_d, V bmin, V bmax, float closest) {  // 73-81
+    const V t1 = mul(sub(bmin, ro), inv_d), t2 = mul(sub(bmax, ro), inv_d);
+    const V tmin{gmin(t1.x, t2.x), gmin(t1.y, t2.y), gmin(t1.z, t2.z)};
+    const V tmax{gmax(t1.x, t2.x), gmax(t1.y, t2.y), gmax(t1.z, t2.z)};
+    const float enter = gmax(gmax(tmin.x, tmin.y), tmin.z);
+    const float exit_ = gmin(gmin(tmax.x, tmax.y), tmax.z);
+    return exit_ >= enter && enter < closest && exit_ > 0.0f;
+}
+
+inline void trace(const Scene& g, V ro, V rd, float& closest, V& normal, uint32_t& hit, bool& front) {
+    closest = 1e10f;
+    normal = mk(0.f, 1.f, 0.f);
+    hit = 0xFFFFFFFFu;
+    front = true;
+    const V inv_d = mk(1.0f / rd.x, 1.0f / rd.y, 1.0f / rd.z);
+    int stack[32];
+    stack[0] = 0;
+    int sp = 1;
+    while (sp > 0) {
+        --sp;
+        const int node = stack[sp];
+        if (!ray_aabb(ro, inv_d, ld(g.node_min, node), ld(g.node_max, node), closest)) continue;
+        const uint32_t cnt = g.count[node], lf = g.left[node];
+        if (cnt > 0) {
+            for (uint32_t i = 0; i < cnt; ++i) {
+                const uint32_t ti = g.prim[lf + i];
+                const V v0 = ld(g.verts, g.idx[size_t(ti) * 3]);
+                const V v1 = ld(g.verts, g.idx[size_t(ti) * 3 + 1]);
+                const V v2 = ld(g.verts, g.idx[size_t(ti) * 3 + 2]);
+                const float t = ray_tri(ro, rd, v0, v1, v2);
+                if (t > 0.0f && t < closest) {
+                    closest = t;
+                    const V n = normalize(cross(sub(v1, v0), sub(v2, v0)));
+                    front = dot(n, rd) < 0.0f;
+                    normal = front ? n : neg(n);
+                    hit = ti;
+                }
+            }
+        } else {
+            const uint32_t r = g.right[node];
+            if (sp < 31) stack[sp++] = int(lf);
+            if (sp < 31) stack[sp++] = int(r);
+        }
+    }
+}
+
+inline V sky_color(V rd) {
+    const float t = 0.5f * (rd.y + 1.0f);
+    return scale(0.8f, mix3(mk(1.f, 1.f, 1.f), mk(0.5f, 0.7f, 1.0f), t));
+}
+
+inline V sample_hemisphere(V n, uint32_t s1, uint32_t s2) {
+    const float r1 = rand_f(s1), r2 = rand_f(s2);
+    const float phi = 2.0f * 3.14159265f * r1;
+    const float cos_t = std::sqrt(r2), sin_t = std::sqrt(1.0f - r2);
+    const V up = std::fabs(n.y) > 0.99f ? mk(1.f, 0.f, 0.f) : mk(0.f, 1.f, 0.f);
+    const V tan1 = normalize(cross(up, n));
+    const V tan2 = cross(n, tan1);
+    float sp, cp;
+    sincos_pinned(phi, sp, cp);
+    return normalize(add(add(scale(cp, scale(sin_t, tan1)), scale(cos_t, n)), scale(sp, scale(sin_t, tan2))));
+}
+
+void pixel(const Scene& g, const float* cam, uint32_t w, uint32_t h, uint32_t frame, float fov,
+           uint32_t px, uint32_t py, float* out) {  // raytrace.comp:163-282
+    const V cam_pos{cam[0], cam[1], cam[2]}, cam_dir{cam[3], cam[4], cam[5]};
+    const V cam_right{cam[6], cam[7], cam[8]}, cam_up{cam[9], cam[10], cam[11]};
+    const float aspect = float(w) / float(h);
+    V pix = mk(0.f, 0.f, 0.f);
+    for (int si = 0; si < 16; ++si) {
+        uint32_t seed = px + py * w + frame * w * h + uint32_t(si) * 12345u;
+        const float jx = rand_f(seed) - 0.5f;
+        const float jy = rand_f(seed + 1u) - 0.5f;
+        const float u = (2.0f * (float(px) + 0.5f + jx) / float(w) - 1.0f) * aspect * fov;
+        const float v = -(2.0f * (float(py) + 0.5f + jy) / float(h) - 1.0f) * fov;
+        V rd = normalize(add(add(cam_dir, scale(u, cam_right)), scale(v, cam_up)));
+        V ro = cam_pos;
+        V thr = mk(1.f, 1.f, 1.f), color = mk(0.f, 0.f, 0.f);
+        for (int bounce = 0; bounce < 16; ++bounce) {
+            float t;
+            V normal;
+            uint32_t hit;
+            bool front;
+            trace(g, ro, rd, t, normal, hit, front);
+            if (t >= 1e9f) {
+                color = add(color, mul(thr, sky_color(rd)));
+                break;
+            }
+            const uint32_t mi = g.geom_material[g.tri_geom[hit]];
+            const V albedo = ld(g.albedo, mi), emission = ld(g.emission, mi);
+            const float rough = g.roughness[mi], metal = g.metallic[mi], ior = g.ior[mi];
+            color = add(color, mul(thr, emission));
+            if (emission.x + emission.y + emission.z > 0.0f) break;
+            const V hp = add(ro, scale(t, rd));
+            if (bounce > 0) {
+                const float p = gmax(thr.x, gmax(thr.y, thr.z));
+                if (rand_f(seed + uint32_t(bounce) * 7u) > p) break;
+                thr = mk(thr.x / p, thr.y / p, thr.z / p);
+            }
+            seed = pcg(seed);
+            if (ior > 0.0f) {
+                const float eta = front ? (1.0f / ior) : ior;
+                const float cos_i = std::fabs(dot(rd, normal));
+                const float sin2_t = eta * eta * (1.0f - cos_i * cos_i);
+                float r0 = (1.0f - ior) / (1.0f + ior);
+                r0 = r0 * r0;
+                const float fresnel = schlick(cos_i, r0);
+                const bool tir = sin2_t > 1.0f;
+                if (rand_f(seed + 5u) < fresnel || tir) {
+                    rd = reflect3(rd, normal);
+                    ro = add(hp, scale(0.001f, normal));
+                } else {
+                    rd = refract3(rd, normal, eta);
+                    ro = sub(hp, scale(0.001f, normal));
+                }
+                thr = mul(thr, albedo);
+            } else if (metal > 0.5f) {
+                const V refl = reflect3(rd, normal);
+                const V diff = sample_hemisphere(normal, seed, seed + 1u);
+                rd = normalize(mix3(refl, diff, rough * rough));
+                thr = mul(thr, albedo);
+                ro = add(hp, scale(0.001f, normal));
+            } else {
+                const V refl = reflect3(rd, normal);
+                const V diff = sample_hemisphere(normal, seed, seed + 1u);
+                const float cos_theta = gmax(dot(neg(rd), normal), 0.0f);
+                const float fresnel = schlick(cos_theta, 0.04f);
+                if (rand_f(seed + 3u) < fresnel) {
+                    rd = normalize(mix3(refl, diff, rough * rough));
+                } else {
+                    rd = diff;
+                    thr = mul(thr, albedo);
+                }
+                ro = add(hp, scale(0.001f, normal));
+            }
+        }
+        pix = add(pix, color);
+    }
+    out[0] = pix.x / 16.0f;
+    out[1] = pix.y / 16.0f;
+    out[2] = pix.z / 16.0f;
+    out[3] = 1.0f;
+}
+
+}  // namespace rt
+
+extern "C" {
+
+// cam: pos, dir, right, up (12 floats); fov = tan(30 degrees) as the library
+// computes it; image: w*h*4 floats.  OpenMP over rows when threads > 0.
+void oracle_raytrace(const float* verts, const uint32_t* idx, const float* node_min,
+                     const float* node_max, const uint32_t* left, const uint32_t* right,
+                     const uint32_t* count, const uint32_t* prim, const uint32_t* tri_geom,
+                     const uint32_t* geom_material, const float* albedo, const float* roughness,
+                     const float* metallic, const float* emission, const float* ior,
+                     const float* cam, uint32_t w, uint32_t h, uint32_t frame, float fov,
+                     int threads, float* image) {
+    const rt::Scene g{verts, node_min, node_max, albedo, roughness, metallic, emission, ior,
+                      idx,   left,     right,    count,  prim,      tri_geom, geom_material};
+#ifdef _OPENMP
+    if (threads > 0) omp_set_num_threads(threads);
+#endif
+#pragma omp parallel for schedule(dynamic, 1) if (threads > 0)
+    for (int64_t py = 0; py < int64_t(h); ++py)
+        for (uint32_t px = 0; px < w; ++px)
+            rt::pixel(g, cam, w, h, frame, fov, px, uint32_t(py), image + (size_t(py) * w + px) * 4);
+}
+
+}  // extern "C"

@@ -69,6 +69,10 @@ def _load():
     lib.oracle_run_f64_state.argtypes = [C.POINTER(OracleScene), C.POINTER(OracleParams),
                                          C.c_uint32, C.c_uint32, C.c_float, _f, _d, _d, _d, _d,
                                          _d, C.c_int, C.POINTER(OracleOut), _u64, C.c_int]
+    lib.oracle_raytrace.restype = None
+    lib.oracle_raytrace.argtypes = [_f, _u, _f, _f, _u, _u, _u, _u, _u, _u, _f, _f, _f, _f, _f,
+                                    _f, C.c_uint32, C.c_uint32, C.c_uint32, C.c_float, C.c_int,
+                                    _f]
     lib.oracle_morton.argtypes = [_f, C.c_uint32, _u, _f]
     lib.oracle_radix_sort.argtypes = [_u, C.c_uint32, _u, _u]
     lib.oracle_karras.argtypes = [_u, C.c_uint32, _u, _u, _u]
@@ -211,6 +215,21 @@ def run_f64_state(arrays: dict, *, pos=None, quat=None, vel=None, omega=None, fr
                                   *[_p(x, _d) for x in keep], threads, C.byref(o),
                                   _p(sig, _u64), LOCK_MODES[lock])
     return _done(rc, "oracle_run_f64_state", out, o, 0, max_pairs, max_contacts, sig)
+
+
+def raytrace(verts, idx, node_min, node_max, left, right, count, prim, tri_geom, geom_material,
+             albedo, roughness, metallic, emission, ior, cam, width, height, frame, fov,
+             threads=0) -> np.ndarray:
+    """CPU restatement of raytrace.comp: (height, width, 4) float32 image."""
+    f = lambda x: np.ascontiguousarray(x, dtype=np.float32).reshape(-1)
+    u = lambda x: np.ascontiguousarray(x).reshape(-1).view(np.uint32)
+    args = [f(verts), u(idx), f(node_min), f(node_max), u(left), u(right), u(count), u(prim),
+            u(tri_geom), u(geom_material), f(albedo), f(roughness), f(metallic), f(emission),
+            f(ior), f(cam)]
+    img = np.zeros((height, width, 4), np.float32)
+    ptrs = [_p(x, _f if x.dtype == np.float32 else _u) for x in args]
+    lib.oracle_raytrace(*ptrs, width, height, frame, fov, threads, _p(img, _f))
+    return img
 
 
 def morton(centroids: np.ndarray):

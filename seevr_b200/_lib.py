@@ -78,6 +78,19 @@ class AdjointGrads(C.Structure):
                 ("omega", C.c_void_p), ("friction", C.c_void_p)]
 
 
+class RtBindings(C.Structure):
+    """seevr_rt_bindings: the 16 device pointers of raytrace.comp."""
+    _fields_ = [("ptr", C.c_void_p * 16)]
+
+
+class RtParams(C.Structure):
+    """seevr_rt_params: raytrace.comp's push constants."""
+    _fields_ = [("cam_pos", C.c_float * 3), ("cam_dir", C.c_float * 3),
+                ("cam_right", C.c_float * 3), ("cam_up", C.c_float * 3),
+                ("width", C.c_uint32), ("height", C.c_uint32), ("frame_num", C.c_uint32),
+                ("num_triangles", C.c_uint32)]
+
+
 class SeevrError(RuntimeError):
     def __init__(self, status: int, message: str):
         super().__init__(f"seevr status {status}: {message}")
@@ -106,6 +119,8 @@ def _load():
         "seevr_physics_kernel_launches": (U64, [P]),
         "seevr_physics_read_lbvh": (I, [P, U32, UP, UP, FP]),
         "seevr_physics_adjoint_substep": (I, [P, U32, U32, F, FP, C.POINTER(AdjointGrads)]),
+        "seevr_raytrace": (I, [C.POINTER(RtBindings), C.POINTER(RtParams), P]),
+        "seevr_raytrace_fov_scale": (F, []),
         "seevr_physics_step_noalloc": (I, [C.POINTER(Bindings), C.POINTER(Params), U32, U32,
                                            U32, U32, U32, U32, F, FP, P]),
         "seevr_bvh_create": (I, [C.POINTER(BvhBindings), U32, C.POINTER(P)]),

@@ -68,6 +68,7 @@ struct seevr_scene {
     // materials
     std::vector<float> mat_albedo, mat_roughness, mat_metallic, mat_emission,
         mat_ior, mat_density;
+    std::vector<uint32_t> tri_geom;  // built on request (seevr_scene_array)
     // hull + support lookup
     std::vector<float> hull_verts;
     std::vector<uint32_t> support_offset, support_lookup;
@@ -797,6 +798,20 @@ void* seevr_scene_array(seevr_scene* s, int id) {
             return s->scene_offsets_view.data();
         case SEEVR_S_COLORS: return s->colors.data();
         case SEEVR_S_HULL_RANGE: return s->hull_range.data();
+        case SEEVR_S_GEOM_MATERIAL: return s->geom_material.data();
+        case SEEVR_S_TRI_GEOM: {
+            // triangle -> geom, from each geom's triangle range (data.zig:642-652)
+            s->tri_geom.assign(s->num_triangles(), 0u);
+            for (uint32_t g = 0; g < s->geom_tri_start.size(); ++g)
+                for (uint32_t t = 0; t < s->geom_tri_count[g]; ++t)
+                    s->tri_geom[s->geom_tri_start[g] + t] = g;
+            return s->tri_geom.data();
+        }
+        case SEEVR_S_MAT_ALBEDO: return s->mat_albedo.data();
+        case SEEVR_S_MAT_ROUGHNESS: return s->mat_roughness.data();
+        case SEEVR_S_MAT_METALLIC: return s->mat_metallic.data();
+        case SEEVR_S_MAT_EMISSION: return s->mat_emission.data();
+        case SEEVR_S_MAT_IOR: return s->mat_ior.data();
         default: return nullptr;
     }
 }

@@ -20,7 +20,7 @@ import numpy as np
 from . import _lib as L
 
 # seevr_scene_array ids -> (dtype, components, count id)
-_S_BODY, _S_GEOM, _S_HULL, _S_VERT, _S_TRI, _S_SUP, _S_SCN = 0, 1, 2, 3, 4, 5, 6
+_S_BODY, _S_GEOM, _S_HULL, _S_VERT, _S_TRI, _S_SUP, _S_SCN, _S_MAT = 0, 1, 2, 3, 4, 5, 6, 7
 _ARRAYS = {
     "body_pos": (0, np.float32, 3, _S_BODY),
     "body_quat": (1, np.float32, 4, _S_BODY),
@@ -45,6 +45,13 @@ _ARRAYS = {
     "scene_body_offset": (20, np.uint32, 1, None),
     "colors": (21, np.float32, 3, _S_VERT),
     "hull_range": (22, np.uint32, 2, _S_GEOM),
+    "geom_material": (23, np.uint32, 1, _S_GEOM),
+    "tri_geom": (24, np.uint32, 1, _S_TRI),
+    "mat_albedo": (25, np.float32, 3, _S_MAT),
+    "mat_roughness": (26, np.float32, 1, _S_MAT),
+    "mat_metallic": (27, np.float32, 1, _S_MAT),
+    "mat_emission": (28, np.float32, 3, _S_MAT),
+    "mat_ior": (29, np.float32, 1, _S_MAT),
 }
 
 # host array name -> binding index

@@ -25,9 +25,15 @@
 // sweep's per-iteration sensitivities nearly cancel (later iterations undo
 // most of an earlier impulse), so FP32 accumulation loses digits, most
 // visibly in the friction gradient, while FP64 keeps the result to the
-// FP32 forward's own accuracy.  The sequential parts run on lane 0 of the
-// bundle's warp, so every sum is accumulated in a fixed order and the
-// gradients are deterministic.
+// FP32 forward's own accuracy.
+//
+// Parallelism: one warp per solver bundle.  The sweep's contacts get the
+// solver's wavefront levels (contacts of one level touch disjoint dynamic
+// bodies), so the recomputed sweep, its reverse and the constants' reverse
+// run a level at a time across the lanes.  Every dynamic body still
+// receives its gradient contributions in the serial order; contributions to
+// fixed bodies (shared by contacts of one level) are kept per contact and
+// summed in contact order at the end, so the result stays deterministic.
 #include "adjoint.cuh"
 
 namespace seevr {
@@ -345,7 +351,8 @@ __device__ __forceinline__ f3 hull_vert(const World& w, uint32_t vs, uint32_t i)
 // 376-387).  The support points are recomputed in FP32 as the narrowphase
 // computed them; the derivatives are FP64.
 __device__ void contact_geom_bwd(const World& w, const Consts& k, const AdjScratch& a, uint32_t c,
-                                 uint32_t ba, uint32_t bb, d3 g_n, double g_pen, d3 g_cp) {
+                                 uint32_t ba, uint32_t bb, d3 g_n, double g_pen, d3 g_cp,
+                                 d3& gpA, d3& gpB, dm3& gRA, dm3& gRB) {
     const uint4 t0 = a.ctape[size_t(c) * 2], t1 = a.ctape[size_t(c) * 2 + 1];
     const f3 pAf = ld3(w.pos, ba), pBf = ld3(w.pos, bb);
     const m3 RAf = quat_to_mat(w.quat, ba), RBf = quat_to_mat(w.quat, bb);
@@ -362,7 +369,8 @@ __device__ void contact_geom_bwd(const World& w, const Consts& k, const AdjScrat
         vf[i] = sub(saf[i], sbf[i]);
         gsa[i] = gsb[i] = gv[i] = dz();
     }
-    d3 gpA = dz(), gpB = dz();
+    gpA = dz();
+    gpB = dz();
     if (t0.x == 2u) {  // segment case: depth = |v1|, n = v1/|v1|, cp = (s1a + s1b)/2
         const d3 v1 = D(vf[1]);
         const double l = sqrt(ddot(v1, v1));
@@ -459,7 +467,8 @@ __device__ void contact_geom_bwd(const World& w, const Consts& k, const AdjScrat
         }
     }
     // s_ia = pA + RA h_ia; s_ib = pB + RB h_ib (i = 1..3)
-    dm3 gRA = dm3zero(), gRB = dm3zero();
+    gRA = dm3zero();
+    gRB = dm3zero();
     for (int i = 1; i < 4; ++i) {
         gpA += gsa[i];
         gpB += gsb[i];
@@ -471,16 +480,30 @@ __device__ void contact_geom_bwd(const World& w, const Consts& k, const AdjScrat
         gRB.c1 += hb.y * gsb[i];
         gRB.c2 += hb.z * gsb[i];
     }
-    addd3(a.gp, ba, gpA);
-    addd3(a.gp, bb, gpB);
-    add_dm3(a.gR, ba, gRA);
-    add_dm3(a.gR, bb, gRB);
 }
 
 constexpr uint32_t kAdjWarps = 4;
+constexpr uint32_t kFixStride = 20;  // v3 w3 p3 R9 friction1
+
+// A contact side's contribution to a fixed body's gradients, kept with the
+// contact (fixed bodies are shared by contacts of one level).
+__device__ __forceinline__ double* fix_slot(const AdjScratch& a, uint32_t c, int side) {
+    return a.fix + (size_t(c) * 2 + side) * kFixStride;
+}
+__device__ __forceinline__ void fix_add3(double* f, int off, d3 v) {
+    f[off] += v.x;
+    f[off + 1] += v.y;
+    f[off + 2] += v.z;
+}
+__device__ __forceinline__ void fix_addR(double* f, const dm3& g) {
+    f[9] += g.c0.x; f[10] += g.c0.y; f[11] += g.c0.z;
+    f[12] += g.c1.x; f[13] += g.c1.y; f[14] += g.c1.z;
+    f[15] += g.c2.x; f[16] += g.c2.y; f[17] += g.c2.z;
+}
 
 __global__ void __launch_bounds__(kAdjWarps * 32)
     k_adjoint(World w, Consts k, Scratch s, AdjScratch a, Grads g, float dt) {
+    const unsigned full = 0xFFFFFFFFu;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t bundle = blockIdx.x * kAdjWarps + (threadIdx.x >> 5);
     if (bundle >= w.nbundles) return;
@@ -497,6 +520,7 @@ __global__ void __launch_bounds__(kAdjWarps * 32)
             a.gp[size_t(b) * 3 + j] = 0.0;
         }
         for (int j = 0; j < 9; ++j) a.gR[size_t(b) * 9 + j] = 0.0;
+        a.last[b] = 0;
     }
     // ---- contact constants (physics.comp:504-521, 533-546) ----
     for (uint32_t c = c0 + lane; c < c1; c += 32) {
@@ -520,16 +544,65 @@ __global__ void __launch_bounds__(kAdjWarps * 32)
         a.lam[c] = 0.f;
         a.glam[c] = 0.0;
         st_grad(a.gc, c, CGrad{dz(), dz(), dz(), 0.0, 0.0, 0.0});
+        double* f = fix_slot(a, c, 0);
+        for (uint32_t j = 0; j < 2 * kFixStride; ++j) f[j] = 0.0;
     }
     __syncwarp();
 
-    // ---- the PGS sweep recomputed in the reference order, taped ----
-    if (lane == 0 && ncb > 0) {
-        for (uint32_t it = 0; it < iters; ++it)
-            for (uint32_t c = c0; c < c1; ++c) {
+    // ---- wavefront levels: a contact comes after every earlier contact
+    // sharing a dynamic body with it, so contacts of one level touch disjoint
+    // dynamic bodies (the solver's rule; skipped contacts get no level) ----
+    uint32_t maxl = 0;
+    for (uint32_t cb = c0; cb < c1; cb += 32) {
+        const uint32_t c = cb + lane;
+        const bool valid = c < c1;
+        uint32_t ba = 0, bb = 0;
+        bool use = false, da = false, db = false;
+        if (valid) {
+            ba = w.geom_body[w.c_a[c]];
+            bb = w.geom_body[w.c_b[c]];
+            use = !(w.inv_mass[ba] == 0.0f && w.inv_mass[bb] == 0.0f);  // physics.comp:531
+            da = use && !load_body(w, ba).fixed;
+            db = use && !load_body(w, bb).fixed;
+        }
+        const uint32_t xa = da ? ba : (0x80000000u | (lane * 2u));
+        const uint32_t xb = db ? bb : (0x80000000u | (lane * 2u + 1u));
+        uint32_t L = use ? max(da ? a.last[ba] : 0u, db ? a.last[bb] : 0u) + 1u : 0u;
+        for (uint32_t j = 0; j < 32; ++j) {
+            const uint32_t aj = __shfl_sync(full, xa, j), bj = __shfl_sync(full, xb, j);
+            const uint32_t Lj = __shfl_sync(full, L, j);
+            if (use && j < lane && (aj == xa || aj == xb || bj == xa || bj == xb)) L = max(L, Lj + 1u);
+        }
+        if (da) atomicMax(&a.last[ba], L);
+        if (db) atomicMax(&a.last[bb], L);
+        if (valid) a.level[c] = use ? L - 1u : kNone;
+        maxl = max(maxl, L);
+        __syncwarp();
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) maxl = max(maxl, __shfl_xor_sync(full, maxl, off));
+    uint32_t* lvl = a.lvl + c0 + bundle;  // [maxl + 1], within [c0 + bundle, c1 + bundle]
+    uint32_t pos = 0;
+    for (uint32_t l = 0; l < maxl; ++l) {
+        if (lane == 0) lvl[l] = pos;
+        for (uint32_t cb = c0; cb < c1; cb += 32) {
+            const uint32_t c = cb + lane;
+            const bool hit = c < c1 && a.level[c] == l;
+            const unsigned m = __ballot_sync(full, hit);
+            if (hit) a.order[c0 + pos + __popc(m & ((1u << lane) - 1u))] = c;
+            pos += __popc(m);
+        }
+    }
+    if (lane == 0) lvl[maxl] = pos;
+    __syncwarp();
+
+    // ---- the PGS sweep recomputed level by level, taped ----
+    for (uint32_t it = 0; it < iters; ++it)
+        for (uint32_t l = 0; l < maxl; ++l) {
+            for (uint32_t j = lvl[l] + lane; j < lvl[l + 1]; j += 32) {
+                const uint32_t c = a.order[c0 + j];
                 const uint32_t ba = w.geom_body[w.c_a[c]], bb = w.geom_body[w.c_b[c]];
                 const Body A = load_body(w, ba), B = load_body(w, bb);
-                if (A.ima == 0.0f && B.ima == 0.0f) continue;  // physics.comp:531
                 f3 va = mk(a.vw[size_t(ba) * 6], a.vw[size_t(ba) * 6 + 1], a.vw[size_t(ba) * 6 + 2]);
                 f3 wa = mk(a.vw[size_t(ba) * 6 + 3], a.vw[size_t(ba) * 6 + 4], a.vw[size_t(ba) * 6 + 5]);
                 f3 vb = mk(a.vw[size_t(bb) * 6], a.vw[size_t(bb) * 6 + 1], a.vw[size_t(bb) * 6 + 2]);
@@ -543,15 +616,19 @@ __global__ void __launch_bounds__(kAdjWarps * 32)
                 t[12] = lam;
                 update_fwd(A, B, ld_par(a.par, c), va, wa, vb, wb, lam);
                 a.lam[c] = lam;
-                for (int j = 0; j < 3; ++j) {
-                    a.vw[size_t(ba) * 6 + j] = (&va.x)[j];
-                    a.vw[size_t(ba) * 6 + 3 + j] = (&wa.x)[j];
-                    a.vw[size_t(bb) * 6 + j] = (&vb.x)[j];
-                    a.vw[size_t(bb) * 6 + 3 + j] = (&wb.x)[j];
-                }
+                if (!A.fixed)
+                    for (int q = 0; q < 3; ++q) {
+                        a.vw[size_t(ba) * 6 + q] = (&va.x)[q];
+                        a.vw[size_t(ba) * 6 + 3 + q] = (&wa.x)[q];
+                    }
+                if (!B.fixed)
+                    for (int q = 0; q < 3; ++q) {
+                        a.vw[size_t(bb) * 6 + q] = (&vb.x)[q];
+                        a.vw[size_t(bb) * 6 + 3 + q] = (&wb.x)[q];
+                    }
             }
-    }
-    __syncwarp();
+            __syncwarp();
+        }
 
     // ---- integration (physics.comp:586-604), reversed ----
     for (uint32_t b = b0 + lane; b < b1; b += 32) {
@@ -598,33 +675,54 @@ __global__ void __launch_bounds__(kAdjWarps * 32)
     }
     __syncwarp();
 
-    if (lane == 0 && ncb > 0) {
-        // ---- the sweep, reversed ----
-        for (int it = int(iters) - 1; it >= 0; --it)
-            for (uint32_t c = c1; c-- > c0;) {
+    // ---- the sweep, reversed: levels in reverse order, the contacts of a
+    // level in parallel; a fixed side's gradient goes to the contact's slot ----
+    for (int it = int(iters) - 1; it >= 0; --it)
+        for (int l = int(maxl) - 1; l >= 0; --l) {
+            for (uint32_t j = lvl[l] + lane; j < lvl[l + 1]; j += 32) {
+                const uint32_t c = a.order[c0 + j];
                 const uint32_t ba = w.geom_body[w.c_a[c]], bb = w.geom_body[w.c_b[c]];
                 const Body A = load_body(w, ba), B = load_body(w, bb);
-                if (A.ima == 0.0f && B.ima == 0.0f) continue;
                 const float* t = a.tape + (size_t(c0) * iters + size_t(it) * ncb + (c - c0)) * 13;
-                d3 Gva = ldd3(a.gv, ba), Gwa = ldd3(a.gw, ba), Gvb = ldd3(a.gv, bb),
-                   Gwb = ldd3(a.gw, bb);
+                d3 Gva = A.fixed ? dz() : ldd3(a.gv, ba), Gwa = A.fixed ? dz() : ldd3(a.gw, ba);
+                d3 Gvb = B.fixed ? dz() : ldd3(a.gv, bb), Gwb = B.fixed ? dz() : ldd3(a.gw, bb);
                 double glam = a.glam[c];
                 CGrad gc = ld_grad(a.gc, c);
                 dm3 gRa = dm3zero(), gRb = dm3zero();
                 update_bwd(A, B, ld_par(a.par, c), mk(t[0], t[1], t[2]), mk(t[3], t[4], t[5]),
                            mk(t[6], t[7], t[8]), mk(t[9], t[10], t[11]), t[12], Gva, Gwa, Gvb, Gwb,
                            glam, gc, gRa, gRb);
-                std3(a.gv, ba, Gva);
-                std3(a.gw, ba, Gwa);
-                std3(a.gv, bb, Gvb);
-                std3(a.gw, bb, Gwb);
+                if (A.fixed) {
+                    double* f = fix_slot(a, c, 0);
+                    fix_add3(f, 0, Gva);
+                    fix_add3(f, 3, Gwa);
+                    fix_addR(f, gRa);
+                } else {
+                    std3(a.gv, ba, Gva);
+                    std3(a.gw, ba, Gwa);
+                    add_dm3(a.gR, ba, gRa);
+                }
+                if (B.fixed) {
+                    double* f = fix_slot(a, c, 1);
+                    fix_add3(f, 0, Gvb);
+                    fix_add3(f, 3, Gwb);
+                    fix_addR(f, gRb);
+                } else {
+                    std3(a.gv, bb, Gvb);
+                    std3(a.gw, bb, Gwb);
+                    add_dm3(a.gR, bb, gRb);
+                }
                 a.glam[c] = glam;
                 st_grad(a.gc, c, gc);
-                add_dm3(a.gR, ba, gRa);
-                add_dm3(a.gR, bb, gRb);
             }
-        // ---- contact constants and contact geometry, reversed ----
-        for (uint32_t c = c0; c < c1; ++c) {
+            __syncwarp();
+        }
+
+    // ---- contact constants and contact geometry, reversed (level order,
+    // which is contact order for the contacts of any one dynamic body) ----
+    for (uint32_t l = 0; l < maxl; ++l) {
+        for (uint32_t j = lvl[l] + lane; j < lvl[l + 1]; j += 32) {
+            const uint32_t c = a.order[c0 + j];
             const uint32_t ga = w.c_a[c], gb = w.c_b[c];
             const uint32_t ba = w.geom_body[ga], bb = w.geom_body[gb];
             const Body A = load_body(w, ba), B = load_body(w, bb);
@@ -654,27 +752,79 @@ __global__ void __launch_bounds__(kAdjWarps * 32)
             const double g_vn0 = (-vn0 < 0.f) ? 0.0 : -double(e) * gc.bias;
             gc.n += g_vn0 * D(sub(vb0, va0));
             const d3 g_ub0 = g_vn0 * n, g_ua0 = -g_ub0;
-            addd3(a.gv, ba, g_ua0);
-            addd3(a.gw, ba, dcross(ra, g_ua0));
             gc.ra += dcross(g_ua0, D(ld3(w.omega, ba)));
-            addd3(a.gv, bb, g_ub0);
-            addd3(a.gw, bb, dcross(rb, g_ub0));
             gc.rb += dcross(g_ub0, D(ld3(w.omega, bb)));
             // mu = sqrt(fa fb)
+            double gfa = 0.0, gfb = 0.0;
             if (p.mu > 0.f) {
                 const double fa = w.friction[ga], fb = w.friction[gb], mu = p.mu;
-                g.friction[ga] += gc.mu * fb / (2.0 * mu);
-                g.friction[gb] += gc.mu * fa / (2.0 * mu);
+                gfa = gc.mu * fb / (2.0 * mu);
+                gfb = gc.mu * fa / (2.0 * mu);
             }
-            // ra = cp - pos_a; rb = cp - pos_b
+            // ra = cp - pos_a; rb = cp - pos_b; the contact point, normal and
+            // depth through the taped support vertices
             const d3 g_cp = gc.ra + gc.rb;
-            addd3(a.gp, ba, -gc.ra);
-            addd3(a.gp, bb, -gc.rb);
-            add_dm3(a.gR, ba, gRa);
-            add_dm3(a.gR, bb, gRb);
-            contact_geom_bwd(w, k, a, c, ba, bb, gc.n, g_pen, g_cp);
+            d3 gpA, gpB;
+            dm3 gRA, gRB;
+            contact_geom_bwd(w, k, a, c, ba, bb, gc.n, g_pen, g_cp, gpA, gpB, gRA, gRB);
+            const d3 gva = g_ua0, gwa = dcross(ra, g_ua0), gvb = g_ub0, gwb = dcross(rb, g_ub0);
+            if (A.fixed) {
+                double* f = fix_slot(a, c, 0);
+                fix_add3(f, 0, gva);
+                fix_add3(f, 3, gwa);
+                fix_add3(f, 6, -gc.ra);
+                fix_add3(f, 6, gpA);
+                fix_addR(f, gRa);
+                fix_addR(f, gRA);
+                f[18] += gfa;
+            } else {  // the serial order of the additions, kept for bit-identical sums
+                addd3(a.gv, ba, gva);
+                addd3(a.gw, ba, gwa);
+                g.friction[ga] += gfa;
+                addd3(a.gp, ba, -gc.ra);
+                add_dm3(a.gR, ba, gRa);
+                addd3(a.gp, ba, gpA);
+                add_dm3(a.gR, ba, gRA);
+            }
+            if (B.fixed) {
+                double* f = fix_slot(a, c, 1);
+                fix_add3(f, 0, gvb);
+                fix_add3(f, 3, gwb);
+                fix_add3(f, 6, -gc.rb);
+                fix_add3(f, 6, gpB);
+                fix_addR(f, gRb);
+                fix_addR(f, gRB);
+                f[18] += gfb;
+            } else {
+                addd3(a.gv, bb, gvb);
+                addd3(a.gw, bb, gwb);
+                g.friction[gb] += gfb;
+                addd3(a.gp, bb, -gc.rb);
+                add_dm3(a.gR, bb, gRb);
+                addd3(a.gp, bb, gpB);
+                add_dm3(a.gR, bb, gRB);
+            }
         }
+        __syncwarp();
     }
+
+    // ---- fixed bodies: the kept contributions, in contact order ----
+    if (lane == 0)
+        for (uint32_t c = c0; c < c1; ++c) {
+            if (a.level[c] == kNone) continue;
+            for (int side = 0; side < 2; ++side) {
+                const uint32_t gi = side == 0 ? w.c_a[c] : w.c_b[c];
+                const uint32_t b = w.geom_body[gi];
+                if (!load_body(w, b).fixed) continue;
+                const double* f = fix_slot(a, c, side);
+                addd3(a.gv, b, d3{f[0], f[1], f[2]});
+                addd3(a.gw, b, d3{f[3], f[4], f[5]});
+                addd3(a.gp, b, d3{f[6], f[7], f[8]});
+                double* R = a.gR + size_t(b) * 9;
+                for (int q = 0; q < 9; ++q) R[q] += f[9 + q];
+                g.friction[gi] += f[18];
+            }
+        }
     __syncwarp();
 
     // ---- rotations -> quaternions, gravity (physics.comp:418-428), reversed

@@ -29,6 +29,14 @@ struct AdjScratch {
     double* glam;    // [max_contacts] dL/dλ
     float* lam;      // [max_contacts] λ during the recomputed sweep
     float* par;      // [max_contacts*12] contact constants (n, ra, rb, bias, kn, mu)
+    // wavefront levels of each bundle's contacts
+    uint32_t* last;  // [N] latest level per body
+    uint32_t* level; // [max_contacts]
+    uint32_t* order; // [max_contacts] contacts grouped by level
+    uint32_t* lvl;   // [max_contacts + max_scenes + 2] level boundaries per bundle
+    // contributions to fixed bodies' gradients, per contact and side (summed
+    // in contact order at the end): v3 w3 p3 R9 friction1 (stride 20)
+    double* fix;     // [max_contacts*40]
 };
 
 int launch_adjoint(const World& w, const Consts& k, const Scratch& s, const AdjScratch& a,

@@ -758,6 +758,11 @@ seevr_status seevr_physics_adjoint_substep(seevr_physics* h, uint32_t num_bodies
         if (st == SEEVR_OK) st = dev_alloc(h, &a.glam, nc);
         if (st == SEEVR_OK) st = dev_alloc(h, &a.lam, nc);
         if (st == SEEVR_OK) st = dev_alloc(h, &a.par, nc * 12);
+        if (st == SEEVR_OK) st = dev_alloc(h, &a.last, nb);
+        if (st == SEEVR_OK) st = dev_alloc(h, &a.level, nc);
+        if (st == SEEVR_OK) st = dev_alloc(h, &a.order, nc);
+        if (st == SEEVR_OK) st = dev_alloc(h, &a.lvl, nc + size_t(h->caps.max_scenes) + 2);
+        if (st == SEEVR_OK) st = dev_alloc(h, &a.fix, nc * 40);
         if (st != SEEVR_OK) return st;
         h->adj_ready = true;
     }

@@ -112,6 +112,7 @@ struct Scratch {
     float* s_n;             // [max_contacts*3] normals in solve order
     float* s_lam;           // [max_contacts] impulses of large bundles
     uint32_t* s_abp;        // [max_contacts*2] body pair in solve order
+    float4* s_rec;          // [max_contacts*kRecWords] per-contact solver records
     uint32_t* bundle_c0;    // [max_scenes + 1] first contact of each bundle
     // solver, per body (global-memory path for scenes too large for smem)
     float* s_R;             // [max_bodies*9]
@@ -165,5 +166,6 @@ int launch_solver_islands(const World& w, const Consts& k, const Scratch& s, uin
                           float dt, cudaStream_t st);
 // Scenes above this many bodies are solved by islands (when allocated).
 constexpr uint32_t kWarpMaxBodies = 1024;
+constexpr uint32_t kRecWords = 8;  // float4 words of a warp-solver contact record
 
 }  // namespace seevr

@@ -60,7 +60,8 @@ constexpr size_t kOffN = align256(kOffSceneOff + 8);
 constexpr size_t kOffLam = align256(kOffN + 12ull * kNaContacts);
 constexpr size_t kOffAbp = align256(kOffLam + 4ull * kNaContacts);
 constexpr size_t kOffBundleC0 = align256(kOffAbp + 8ull * kNaContacts);
-constexpr size_t kNaBytes = align256(kOffBundleC0 + 16);
+constexpr size_t kOffRec = align256(kOffBundleC0 + 16);
+constexpr size_t kNaBytes = align256(kOffRec + 16ull * kRecWords * kNaContacts);
 static_assert(kNaBytes == SEEVR_NOALLOC_SCRATCH_BYTES, "header constant out of date");
 
 // The scratch itself.  In host code this name is a host-side stand-in, not
@@ -197,6 +198,7 @@ extern "C" seevr_status seevr_physics_step_noalloc(
     s.s_lam = reinterpret_cast<float*>(at(kOffLam));
     s.s_abp = reinterpret_cast<uint32_t*>(at(kOffAbp));
     s.bundle_c0 = reinterpret_cast<uint32_t*>(at(kOffBundleC0));
+    s.s_rec = reinterpret_cast<float4*>(at(kOffRec));
     uint32_t* body_scene = reinterpret_cast<uint32_t*>(at(kOffBodyScene));
     uint32_t* scene_off = reinterpret_cast<uint32_t*>(at(kOffSceneOff));
 

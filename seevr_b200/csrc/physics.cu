@@ -465,6 +465,7 @@ seevr_status seevr_physics_create(const seevr_bindings* b, const seevr_caps* cap
     ALLOC(h->s.s_n, size_t(c.max_contacts) * 3);
     ALLOC(h->s.s_lam, c.max_contacts);
     ALLOC(h->s.s_abp, size_t(c.max_contacts) * 2);
+    ALLOC(h->s.s_rec, size_t(c.max_contacts) * kRecWords);
     ALLOC(h->s.bundle_c0, size_t(c.max_scenes) + 2);
     ALLOC(h->body_bundle, c.max_bodies);
     ALLOC(h->s.s_R, size_t(c.max_bodies) * 9);

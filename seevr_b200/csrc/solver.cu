@@ -206,7 +206,24 @@ __global__ void k_bundle_ranges(World w, uint32_t* __restrict__ bundle_c0) {
 // later lane sharing a dynamic body with lane j moves past lane j's level.
 constexpr uint32_t kWarpsPerBlock = 4;
 constexpr uint32_t kWarpLamCap = 1024;   // impulses per bundle held in smem
-constexpr uint32_t kWarpLevelCap = 128;  // level boundaries held in smem
+constexpr uint32_t kWarpLevelCap = 128;  // passes held in smem
+constexpr uint32_t kPassShift = 26, kPassMask = (1u << kPassShift) - 1u;
+
+// A contact's record (kRecWords float4, 128 bytes): n ra rb bias kn mu,
+// both bodies' quaternion, inverse inertia and inverse mass, the bundle-local
+// body indices and the fixed flags (bit 0: a, bit 1: b).
+__device__ __forceinline__ void load_rec(const float4* __restrict__ src, float4 (&r)[kRecWords]) {
+#pragma unroll
+    for (uint32_t j = 0; j < kRecWords; ++j) r[j] = src[j];
+}
+__device__ __forceinline__ void solve_rec(float* V, float* W, const float4 (&r)[kRecWords], float* lam) {
+    const uint32_t fl = __float_as_uint(r[7].z);
+    solve_core(V, W, __float_as_uint(r[7].x), __float_as_uint(r[7].y), (fl & 1u) != 0,
+               (fl & 2u) != 0, r[6].z, r[6].w, quat_to_mat(r[3].x, r[3].y, r[3].z, r[3].w),
+               quat_to_mat(r[4].x, r[4].y, r[4].z, r[4].w), mk(r[5].x, r[5].y, r[5].z),
+               mk(r[5].w, r[6].x, r[6].y), mk(r[0].x, r[0].y, r[0].z), mk(r[0].w, r[1].x, r[1].y),
+               mk(r[1].z, r[1].w, r[2].x), r[2].y, r[2].z, r[2].w, lam);
+}
 
 __host__ __device__ constexpr uint32_t warp_smem_words(uint32_t nbmax) {
     return 7 * nbmax + kWarpLamCap + kWarpLevelCap;
@@ -234,17 +251,15 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
     uint32_t* last = in_smem ? reinterpret_cast<uint32_t*>(base + 6 * nbmax) : s.s_last + b0;
     float* lam = ncb <= kWarpLamCap ? base + 7 * nbmax : s.s_lam + c0;
     uint32_t* lvl_sm = reinterpret_cast<uint32_t*>(base + 7 * nbmax + kWarpLamCap);
-    float* R = s.s_R + size_t(b0) * 9;
     for (uint32_t i = lane; i < nbs; i += 32) {
         if (in_smem) {
             st3(V, i, ld3(w.vel, b0 + i));
             st3(Wv, i, ld3(w.omega, b0 + i));
         }
-        st_m3(R, i, quat_to_mat(w.quat, b0 + i));
         last[i] = 0;
     }
     __syncwarp();
-    BodyView B{V, Wv, R, w.inv_inertia + size_t(b0) * 3, w.inv_mass + b0};
+    BodyView B{V, Wv, nullptr, w.inv_inertia + size_t(b0) * 3, w.inv_mass + b0};
 
     // ---- bodies of each contact; both inverse masses zero -> skipped (531)
     for (uint32_t c = c0 + lane; c < c1; c += 32) {
@@ -323,11 +338,14 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) maxl = max(maxl, __shfl_xor_sync(full, maxl, off));
 
-    // ---- positions: contacts grouped by level, index order within a level
-    uint32_t* lvl = maxl < kWarpLevelCap ? lvl_sm : s.s_lvl_start + c0 + bundle;
-    uint32_t pos = 0;
+    // ---- positions: contacts grouped by level, index order within a level;
+    // passes: runs of at most 32 positions of one level (start | count << 26),
+    // the unit the lanes solve together.  A pass holds at least one contact,
+    // so the passes fit in [c0 + bundle, c1 + bundle] of s_lvl_start.
+    uint32_t* gpass = s.s_lvl_start + c0 + bundle;
+    uint32_t pos = 0, npass = 0;
     for (uint32_t l = 0; l < maxl; ++l) {
-        if (lane == 0) lvl[l] = pos;
+        const uint32_t beg = pos;
         for (uint32_t cb = c0; cb < c1; cb += 32) {
             const uint32_t c = cb + lane;
             const bool hit = c < c1 && s.s_level[c] == l;
@@ -335,14 +353,21 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
             if (hit) s.s_order[c0 + pos + __popc(m & ((1u << lane) - 1u))] = c;
             pos += __popc(m);
         }
+        for (uint32_t q = beg + lane * 32; q < pos; q += 32 * 32)
+            gpass[npass + (q - beg) / 32] = q | (min(32u, pos - q) << kPassShift);
+        npass += (pos - beg + 31) / 32;
     }
-    if (lane == 0) lvl[maxl] = pos;
     __syncwarp();
+    const bool pass_sm = npass <= kWarpLevelCap;
+    if (pass_sm)
+        for (uint32_t j = lane; j < npass; j += 32) lvl_sm[j] = gpass[j];
+    const uint32_t* pass = pass_sm ? lvl_sm : gpass;
 
-    // ---- per-contact constants in position order (physics.comp:504-521,
-    // 533-546), from the pre-solve velocities
+    // ---- per-contact records in position order (physics.comp:504-521,
+    // 533-546): the constants, computed from the pre-solve velocities, and
+    // both bodies' data, so a sweep step issues one run of loads
     for (uint32_t i = lane; i < pos; i += 32) {
-        const uint32_t c = s.s_order[c0 + i], q = c0 + i;
+        const uint32_t c = s.s_order[c0 + i];
         const uint32_t ga = w.c_a[c], gb = w.c_b[c];
         const uint32_t la = s.s_ab[size_t(c) * 2], lb = s.s_ab[size_t(c) * 2 + 1];
         const uint32_t a = b0 + la, b = b0 + lb;
@@ -354,44 +379,57 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
         const float e = gmax(w.restitution[ga], w.restitution[gb]);
         const float bias = k.baumgarte * gmax(w.c_pen[c] - k.slop, 0.0f) / dt + e * gmax(-vn, 0.0f);
         const float ima = B.invm[la], imb = B.invm[lb];
-        const m3 Ra = ld_m3(B.R, la), Rb = ld_m3(B.R, lb);
+        const float4 qa = make_float4(w.quat[size_t(a) * 4], w.quat[size_t(a) * 4 + 1],
+                                      w.quat[size_t(a) * 4 + 2], w.quat[size_t(a) * 4 + 3]);
+        const float4 qb = make_float4(w.quat[size_t(b) * 4], w.quat[size_t(b) * 4 + 1],
+                                      w.quat[size_t(b) * 4 + 2], w.quat[size_t(b) * 4 + 3]);
+        const m3 Ra = quat_to_mat(qa.x, qa.y, qa.z, qa.w), Rb = quat_to_mat(qb.x, qb.y, qb.z, qb.w);
+        const f3 Ia = ld3(B.invI, la), Ib = ld3(B.invI, lb);
         const f3 ran = cross(ra, n), rbn = cross(rb, n);
-        const float kn = ima + imb + dot(ran, apply_inv_I(Ra, ld3(B.invI, la), ran)) +
-                         dot(rbn, apply_inv_I(Rb, ld3(B.invI, lb), rbn));
-        st3(s.s_n, q, n);
-        st3(s.s_ra, q, ra);
-        st3(s.s_rb, q, rb);
-        s.s_bias[q] = bias;
-        s.s_kn[q] = kn;
-        s.s_mu[q] = sqrtf(w.friction[ga] * w.friction[gb]);
-        s.s_abp[size_t(q) * 2] = la;
-        s.s_abp[size_t(q) * 2 + 1] = lb;
+        const float kn = ima + imb + dot(ran, apply_inv_I(Ra, Ia, ran)) + dot(rbn, apply_inv_I(Rb, Ib, rbn));
+        float4* r = s.s_rec + size_t(c0 + i) * kRecWords;
+        r[0] = make_float4(n.x, n.y, n.z, ra.x);
+        r[1] = make_float4(ra.y, ra.z, rb.x, rb.y);
+        r[2] = make_float4(rb.z, bias, kn, sqrtf(w.friction[ga] * w.friction[gb]));
+        r[3] = qa;
+        r[4] = qb;
+        r[5] = make_float4(Ia.x, Ia.y, Ia.z, Ib.x);
+        r[6] = make_float4(Ib.y, Ib.z, ima, imb);
+        r[7] = make_float4(__uint_as_float(la), __uint_as_float(lb),
+                           __uint_as_float((is_fixed(B, la) ? 1u : 0u) | (is_fixed(B, lb) ? 2u : 0u)),
+                           0.0f);
         lam[i] = 0.0f;
     }
     __syncwarp();
 
     // ---- Gauss-Seidel sweeps ----
     if (mode == 0) {
-        if (lane == 0)
+        if (lane == 0) {
+            float4 r[kRecWords];
             for (uint32_t it = 0; it < k.pgs_iterations; ++it)
                 for (uint32_t i = 0; i < pos; ++i) {
-                    const uint32_t q = c0 + i;
-                    solve_one(B, s.s_abp[size_t(q) * 2], s.s_abp[size_t(q) * 2 + 1], ld3(s.s_n, q),
-                              ld3(s.s_ra, q), ld3(s.s_rb, q), s.s_bias[q], s.s_kn[q], s.s_mu[q],
-                              &lam[i]);
+                    load_rec(s.s_rec + size_t(c0 + i) * kRecWords, r);
+                    solve_rec(V, Wv, r, &lam[i]);
                 }
-    } else {
-        for (uint32_t it = 0; it < k.pgs_iterations; ++it) {
-            for (uint32_t l = 0; l < maxl; ++l) {
-                const uint32_t beg = lvl[l], end = lvl[l + 1];
-                for (uint32_t i = beg + lane; i < end; i += 32) {
-                    const uint32_t q = c0 + i;
-                    solve_one(B, s.s_abp[size_t(q) * 2], s.s_abp[size_t(q) * 2 + 1], ld3(s.s_n, q),
-                              ld3(s.s_ra, q), ld3(s.s_rb, q), s.s_bias[q], s.s_kn[q], s.s_mu[q],
-                              &lam[i]);
-                }
-                __syncwarp();
-            }
+        }
+    } else if (npass > 0) {
+        // the next pass's records are loaded while this pass solves
+        float4 cur[kRecWords], nxt[kRecWords];
+        uint32_t pe = pass[0];
+        if (lane < (pe >> kPassShift))
+            load_rec(s.s_rec + size_t(c0 + (pe & kPassMask) + lane) * kRecWords, nxt);
+        const uint32_t total = k.pgs_iterations * npass;
+        uint32_t p = 0;
+        for (uint32_t t = 0; t < total; ++t) {
+#pragma unroll
+            for (uint32_t j = 0; j < kRecWords; ++j) cur[j] = nxt[j];
+            const uint32_t ce = pe;
+            p = p + 1 == npass ? 0u : p + 1;
+            pe = pass[p];
+            if (t + 1 < total && lane < (pe >> kPassShift))
+                load_rec(s.s_rec + size_t(c0 + (pe & kPassMask) + lane) * kRecWords, nxt);
+            if (lane < (ce >> kPassShift)) solve_rec(V, Wv, cur, &lam[(ce & kPassMask) + lane]);
+            __syncwarp();
         }
     }
     __syncwarp();

@@ -19,13 +19,14 @@ __device__ __forceinline__ bool is_fixed(const BodyView& B, uint32_t i) {
            B.invI[i * 3 + 2] == 0.0f;
 }
 
-// One normal + friction update of contact c (physics.comp:525-580).
-__device__ __forceinline__ void solve_one(const BodyView& B, uint32_t la, uint32_t lb, f3 n, f3 ra,
-                                          f3 rb, float bias, float kn, float mu, float* lam) {
-    const float ima = B.invm[la], imb = B.invm[lb];
-    const m3 Ra = ld_m3(B.R, la), Rb = ld_m3(B.R, lb);
-    const f3 Ia = ld3(B.invI, la), Ib = ld3(B.invI, lb);
-    f3 va = ld3(B.v, la), wa = ld3(B.w, la), vb = ld3(B.v, lb), wb = ld3(B.w, lb);
+// One normal + friction update of contact c (physics.comp:525-580), given
+// the two bodies' constant data; v, w: velocities and angular velocities,
+// indexed by la / lb; a fixed body's velocities are not written.
+__device__ __forceinline__ void solve_core(float* V, float* W, uint32_t la, uint32_t lb, bool fixed_a,
+                                           bool fixed_b, float ima, float imb, const m3& Ra,
+                                           const m3& Rb, f3 Ia, f3 Ib, f3 n, f3 ra, f3 rb,
+                                           float bias, float kn, float mu, float* lam) {
+    f3 va = ld3(V, la), wa = ld3(W, la), vb = ld3(V, lb), wb = ld3(W, lb);
     f3 ua = add(va, cross(wa, ra)), ub = add(vb, cross(wb, rb));
     const float vn = dot(sub(ub, ua), n);
     float d_ln = (-vn + bias) / kn;
@@ -55,14 +56,21 @@ __device__ __forceinline__ void solve_one(const BodyView& B, uint32_t la, uint32
         wa = add(wa, apply_inv_I(Ra, Ia, cross(ra, it)));
         wb = sub(wb, apply_inv_I(Rb, Ib, cross(rb, it)));
     }
-    if (!is_fixed(B, la)) {
-        st3(B.v, la, va);
-        st3(B.w, la, wa);
+    if (!fixed_a) {
+        st3(V, la, va);
+        st3(W, la, wa);
     }
-    if (!is_fixed(B, lb)) {
-        st3(B.v, lb, vb);
-        st3(B.w, lb, wb);
+    if (!fixed_b) {
+        st3(V, lb, vb);
+        st3(W, lb, wb);
     }
+}
+
+__device__ __forceinline__ void solve_one(const BodyView& B, uint32_t la, uint32_t lb, f3 n, f3 ra,
+                                          f3 rb, float bias, float kn, float mu, float* lam) {
+    solve_core(B.v, B.w, la, lb, is_fixed(B, la), is_fixed(B, lb), B.invm[la], B.invm[lb],
+               ld_m3(B.R, la), ld_m3(B.R, lb), ld3(B.invI, la), ld3(B.invI, lb), n, ra, rb, bias,
+               kn, mu, lam);
 }
 
 }  // namespace seevr

@@ -8,11 +8,21 @@
 // (i, j) lexicographic order.  Pairs beyond max_pairs are dropped while the
 // total keeps counting, as in the reference (physics.comp:465-466).
 //
-// One warp per row: lanes test 32 consecutive columns at a time and the
-// ballot/popc prefix gives each hit its slot in ascending-j order.  The
-// count pass keeps each 32-column ballot word in a per-row mask array (when
-// the library could size it for the largest scene), so the write pass reads
-// the words back instead of re-testing, and stops at the row's count.
+// Rows are processed by warps: lanes test 32 consecutive columns at a time
+// and the ballot/popc prefix gives each hit its slot in ascending-j order.
+// The count pass keeps each 32-column ballot word in a per-row mask array
+// (when the library could size it for the largest scene), so the write pass
+// reads the words back instead of re-testing.
+//
+// Scenes of at most kTileBodies bodies (k_broad_tile): each of a scene's
+// blocks (one per kTileRows rows) stages the scene's AABBs and static flags
+// in shared memory, so a column test reads shared memory only; the scene's
+// rows are dealt out to the warps of its blocks in turn (row work shrinks
+// with the row index, so consecutive rows go to different warps).  The write
+// pass loads a row's overlap words with one coalesced load and places the
+// hits with a warp prefix sum over the words' population counts.  Larger
+// scenes use one warp per row reading the AABBs from global memory
+// (k_broad_n2).
 #include "common.cuh"
 
 namespace seevr {
@@ -70,8 +80,128 @@ __global__ void __launch_bounds__(256) k_broad_n2(World w, const uint32_t* __res
     if (!kWrite && lane == 0) row_count[i] = count;
 }
 
-int launch_broadphase_n2(const World& w, const Scratch& s, cudaStream_t st) {
+constexpr uint32_t kTileThreads = 256, kTileWarps = kTileThreads / 32;
+
+template <bool kWrite>
+__global__ void __launch_bounds__(kTileThreads)
+    k_broad_tile(World w, const uint2* __restrict__ tiles, uint32_t uniform_slices,
+                 const uint32_t* __restrict__ row_off, uint32_t* __restrict__ row_count,
+                 uint32_t* __restrict__ mask, uint32_t stride) {
+    extern __shared__ float sm[];
+    uint32_t scene, slice, slices;
+    if (tiles) {
+        const uint2 t = tiles[blockIdx.x];
+        scene = t.x;
+        slice = t.y & 0xFFFFu;
+        slices = t.y >> 16;
+    } else {
+        scene = blockIdx.x / uniform_slices;
+        slice = blockIdx.x % uniform_slices;
+        slices = uniform_slices;
+    }
+    const uint32_t s0 = w.scene_off[scene], s1 = w.scene_off[scene + 1];
+    const uint32_t n = s1 - s0;
+    const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+    const bool test = !kWrite || !mask;  // this pass evaluates the overlap tests
+    float* mn = sm;
+    float* mx = sm + 3 * n;
+    float* stat = sm + 6 * n;  // 1: inv_mass <= 0
+    if (test) {
+        for (uint32_t t = threadIdx.x; t < 3 * n; t += kTileThreads) {
+            mn[t] = w.aabb_min[size_t(s0) * 3 + t];
+            mx[t] = w.aabb_max[size_t(s0) * 3 + t];
+        }
+        for (uint32_t t = threadIdx.x; t < n; t += kTileThreads)
+            stat[t] = w.inv_mass[s0 + t] <= 0.0f ? 1.0f : 0.0f;
+        __syncthreads();
+    }
+    const unsigned below = (1u << lane) - 1u;
+    for (uint32_t r = slice * kTileWarps + wid; r < n; r += slices * kTileWarps) {
+        const uint32_t i = s0 + r;
+        const uint32_t ncol = n - r - 1;  // columns j = i+1 .. s1-1
+        const uint32_t nch = (ncol + 31) / 32;
+        uint32_t* mrow = mask ? mask + size_t(i) * stride : nullptr;
+        if (!kWrite) {
+            const f3 mna = ld3(mn, r), mxa = ld3(mx, r);
+            const bool static_i = stat[r] != 0.0f;
+            uint32_t count = 0;
+            for (uint32_t ch = 0; ch < nch; ++ch) {
+                const uint32_t jl = r + 1 + 32 * ch + lane;  // scene-local column
+                const bool hit = jl < n && !(static_i && stat[jl] != 0.0f) &&
+                                 overlap(mna, mxa, ld3(mn, jl), ld3(mx, jl));
+                const unsigned m = __ballot_sync(0xFFFFFFFFu, hit);
+                if (mrow && lane == 0) mrow[ch] = m;
+                count += __popc(m);
+            }
+            if (lane == 0) row_count[i] = count;
+        } else {
+            const uint32_t total = row_count[i];
+            if (total == 0) continue;
+            const f3 mna = test ? ld3(mn, r) : mk(0.f, 0.f, 0.f);
+            const f3 mxa = test ? ld3(mx, r) : mna;
+            const bool static_i = test && stat[r] != 0.0f;
+            uint32_t slot0 = row_off[i];
+            for (uint32_t c0 = 0; c0 < nch; c0 += 32) {
+                // lane l holds word c0 + l
+                unsigned word = 0;
+                if (mrow) {
+                    if (c0 + lane < nch) word = mrow[c0 + lane];
+                } else {
+                    for (uint32_t q = 0; q < 32 && c0 + q < nch; ++q) {
+                        const uint32_t jl = r + 1 + 32 * (c0 + q) + lane;
+                        const bool hit = jl < n && !(static_i && stat[jl] != 0.0f) &&
+                                         overlap(mna, mxa, ld3(mn, jl), ld3(mx, jl));
+                        const unsigned m = __ballot_sync(0xFFFFFFFFu, hit);
+                        if (lane == q) word = m;
+                    }
+                }
+                // exclusive prefix of the words' population counts
+                const uint32_t pc = __popc(word);
+                uint32_t incl = pc;
+#pragma unroll
+                for (int off = 1; off < 32; off <<= 1) {
+                    const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, off);
+                    if (int(lane) >= off) incl += v;
+                }
+                const uint32_t excl = incl - pc;
+                unsigned nz = __ballot_sync(0xFFFFFFFFu, word != 0u);
+                while (nz) {
+                    const uint32_t q = uint32_t(__ffs(int(nz))) - 1u;
+                    nz &= nz - 1u;
+                    const unsigned m = __shfl_sync(0xFFFFFFFFu, word, q);
+                    const uint32_t pre = __shfl_sync(0xFFFFFFFFu, excl, q);
+                    if ((m >> lane) & 1u) {
+                        const uint32_t slot = slot0 + pre + __popc(m & below);
+                        if (slot < w.max_pairs) {
+                            w.pairs[size_t(slot) * 2] = i;
+                            w.pairs[size_t(slot) * 2 + 1] = i + 1 + 32 * (c0 + q) + lane;
+                        }
+                    }
+                }
+                slot0 += __shfl_sync(0xFFFFFFFFu, incl, 31);
+            }
+        }
+    }
+}
+
+int launch_broadphase_n2(const World& w, const Scratch& s, uint32_t max_scene_bodies,
+                         cudaStream_t st) {
     if (w.nb == 0) return 0;
+    if (max_scene_bodies <= kTileBodies && w.ns > 0) {
+        // one block per kTileRows rows of each scene (the tile table), or
+        // without a table the largest scene's block count for every scene
+        const uint32_t slices = max(1u, (max_scene_bodies + kTileRows - 1) / kTileRows);
+        const uint2* tiles = s.bp_ntiles ? s.bp_tiles : nullptr;
+        const uint32_t blocks = tiles ? s.bp_ntiles : w.ns * slices;
+        const size_t smem = size_t(7) * max_scene_bodies * sizeof(float);
+        k_broad_tile<false><<<blocks, kTileThreads, smem, st>>>(w, tiles, slices, nullptr,
+                                                                s.row_count, s.bp_mask, s.bp_stride);
+        launch_exclusive_scan(s.row_count, s.row_off, nullptr, w.nb, &w.counters[0], w.max_pairs,
+                              kFlagPairOverflow, s, st);
+        k_broad_tile<true><<<blocks, kTileThreads, s.bp_mask ? 0 : smem, st>>>(
+            w, tiles, slices, s.row_off, s.row_count, s.bp_mask, s.bp_stride);
+        return 3;
+    }
     const uint32_t threads = 256;
     const uint32_t blocks = uint32_t((uint64_t(w.nb) * 32 + threads - 1) / threads);
     k_broad_n2<false><<<blocks, threads, 0, st>>>(w, nullptr, s.row_count, s.bp_mask, s.bp_stride);
@@ -79,6 +209,14 @@ int launch_broadphase_n2(const World& w, const Scratch& s, cudaStream_t st) {
                           kFlagPairOverflow, s, st);
     k_broad_n2<true><<<blocks, threads, 0, st>>>(w, s.row_off, s.row_count, s.bp_mask, s.bp_stride);
     return 3;
+}
+
+cudaError_t init_broadphase() {
+    const int bytes = int(7 * kTileBodies * sizeof(float));
+    const cudaError_t e =
+        cudaFuncSetAttribute(k_broad_tile<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_broad_tile<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
 }  // namespace seevr

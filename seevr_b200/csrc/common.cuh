@@ -122,6 +122,10 @@ struct Scratch {
     // count pass (NULL: the write pass re-tests)
     uint32_t* bp_mask;      // [rows * bp_stride]
     uint32_t bp_stride;     // words per row
+    // all-pairs broadphase blocks: (scene, slice | slices << 16) per block
+    // (NULL: every scene gets the slices of the largest)
+    uint2* bp_tiles;
+    uint32_t bp_ntiles;
     IslandScratch isl;
 };
 
@@ -144,7 +148,13 @@ int launch_body_stage(const World& w, const Consts& k, uint32_t flags, float dt,
 int launch_exclusive_scan(const uint32_t* in, uint32_t* out, const uint32_t* n_dev,
                           uint32_t n_cap, uint32_t* total_out, uint32_t total_cap,
                           uint32_t overflow_bit, const Scratch& s, cudaStream_t st);
-int launch_broadphase_n2(const World& w, const Scratch& s, cudaStream_t st);
+int launch_broadphase_n2(const World& w, const Scratch& s, uint32_t max_scene_bodies,
+                         cudaStream_t st);
+cudaError_t init_broadphase();
+// all-pairs broadphase on shared-memory tiles: scenes up to kTileBodies
+// bodies, one block per kTileRows rows of a scene
+constexpr uint32_t kTileBodies = 2048;
+constexpr uint32_t kTileRows = 64;
 int launch_narrowphase(const World& w, const Consts& k, const Scratch& s, cudaStream_t st);
 // Narrowphase that also tapes the supporting hull vertices of each contact's
 // final portal (2 uint4 per pair / contact) for the adjoint.

@@ -80,6 +80,7 @@ void setup_device(int dev) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e == cudaSuccess) e = init_solver();
+    if (e == cudaSuccess) e = init_broadphase();
     g_setup_err[dev] = e;
     g_dev_ptr[dev] = e == cudaSuccess ? static_cast<unsigned char*>(p) : nullptr;
 }
@@ -269,7 +270,7 @@ extern "C" seevr_status seevr_physics_step_noalloc(
     for (uint32_t sub = 0; sub < substeps; ++sub) {
         launch_body_stage(w, k, (sub > 0 ? kIntegrate : 0u) | kGravity | kAabb, sub_dt, gravity[0],
                           gravity[1], gravity[2], st);
-        launch_broadphase_n2(w, s, st);
+        launch_broadphase_n2(w, s, num_bodies, st);
         launch_narrowphase(w, k, s, st);
         cudaMemsetAsync(w.lambda, 0, sizeof(float) * max_contacts, st);
         launch_solver(w, k, s, mode, sub_dt, num_bodies, num_bodies, st);

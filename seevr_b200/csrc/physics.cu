@@ -111,6 +111,8 @@ struct seevr_physics {
     bool adj_ready = false;
     // broadphase overlap words (s.bp_mask), sized for the scene layout
     size_t bp_mask_cap = 0;
+    // broadphase tile table (s.bp_tiles) capacity, in tiles
+    uint32_t bp_tiles_cap = 0;
 };
 
 namespace {
@@ -132,6 +134,8 @@ void free_all(seevr_physics* h) {
     if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
     if (h->s.bp_mask) cudaFree(h->s.bp_mask);
     h->s.bp_mask = nullptr;
+    if (h->s.bp_tiles) cudaFree(h->s.bp_tiles);
+    h->s.bp_tiles = nullptr;
     for (void* p : h->allocations) cudaFree(p);
     h->allocations.clear();
     for (auto& e : h->ev)
@@ -285,7 +289,7 @@ uint64_t issue_frame(seevr_physics* h, uint32_t nb, uint32_t nv, uint32_t nhv, u
         T.begin();
         n += h->params.broadphase == SEEVR_BROADPHASE_LBVH
                  ? launch_broadphase_lbvh(w, h->s, h->lb, st)
-                 : launch_broadphase_n2(w, h->s, st);
+                 : launch_broadphase_n2(w, h->s, h->max_scene_bodies, st);
         T.end(kStBroad);
         T.begin();
         n += launch_narrowphase(w, h->k, h->s, st);
@@ -351,6 +355,37 @@ seevr_status ensure_bp_mask(seevr_physics* h, uint32_t nb, uint32_t maxs) {
         h->bp_mask_cap = words;
     }
     h->s.bp_stride = stride;
+    return SEEVR_OK;
+}
+
+// Tile table of the all-pairs broadphase: ceil(n / kTileRows) blocks for a
+// scene of n bodies, so that large scenes are spread over as many warps as
+// their rows need (only for layouts the shared-memory kernel takes).
+seevr_status set_bp_tiles(seevr_physics* h, const uint32_t* body_offset, uint32_t num_scenes,
+                          uint32_t maxs) {
+    h->s.bp_ntiles = 0;
+    if (maxs > kTileBodies) return SEEVR_OK;
+    std::vector<uint2> tiles;
+    for (uint32_t s = 0; s < num_scenes; ++s) {
+        const uint32_t n = body_offset[s + 1] - body_offset[s];
+        const uint32_t k = std::max(1u, (n + kTileRows - 1) / kTileRows);
+        for (uint32_t j = 0; j < k; ++j) tiles.push_back(make_uint2(s, j | (k << 16)));
+    }
+    if (tiles.size() > h->bp_tiles_cap) {
+        if (h->s.bp_tiles) cudaFree(h->s.bp_tiles);
+        h->s.bp_tiles = nullptr;
+        h->bp_tiles_cap = 0;
+        void* q = nullptr;
+        if (cudaMalloc(&q, tiles.size() * sizeof(uint2)) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(SEEVR_ERR_OUT_OF_MEMORY, "cudaMalloc of the broadphase tile table failed");
+        }
+        h->s.bp_tiles = static_cast<uint2*>(q);
+        h->bp_tiles_cap = uint32_t(tiles.size());
+    }
+    SEEVR_CUDA(cudaMemcpy(h->s.bp_tiles, tiles.data(), tiles.size() * sizeof(uint2),
+                          cudaMemcpyHostToDevice));
+    h->s.bp_ntiles = uint32_t(tiles.size());
     return SEEVR_OK;
 }
 
@@ -527,6 +562,8 @@ seevr_status seevr_physics_create(const seevr_bindings* b, const seevr_caps* cap
         st = fail(SEEVR_ERR_CUDA, "cudaMemset failed");
     if (st == SEEVR_OK && init_solver() != cudaSuccess)
         st = fail(SEEVR_ERR_CUDA, "cudaFuncSetAttribute for the solver failed");
+    if (st == SEEVR_OK && init_broadphase() != cudaSuccess)
+        st = fail(SEEVR_ERR_CUDA, "cudaFuncSetAttribute for the broadphase failed");
     if (st != SEEVR_OK) {
         cudaGetLastError();
         free_all(h);
@@ -567,6 +604,8 @@ seevr_status seevr_physics_set_scenes(seevr_physics* h, const uint32_t* body_off
                     "batches");
     const seevr_status ms = ensure_bp_mask(h, nb, maxs);
     if (ms != SEEVR_OK) return ms;
+    const seevr_status ts = set_bp_tiles(h, body_offset, num_scenes, maxs);
+    if (ts != SEEVR_OK) return ts;
     uint32_t max_bundle = 0;
     const uint32_t target = h->params.bundle_bodies ? h->params.bundle_bodies : 512u;
     const std::vector<uint32_t> bundles = make_bundles(body_offset, num_scenes, target, &max_bundle);
@@ -780,7 +819,7 @@ seevr_status seevr_physics_adjoint_substep(seevr_physics* h, uint32_t num_bodies
     // the substep's forward up to its contacts, in the order of issue_frame
     n += launch_body_stage(w, h->k, kGravity | kAabb, dt, gravity[0], gravity[1], gravity[2], s);
     n += h->params.broadphase == SEEVR_BROADPHASE_LBVH ? launch_broadphase_lbvh(w, h->s, h->lb, s)
-                                                       : launch_broadphase_n2(w, h->s, s);
+                                                       : launch_broadphase_n2(w, h->s, h->max_scene_bodies, s);
     n += launch_narrowphase_taped(w, h->k, h->s, a.ptape, a.ctape, s);
     n += launch_bundle_ranges(w, h->s, s);
     const Grads g{grads->pos, grads->quat, grads->vel, grads->omega, grads->friction};

@@ -208,6 +208,7 @@ constexpr uint32_t kWarpsPerBlock = 4;
 constexpr uint32_t kWarpLamCap = 1024;   // impulses per bundle held in smem
 constexpr uint32_t kWarpLevelCap = 128;  // passes held in smem
 constexpr uint32_t kPassShift = 26, kPassMask = (1u << kPassShift) - 1u;
+constexpr uint32_t kRegChunks = 8;  // contacts per lane kept in registers by the setup
 
 // A contact's record (kRecWords float4, 128 bytes): n ra rb bias kn mu,
 // both bodies' quaternion, inverse inertia and inverse mass, the bundle-local
@@ -216,6 +217,50 @@ __device__ __forceinline__ void load_rec(const float4* __restrict__ src, float4 
 #pragma unroll
     for (uint32_t j = 0; j < kRecWords; ++j) r[j] = src[j];
 }
+// Contact c's record at slot q (physics.comp:504-521, 533-546): the
+// constants, computed from the pre-solve velocities, and both bodies' data.
+__device__ __forceinline__ void write_rec(const World& w, const Consts& k, const Scratch& s,
+                                          const BodyView& B, uint32_t b0, uint32_t c, uint32_t la,
+                                          uint32_t lb, uint32_t q, float dt) {
+    const uint32_t ga = w.c_a[c], gb = w.c_b[c];
+    const uint32_t a = b0 + la, b = b0 + lb;
+    const f3 n = ld3(w.c_normal, c), cp = ld3(w.c_pos, c);
+    const f3 ra = sub(cp, ld3(w.pos, a)), rb = sub(cp, ld3(w.pos, b));
+    const f3 va = add(ld3(B.v, la), cross(ld3(B.w, la), ra));
+    const f3 vb = add(ld3(B.v, lb), cross(ld3(B.w, lb), rb));
+    const float vn = dot(sub(vb, va), n);
+    const float e = gmax(w.restitution[ga], w.restitution[gb]);
+    const float bias = k.baumgarte * gmax(w.c_pen[c] - k.slop, 0.0f) / dt + e * gmax(-vn, 0.0f);
+    const float ima = B.invm[la], imb = B.invm[lb];
+    const float4 qa = make_float4(w.quat[size_t(a) * 4], w.quat[size_t(a) * 4 + 1],
+                                  w.quat[size_t(a) * 4 + 2], w.quat[size_t(a) * 4 + 3]);
+    const float4 qb = make_float4(w.quat[size_t(b) * 4], w.quat[size_t(b) * 4 + 1],
+                                  w.quat[size_t(b) * 4 + 2], w.quat[size_t(b) * 4 + 3]);
+    const m3 Ra = quat_to_mat(qa.x, qa.y, qa.z, qa.w), Rb = quat_to_mat(qb.x, qb.y, qb.z, qb.w);
+    const f3 Ia = ld3(B.invI, la), Ib = ld3(B.invI, lb);
+    const f3 ran = cross(ra, n), rbn = cross(rb, n);
+    const float kn = ima + imb + dot(ran, apply_inv_I(Ra, Ia, ran)) + dot(rbn, apply_inv_I(Rb, Ib, rbn));
+    float4* r = s.s_rec + size_t(q) * kRecWords;
+    r[0] = make_float4(n.x, n.y, n.z, ra.x);
+    r[1] = make_float4(ra.y, ra.z, rb.x, rb.y);
+    r[2] = make_float4(rb.z, bias, kn, sqrtf(w.friction[ga] * w.friction[gb]));
+    r[3] = qa;
+    r[4] = qb;
+    r[5] = make_float4(Ia.x, Ia.y, Ia.z, Ib.x);
+    r[6] = make_float4(Ib.y, Ib.z, ima, imb);
+    r[7] = make_float4(__uint_as_float(la), __uint_as_float(lb),
+                       __uint_as_float((is_fixed(B, la) ? 1u : 0u) | (is_fixed(B, lb) ? 2u : 0u)),
+                       0.0f);
+}
+
+// Passes of the positions [beg, pos) of one level, from entry npass on.
+__device__ __forceinline__ uint32_t write_passes(uint32_t* gpass, uint32_t npass, uint32_t beg,
+                                                 uint32_t pos, uint32_t lane) {
+    for (uint32_t q = beg + lane * 32; q < pos; q += 32 * 32)
+        gpass[npass + (q - beg) / 32] = q | (min(32u, pos - q) << kPassShift);
+    return npass + (pos - beg + 31) / 32;
+}
+
 __device__ __forceinline__ void solve_rec(float* V, float* W, const float4 (&r)[kRecWords], float* lam) {
     const uint32_t fl = __float_as_uint(r[7].z);
     solve_core(V, W, __float_as_uint(r[7].x), __float_as_uint(r[7].y), (fl & 1u) != 0,
@@ -261,146 +306,175 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
     __syncwarp();
     BodyView B{V, Wv, nullptr, w.inv_inertia + size_t(b0) * 3, w.inv_mass + b0};
 
-    // ---- bodies of each contact; both inverse masses zero -> skipped (531)
-    for (uint32_t c = c0 + lane; c < c1; c += 32) {
-        const uint32_t la = w.geom_body[w.c_a[c]] - b0, lb = w.geom_body[w.c_b[c]] - b0;
-        const bool skip = B.invm[la] == 0.0f && B.invm[lb] == 0.0f;
-        s.s_ab[size_t(c) * 2] = skip ? kNone : la;
-        s.s_ab[size_t(c) * 2 + 1] = lb;
-    }
-    __syncwarp();
-
-    // ---- levels: colours (COLORED), wavefront levels (WAVEFRONT) or one
-    // level in index order (SEQUENTIAL)
-    uint32_t maxl = 0;
-    bool coloured = mode == 2;
-    if (coloured) {
-        // greedy colouring in contact order: the smallest colour not used by
-        // an earlier contact at either of its dynamic bodies (per-body colour
-        // masks in `last`); more than 32 colours at a body falls back to the
-        // wavefront levels
-        uint32_t ok = 1u, mx = 0u;
-        if (lane == 0) {
-            for (uint32_t c = c0; c < c1; ++c) {
-                const uint32_t la = s.s_ab[size_t(c) * 2], lb = s.s_ab[size_t(c) * 2 + 1];
-                if (la == kNone) {
-                    s.s_level[c] = kNone;
-                    continue;
-                }
-                const bool da = !is_fixed(B, la), db = !is_fixed(B, lb);
-                const uint32_t used = (da ? last[la] : 0u) | (db ? last[lb] : 0u);
-                if (used == 0xFFFFFFFFu) {
-                    ok = 0u;
-                    break;
-                }
-                const uint32_t col = uint32_t(__ffs(int(~used))) - 1u;
-                if (da) last[la] |= 1u << col;
-                if (db) last[lb] |= 1u << col;
-                s.s_level[c] = col;
-                mx = max(mx, col + 1u);
-            }
-        }
-        ok = __shfl_sync(full, ok, 0);
-        maxl = __shfl_sync(full, mx, 0);
-        if (!ok) {
-            coloured = false;
-            maxl = 0;
-            for (uint32_t i = lane; i < nbs; i += 32) last[i] = 0;
-        }
-        __syncwarp();
-    }
-    for (uint32_t cb = c0; !coloured && cb < c1; cb += 32) {
-        const uint32_t c = cb + lane;
-        const bool valid = c < c1;
-        const uint32_t la = valid ? s.s_ab[size_t(c) * 2] : kNone;
-        const uint32_t lb = valid ? s.s_ab[size_t(c) * 2 + 1] : 0u;
-        const bool use = valid && la != kNone;
-        uint32_t L = use ? 1u : 0u;
-        if (mode != 0) {
-            const bool da = use && !is_fixed(B, la), db = use && !is_fixed(B, lb);
-            // dynamic bodies, or a sentinel unique to this lane and role
-            const uint32_t xa = da ? la : (0x80000000u | (lane * 2u));
-            const uint32_t xb = db ? lb : (0x80000000u | (lane * 2u + 1u));
-            if (use) L = max(da ? last[la] : 0u, db ? last[lb] : 0u) + 1u;
-            for (uint32_t j = 0; j < 32; ++j) {
-                const uint32_t aj = __shfl_sync(full, xa, j), bj = __shfl_sync(full, xb, j);
-                const uint32_t Lj = __shfl_sync(full, L, j);
-                if (use && j < lane && (aj == xa || aj == xb || bj == xa || bj == xb))
-                    L = max(L, Lj + 1u);
-            }
-            if (da) atomicMax(&last[la], L);
-            if (db) atomicMax(&last[lb], L);
-        }
-        if (valid) s.s_level[c] = use ? L - 1u : kNone;
-        maxl = max(maxl, L);
-        __syncwarp();
-    }
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) maxl = max(maxl, __shfl_xor_sync(full, maxl, off));
-
-    // ---- positions: contacts grouped by level, index order within a level;
-    // passes: runs of at most 32 positions of one level (start | count << 26),
-    // the unit the lanes solve together.  A pass holds at least one contact,
-    // so the passes fit in [c0 + bundle, c1 + bundle] of s_lvl_start.
     uint32_t* gpass = s.s_lvl_start + c0 + bundle;
-    uint32_t pos = 0, npass = 0;
-    for (uint32_t l = 0; l < maxl; ++l) {
-        const uint32_t beg = pos;
-        for (uint32_t cb = c0; cb < c1; cb += 32) {
-            const uint32_t c = cb + lane;
-            const bool hit = c < c1 && s.s_level[c] == l;
-            const unsigned m = __ballot_sync(full, hit);
-            if (hit) s.s_order[c0 + pos + __popc(m & ((1u << lane) - 1u))] = c;
-            pos += __popc(m);
+    uint32_t maxl = 0, pos = 0, npass = 0;
+    if (mode != 2 && ncb <= 32 * kRegChunks) {
+        // ---- register path: each lane keeps its contacts (c0 + lane + 32 k)
+        // with their bodies, levels and positions in registers
+        const uint32_t K = (ncb + 31) / 32;
+        uint32_t ab[kRegChunks], lv[kRegChunks], pk[kRegChunks];
+#pragma unroll
+        for (uint32_t j = 0; j < kRegChunks; ++j) {
+            const uint32_t c = c0 + 32 * j + lane;
+            ab[j] = 0xFFFFFFFFu;
+            if (j < K && c < c1)
+                ab[j] = (w.geom_body[w.c_a[c]] - b0) | ((w.geom_body[w.c_b[c]] - b0) << 16);
         }
-        for (uint32_t q = beg + lane * 32; q < pos; q += 32 * 32)
-            gpass[npass + (q - beg) / 32] = q | (min(32u, pos - q) << kPassShift);
-        npass += (pos - beg + 31) / 32;
+#pragma unroll
+        for (uint32_t j = 0; j < kRegChunks; ++j) {
+            lv[j] = kNone;
+            if (j >= K) continue;  // warp-uniform
+            const bool valid = ab[j] != 0xFFFFFFFFu;
+            const uint32_t la = ab[j] & 0xFFFFu, lb = ab[j] >> 16;
+            // both inverse masses zero -> skipped (physics.comp:531)
+            const bool use = valid && !(B.invm[la] == 0.0f && B.invm[lb] == 0.0f);
+            uint32_t L = use ? 1u : 0u;
+            if (mode != 0) {
+                const bool da = use && !is_fixed(B, la), db = use && !is_fixed(B, lb);
+                const uint32_t xa = da ? la : (0x80000000u | (lane * 2u));
+                const uint32_t xb = db ? lb : (0x80000000u | (lane * 2u + 1u));
+                if (use) L = max(da ? last[la] : 0u, db ? last[lb] : 0u) + 1u;
+                for (uint32_t i = 0; i < 32; ++i) {
+                    const uint32_t ai = __shfl_sync(full, xa, i), bi = __shfl_sync(full, xb, i);
+                    const uint32_t Li = __shfl_sync(full, L, i);
+                    if (use && i < lane && (ai == xa || ai == xb || bi == xa || bi == xb))
+                        L = max(L, Li + 1u);
+                }
+                if (da) atomicMax(&last[la], L);
+                if (db) atomicMax(&last[lb], L);
+                __syncwarp();
+            }
+            if (use) lv[j] = L - 1u;
+            maxl = max(maxl, L);
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) maxl = max(maxl, __shfl_xor_sync(full, maxl, off));
+        const unsigned below = (1u << lane) - 1u;
+        for (uint32_t l = 0; l < maxl; ++l) {
+            const uint32_t beg = pos;
+#pragma unroll
+            for (uint32_t j = 0; j < kRegChunks; ++j) {
+                const bool hit = lv[j] == l;
+                const unsigned m = __ballot_sync(full, hit);
+                if (hit) pk[j] = pos + __popc(m & below);
+                pos += __popc(m);
+            }
+            npass = write_passes(gpass, npass, beg, pos, lane);
+        }
+#pragma unroll
+        for (uint32_t j = 0; j < kRegChunks; ++j) {
+            if (lv[j] == kNone) continue;
+            const uint32_t c = c0 + 32 * j + lane;
+            s.s_order[c0 + pk[j]] = c;
+            write_rec(w, k, s, B, b0, c, ab[j] & 0xFFFFu, ab[j] >> 16, c0 + pk[j], dt);
+            lam[pk[j]] = 0.0f;
+        }
+    } else {
+        // ---- memory path (colouring, or more contacts than the registers hold)
+        // ---- bodies of each contact; both inverse masses zero -> skipped (531)
+        for (uint32_t c = c0 + lane; c < c1; c += 32) {
+            const uint32_t la = w.geom_body[w.c_a[c]] - b0, lb = w.geom_body[w.c_b[c]] - b0;
+            const bool skip = B.invm[la] == 0.0f && B.invm[lb] == 0.0f;
+            s.s_ab[size_t(c) * 2] = skip ? kNone : la;
+            s.s_ab[size_t(c) * 2 + 1] = lb;
+        }
+        __syncwarp();
+
+        // ---- levels: colours (COLORED), wavefront levels (WAVEFRONT) or one
+        // level in index order (SEQUENTIAL)
+        bool coloured = mode == 2;
+        if (coloured) {
+            // greedy colouring in contact order: the smallest colour not used by
+            // an earlier contact at either of its dynamic bodies (per-body colour
+            // masks in `last`); more than 32 colours at a body falls back to the
+            // wavefront levels
+            uint32_t ok = 1u, mx = 0u;
+            if (lane == 0) {
+                for (uint32_t c = c0; c < c1; ++c) {
+                    const uint32_t la = s.s_ab[size_t(c) * 2], lb = s.s_ab[size_t(c) * 2 + 1];
+                    if (la == kNone) {
+                        s.s_level[c] = kNone;
+                        continue;
+                    }
+                    const bool da = !is_fixed(B, la), db = !is_fixed(B, lb);
+                    const uint32_t used = (da ? last[la] : 0u) | (db ? last[lb] : 0u);
+                    if (used == 0xFFFFFFFFu) {
+                        ok = 0u;
+                        break;
+                    }
+                    const uint32_t col = uint32_t(__ffs(int(~used))) - 1u;
+                    if (da) last[la] |= 1u << col;
+                    if (db) last[lb] |= 1u << col;
+                    s.s_level[c] = col;
+                    mx = max(mx, col + 1u);
+                }
+            }
+            ok = __shfl_sync(full, ok, 0);
+            maxl = __shfl_sync(full, mx, 0);
+            if (!ok) {
+                coloured = false;
+                maxl = 0;
+                for (uint32_t i = lane; i < nbs; i += 32) last[i] = 0;
+            }
+            __syncwarp();
+        }
+        for (uint32_t cb = c0; !coloured && cb < c1; cb += 32) {
+            const uint32_t c = cb + lane;
+            const bool valid = c < c1;
+            const uint32_t la = valid ? s.s_ab[size_t(c) * 2] : kNone;
+            const uint32_t lb = valid ? s.s_ab[size_t(c) * 2 + 1] : 0u;
+            const bool use = valid && la != kNone;
+            uint32_t L = use ? 1u : 0u;
+            if (mode != 0) {
+                const bool da = use && !is_fixed(B, la), db = use && !is_fixed(B, lb);
+                // dynamic bodies, or a sentinel unique to this lane and role
+                const uint32_t xa = da ? la : (0x80000000u | (lane * 2u));
+                const uint32_t xb = db ? lb : (0x80000000u | (lane * 2u + 1u));
+                if (use) L = max(da ? last[la] : 0u, db ? last[lb] : 0u) + 1u;
+                for (uint32_t j = 0; j < 32; ++j) {
+                    const uint32_t aj = __shfl_sync(full, xa, j), bj = __shfl_sync(full, xb, j);
+                    const uint32_t Lj = __shfl_sync(full, L, j);
+                    if (use && j < lane && (aj == xa || aj == xb || bj == xa || bj == xb))
+                        L = max(L, Lj + 1u);
+                }
+                if (da) atomicMax(&last[la], L);
+                if (db) atomicMax(&last[lb], L);
+            }
+            if (valid) s.s_level[c] = use ? L - 1u : kNone;
+            maxl = max(maxl, L);
+            __syncwarp();
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) maxl = max(maxl, __shfl_xor_sync(full, maxl, off));
+
+        // ---- positions: contacts grouped by level, index order within a level;
+        // passes: runs of at most 32 positions of one level (start | count << 26),
+        // the unit the lanes solve together.  A pass holds at least one contact,
+        // so the passes fit in [c0 + bundle, c1 + bundle] of s_lvl_start.
+        for (uint32_t l = 0; l < maxl; ++l) {
+            const uint32_t beg = pos;
+            for (uint32_t cb = c0; cb < c1; cb += 32) {
+                const uint32_t c = cb + lane;
+                const bool hit = c < c1 && s.s_level[c] == l;
+                const unsigned m = __ballot_sync(full, hit);
+                if (hit) s.s_order[c0 + pos + __popc(m & ((1u << lane) - 1u))] = c;
+                pos += __popc(m);
+            }
+            npass = write_passes(gpass, npass, beg, pos, lane);
+        }
+        __syncwarp();
+        for (uint32_t i = lane; i < pos; i += 32) {
+            const uint32_t c = s.s_order[c0 + i];
+            write_rec(w, k, s, B, b0, c, s.s_ab[size_t(c) * 2], s.s_ab[size_t(c) * 2 + 1], c0 + i, dt);
+            lam[i] = 0.0f;
+        }
     }
     __syncwarp();
     const bool pass_sm = npass <= kWarpLevelCap;
     if (pass_sm)
         for (uint32_t j = lane; j < npass; j += 32) lvl_sm[j] = gpass[j];
-    const uint32_t* pass = pass_sm ? lvl_sm : gpass;
-
-    // ---- per-contact records in position order (physics.comp:504-521,
-    // 533-546): the constants, computed from the pre-solve velocities, and
-    // both bodies' data, so a sweep step issues one run of loads
-    for (uint32_t i = lane; i < pos; i += 32) {
-        const uint32_t c = s.s_order[c0 + i];
-        const uint32_t ga = w.c_a[c], gb = w.c_b[c];
-        const uint32_t la = s.s_ab[size_t(c) * 2], lb = s.s_ab[size_t(c) * 2 + 1];
-        const uint32_t a = b0 + la, b = b0 + lb;
-        const f3 n = ld3(w.c_normal, c), cp = ld3(w.c_pos, c);
-        const f3 ra = sub(cp, ld3(w.pos, a)), rb = sub(cp, ld3(w.pos, b));
-        const f3 va = add(ld3(B.v, la), cross(ld3(B.w, la), ra));
-        const f3 vb = add(ld3(B.v, lb), cross(ld3(B.w, lb), rb));
-        const float vn = dot(sub(vb, va), n);
-        const float e = gmax(w.restitution[ga], w.restitution[gb]);
-        const float bias = k.baumgarte * gmax(w.c_pen[c] - k.slop, 0.0f) / dt + e * gmax(-vn, 0.0f);
-        const float ima = B.invm[la], imb = B.invm[lb];
-        const float4 qa = make_float4(w.quat[size_t(a) * 4], w.quat[size_t(a) * 4 + 1],
-                                      w.quat[size_t(a) * 4 + 2], w.quat[size_t(a) * 4 + 3]);
-        const float4 qb = make_float4(w.quat[size_t(b) * 4], w.quat[size_t(b) * 4 + 1],
-                                      w.quat[size_t(b) * 4 + 2], w.quat[size_t(b) * 4 + 3]);
-        const m3 Ra = quat_to_mat(qa.x, qa.y, qa.z, qa.w), Rb = quat_to_mat(qb.x, qb.y, qb.z, qb.w);
-        const f3 Ia = ld3(B.invI, la), Ib = ld3(B.invI, lb);
-        const f3 ran = cross(ra, n), rbn = cross(rb, n);
-        const float kn = ima + imb + dot(ran, apply_inv_I(Ra, Ia, ran)) + dot(rbn, apply_inv_I(Rb, Ib, rbn));
-        float4* r = s.s_rec + size_t(c0 + i) * kRecWords;
-        r[0] = make_float4(n.x, n.y, n.z, ra.x);
-        r[1] = make_float4(ra.y, ra.z, rb.x, rb.y);
-        r[2] = make_float4(rb.z, bias, kn, sqrtf(w.friction[ga] * w.friction[gb]));
-        r[3] = qa;
-        r[4] = qb;
-        r[5] = make_float4(Ia.x, Ia.y, Ia.z, Ib.x);
-        r[6] = make_float4(Ib.y, Ib.z, ima, imb);
-        r[7] = make_float4(__uint_as_float(la), __uint_as_float(lb),
-                           __uint_as_float((is_fixed(B, la) ? 1u : 0u) | (is_fixed(B, lb) ? 2u : 0u)),
-                           0.0f);
-        lam[i] = 0.0f;
-    }
     __syncwarp();
+    const uint32_t* pass = pass_sm ? lvl_sm : gpass;
 
     // ---- Gauss-Seidel sweeps ----
     if (mode == 0) {

@@ -48,6 +48,18 @@ def test_pile_with_contacts_bit_exact(cuda):
     assert_bit_exact(got, ref)
 
 
+def test_large_scene_many_contacts_bit_exact(cuda):
+    """About 860 bodies in one scene (one warp, velocities in global memory) with
+    more contacts than the solver setup keeps in registers (256 per warp):
+    the memory path of the level assignment and ordering."""
+    d = Data.pile(seed=6, n_boxes=450, n_spheres=450, lo=(-8, 0, -8), hi=(8, 5, 8))
+    assert 512 < d.num_bodies <= 1024
+    ref = oracle(d, frames=60, pgs=10)
+    assert ref["num_contacts"] > 300
+    got = gpu_run(d, cuda, frames=60, pgs=10)
+    assert_bit_exact(got, ref)
+
+
 def test_config0_pile_bit_exact(cuda):
     """512 bodies (256 boxes + 256 16-segment spheres) + ground, 30 PGS
     iterations, 4 frames."""

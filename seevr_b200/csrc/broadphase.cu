@@ -16,10 +16,12 @@
 //
 // Scenes of at most kTileBodies bodies (k_broad_tile): each of a scene's
 // blocks (one per kTileRows rows) stages the scene's AABBs and static flags
-// in shared memory, so a column test reads shared memory only; the scene's
-// rows are dealt out to the warps of its blocks in turn (row work shrinks
-// with the row index, so consecutive rows go to different warps).  The write
-// pass loads a row's overlap words with one coalesced load and places the
+// in shared memory, so a column test reads shared memory only.  The count
+// pass deals groups of kRowGroup consecutive rows to the warps of the
+// scene's blocks in turn (row work shrinks with the row index); a warp reads
+// 32 columns and tests them against every row of its group.  Its overlap
+// words are column-aligned (word c of a row: scene columns 32c .. 32c+31).
+// The write pass loads a row's words with one coalesced load and places the
 // hits with a warp prefix sum over the words' population counts.  Larger
 // scenes use one warp per row reading the AABBs from global memory
 // (k_broad_n2).
@@ -81,6 +83,7 @@ __global__ void __launch_bounds__(256) k_broad_n2(World w, const uint32_t* __res
 }
 
 constexpr uint32_t kTileThreads = 256, kTileWarps = kTileThreads / 32;
+constexpr uint32_t kRowGroup = 4;  // rows a warp tests against one column read
 
 template <bool kWrite>
 __global__ void __launch_bounds__(kTileThreads)
@@ -115,71 +118,95 @@ __global__ void __launch_bounds__(kTileThreads)
             stat[t] = w.inv_mass[s0 + t] <= 0.0f ? 1.0f : 0.0f;
         __syncthreads();
     }
+    const uint32_t nwords = (n + 31) / 32;  // column words of the scene
+    if (!kWrite) {
+        // kRowGroup consecutive rows per warp step: a column's AABB is read
+        // once and tested against every row of the group
+        for (uint32_t g = slice * kTileWarps + wid; g * kRowGroup < n; g += slices * kTileWarps) {
+            const uint32_t r0 = g * kRowGroup;
+            f3 rmn[kRowGroup], rmx[kRowGroup];
+            bool rst[kRowGroup];
+            uint32_t cnt[kRowGroup];
+#pragma unroll
+            for (uint32_t q = 0; q < kRowGroup; ++q) {
+                const uint32_t r = min(r0 + q, n - 1);
+                rmn[q] = ld3(mn, r);
+                rmx[q] = ld3(mx, r);
+                rst[q] = stat[r] != 0.0f;
+                cnt[q] = 0;
+            }
+            for (uint32_t c = (r0 + 1) / 32; c < nwords; ++c) {
+                const uint32_t j = 32 * c + lane;
+                const uint32_t jj = j < n ? j : n - 1;
+                const f3 cmn = ld3(mn, jj), cmx = ld3(mx, jj);
+                const bool cst = stat[jj] != 0.0f;
+                unsigned mine = 0;
+#pragma unroll
+                for (uint32_t q = 0; q < kRowGroup; ++q) {
+                    const bool hit = j < n && j > r0 + q && !(rst[q] && cst) &&
+                                     overlap(rmn[q], rmx[q], cmn, cmx);
+                    const unsigned m = __ballot_sync(0xFFFFFFFFu, hit);
+                    cnt[q] += __popc(m);
+                    if (lane == q) mine = m;
+                }
+                if (mask && lane < kRowGroup && r0 + lane < n)
+                    mask[size_t(s0 + r0 + lane) * stride + c] = mine;
+            }
+            if (lane == 0)
+#pragma unroll
+                for (uint32_t q = 0; q < kRowGroup; ++q)
+                    if (r0 + q < n) row_count[s0 + r0 + q] = cnt[q];
+        }
+        return;
+    }
     const unsigned below = (1u << lane) - 1u;
     for (uint32_t r = slice * kTileWarps + wid; r < n; r += slices * kTileWarps) {
         const uint32_t i = s0 + r;
-        const uint32_t ncol = n - r - 1;  // columns j = i+1 .. s1-1
-        const uint32_t nch = (ncol + 31) / 32;
-        uint32_t* mrow = mask ? mask + size_t(i) * stride : nullptr;
-        if (!kWrite) {
-            const f3 mna = ld3(mn, r), mxa = ld3(mx, r);
-            const bool static_i = stat[r] != 0.0f;
-            uint32_t count = 0;
-            for (uint32_t ch = 0; ch < nch; ++ch) {
-                const uint32_t jl = r + 1 + 32 * ch + lane;  // scene-local column
-                const bool hit = jl < n && !(static_i && stat[jl] != 0.0f) &&
-                                 overlap(mna, mxa, ld3(mn, jl), ld3(mx, jl));
-                const unsigned m = __ballot_sync(0xFFFFFFFFu, hit);
-                if (mrow && lane == 0) mrow[ch] = m;
-                count += __popc(m);
-            }
-            if (lane == 0) row_count[i] = count;
-        } else {
-            const uint32_t total = row_count[i];
-            if (total == 0) continue;
-            const f3 mna = test ? ld3(mn, r) : mk(0.f, 0.f, 0.f);
-            const f3 mxa = test ? ld3(mx, r) : mna;
-            const bool static_i = test && stat[r] != 0.0f;
-            uint32_t slot0 = row_off[i];
-            for (uint32_t c0 = 0; c0 < nch; c0 += 32) {
-                // lane l holds word c0 + l
-                unsigned word = 0;
-                if (mrow) {
-                    if (c0 + lane < nch) word = mrow[c0 + lane];
-                } else {
-                    for (uint32_t q = 0; q < 32 && c0 + q < nch; ++q) {
-                        const uint32_t jl = r + 1 + 32 * (c0 + q) + lane;
-                        const bool hit = jl < n && !(static_i && stat[jl] != 0.0f) &&
-                                         overlap(mna, mxa, ld3(mn, jl), ld3(mx, jl));
-                        const unsigned m = __ballot_sync(0xFFFFFFFFu, hit);
-                        if (lane == q) word = m;
-                    }
+        const uint32_t total = row_count[i];
+        if (total == 0) continue;
+        const uint32_t* mrow = mask ? mask + size_t(i) * stride : nullptr;
+        const f3 mna = test ? ld3(mn, r) : mk(0.f, 0.f, 0.f);
+        const f3 mxa = test ? ld3(mx, r) : mna;
+        const bool static_i = test && stat[r] != 0.0f;
+        uint32_t slot0 = row_off[i];
+        for (uint32_t c0 = (r + 1) / 32; c0 < nwords; c0 += 32) {
+            // lane l holds column word c0 + l
+            unsigned word = 0;
+            if (mrow) {
+                if (c0 + lane < nwords) word = mrow[c0 + lane];
+            } else {
+                for (uint32_t q = 0; q < 32 && c0 + q < nwords; ++q) {
+                    const uint32_t j = 32 * (c0 + q) + lane;
+                    const bool hit = j < n && j > r && !(static_i && stat[j] != 0.0f) &&
+                                     overlap(mna, mxa, ld3(mn, j), ld3(mx, j));
+                    const unsigned m = __ballot_sync(0xFFFFFFFFu, hit);
+                    if (lane == q) word = m;
                 }
-                // exclusive prefix of the words' population counts
-                const uint32_t pc = __popc(word);
-                uint32_t incl = pc;
+            }
+            // exclusive prefix of the words' population counts
+            const uint32_t pc = __popc(word);
+            uint32_t incl = pc;
 #pragma unroll
-                for (int off = 1; off < 32; off <<= 1) {
-                    const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, off);
-                    if (int(lane) >= off) incl += v;
-                }
-                const uint32_t excl = incl - pc;
-                unsigned nz = __ballot_sync(0xFFFFFFFFu, word != 0u);
-                while (nz) {
-                    const uint32_t q = uint32_t(__ffs(int(nz))) - 1u;
-                    nz &= nz - 1u;
-                    const unsigned m = __shfl_sync(0xFFFFFFFFu, word, q);
-                    const uint32_t pre = __shfl_sync(0xFFFFFFFFu, excl, q);
-                    if ((m >> lane) & 1u) {
-                        const uint32_t slot = slot0 + pre + __popc(m & below);
-                        if (slot < w.max_pairs) {
-                            w.pairs[size_t(slot) * 2] = i;
-                            w.pairs[size_t(slot) * 2 + 1] = i + 1 + 32 * (c0 + q) + lane;
-                        }
+            for (int off = 1; off < 32; off <<= 1) {
+                const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, off);
+                if (int(lane) >= off) incl += v;
+            }
+            const uint32_t excl = incl - pc;
+            unsigned nz = __ballot_sync(0xFFFFFFFFu, word != 0u);
+            while (nz) {
+                const uint32_t q = uint32_t(__ffs(int(nz))) - 1u;
+                nz &= nz - 1u;
+                const unsigned m = __shfl_sync(0xFFFFFFFFu, word, q);
+                const uint32_t pre = __shfl_sync(0xFFFFFFFFu, excl, q);
+                if ((m >> lane) & 1u) {
+                    const uint32_t slot = slot0 + pre + __popc(m & below);
+                    if (slot < w.max_pairs) {
+                        w.pairs[size_t(slot) * 2] = i;
+                        w.pairs[size_t(slot) * 2 + 1] = s0 + 32 * (c0 + q) + lane;
                     }
                 }
-                slot0 += __shfl_sync(0xFFFFFFFFu, incl, 31);
             }
+            slot0 += __shfl_sync(0xFFFFFFFFu, incl, 31);
         }
     }
 }

@@ -330,10 +330,12 @@ seevr_status check_step_args(seevr_physics* h, uint32_t nb, uint32_t nv, uint32_
 }
 
 // Overlap-word rows of the all-pairs broadphase for nb bodies in scenes of
-// at most maxs bodies: one 32-bit word per 32 columns of the longest row.
+// at most maxs bodies: one 32-bit word per 32 columns of the largest scene.
 // Layouts needing more than 1 GiB go without (the write pass re-tests).
 seevr_status ensure_bp_mask(seevr_physics* h, uint32_t nb, uint32_t maxs) {
-    const uint32_t stride = maxs > 1 ? (maxs - 1 + 31) / 32 : 1u;
+    // (maxs + 31) / 32 words: column-aligned words of the shared-memory
+    // kernel; the global-memory kernel's row-relative words need no more
+    const uint32_t stride = maxs > 0 ? (maxs + 31) / 32 : 1u;
     const size_t words = size_t(nb ? nb : 1) * stride;
     if (words * sizeof(uint32_t) > (size_t(1) << 30)) {
         if (h->s.bp_mask) cudaFree(h->s.bp_mask);

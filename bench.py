@@ -323,7 +323,8 @@ def ours(a, rank, world, local_rank):
 
     # ---- roofline of the dominant stage kernel
     peak, peak_kind = measured_peaks()
-    roof = roofline(stage_ms, nb, nhv, nv, pairs, contacts, a.substeps, peak, peak_kind)
+    roof = roofline(stage_ms, nb, nhv, nv, pairs, contacts, a.substeps, peak, peak_kind,
+                    NCU_TRAFFIC_DEFAULT if default_workload(a) else None)
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -536,7 +537,25 @@ def plain_dropin(a, d, pre_state, dev):
             "batched_vs_plain_max_rel_state_err": err}
 
 
-def roofline(stage_ms, nb, nhv, nv, pairs, contacts, substeps, peak, peak_kind):
+# DRAM bytes (read + write) per substep launch of each stage's main kernel,
+# from one ncu capture of the default workload (4,096 scenes, bodies 8-512,
+# 16-segment spheres, 10 substeps x 30 PGS iterations, 20 substeps after the
+# 90-frame pre-roll: profiles/launches_batched4096.md).  Reported as
+# roofline.traffic only when the bench runs that workload.
+NCU_TRAFFIC_DEFAULT = {
+    "phys/pgs_solve": ("k_solver_warp", 43545792),
+    "phys/narrow_phase": ("k_narrow", 427834701),
+    "phys/aabb": ("k_body_stage", 1021787686),
+    "phys/broad_phase": ("k_broad_tile (count + write)", 37183770 + 23357722),
+}
+
+
+def default_workload(a):
+    return (a.scenes, a.min_bodies, a.max_bodies, a.segments, a.substeps, a.pgs, a.preroll) == \
+        (4096, 8, 512, 16, 10, 30, 90)
+
+
+def roofline(stage_ms, nb, nhv, nv, pairs, contacts, substeps, peak, peak_kind, traffic_table=None):
     """Algorithmic bytes per launch of each stage kernel (last-substep pair and
     contact counts) over its measured time; the dominant stage is reported."""
     per_substep = {
@@ -551,8 +570,11 @@ def roofline(stage_ms, nb, nhv, nv, pairs, contacts, substeps, peak, peak_kind):
     t_launch = stage_ms[best] / (substeps if best in per_substep else 1)
     algo = per_substep.get(best, once.get(best, 0))
     achieved = algo / (t_launch / 1e3) / 1e9 if t_launch > 0 else 0.0
+    measured = (traffic_table or {}).get(best)
     return {"bound": "hbm", "kernel": best, "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+            "frac": achieved / peak, "peak_source": peak_kind,
+            "traffic": measured[1] if measured else None,
+            "traffic_kernel": measured[0] if measured else None,
             "algorithmic_bytes_per_launch": algo, "launch_ms": t_launch,
             "note": "stage share of the frame: " + ", ".join(
                 f"{k.split('/')[1]} {v / max(sum(stage_ms.values()), 1e-9):.0%}"

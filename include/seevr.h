@@ -255,8 +255,8 @@ void seevr_physics_destroy(seevr_physics* h);
  *  - Ordered on `stream` (a cudaStream_t, NULL = default stream) on the
  *    current device; synchronous unless params->flags has NO_SYNC.
  *  - The first call on a device looks up the scratch array's device address
- *    (cudaGetSymbolAddress) and configures the solver kernel; make that
- *    first call before any stream capture.
+ *    (cudaGetSymbolAddress) and configures the solver and broadphase
+ *    kernels; make that first call before any stream capture.
  *  - Every call shares the one array: calls whose GPU work may overlap
  *    (other streams or host threads on the same device) race and must be
  *    serialised by the caller.  Each call clears what must start at zero. */

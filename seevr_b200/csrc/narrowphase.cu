@@ -151,13 +151,14 @@ __device__ __forceinline__ void finish(float4* res0, float4* res1, uint32_t* fla
 }
 
 constexpr uint32_t kNarrowThreads = 128;
+constexpr uint32_t kNarrowBlocksPerSm = 7;  // resident blocks per SM of the persistent grid (measured best of 4-8)
 
 // kTape: also record, per pair, which hull vertices support the final
 // portal (tape[2p] = {case, m1.ia, m1.ib, m2.ia}, tape[2p+1] = {m2.ib,
 // m3.ia, m3.ib, 0}; case 1 = penetration portal, 2 = the segment case of
 // physics.comp:267-271), from which the adjoint differentiates the contact.
 template <bool kTape>
-__global__ void __launch_bounds__(kNarrowThreads)
+__global__ void __launch_bounds__(kNarrowThreads, kNarrowBlocksPerSm)
     k_narrow(World w, Consts k, float4* __restrict__ res0, float4* __restrict__ res1,
              uint32_t* __restrict__ flag, uint32_t* __restrict__ ticket,
              uint4* __restrict__ tape) {
@@ -380,7 +381,7 @@ int launch_narrowphase_taped(const World& w, const Consts& k, const Scratch& s, 
     // persistent grid: a few resident blocks per SM; the pair ticket lives
     // in status[1] and is cleared here
     cudaMemsetAsync(&s.status[1], 0, sizeof(uint32_t), st);
-    const uint32_t blocks = grid_for(w.max_pairs, kNarrowThreads, 148 * 4);
+    const uint32_t blocks = grid_for(w.max_pairs, kNarrowThreads, 148 * kNarrowBlocksPerSm);
     if (pair_tape)
         k_narrow<true><<<blocks, kNarrowThreads, 0, st>>>(w, k, s.pair_res0, s.pair_res1,
                                                           s.pair_flag, &s.status[1], pair_tape);

@@ -60,6 +60,19 @@ def test_large_scene_many_contacts_bit_exact(cuda):
     assert_bit_exact(got, ref)
 
 
+def test_scene_above_tile_limit_bit_exact(cuda):
+    """2,601 bodies in one scene: above the 2,048 bodies the
+    shared-memory broadphase stages, so pairs come from the global-memory
+    all-pairs kernel, and above 1,024 bodies, so contacts are solved per
+    island."""
+    d = Data.pile(seed=11, n_boxes=1300, n_spheres=1300, lo=(-16, 0, -16), hi=(18, 3, 18))
+    assert d.num_bodies > 2048
+    ref = oracle(d, frames=30, pgs=4)
+    assert ref["num_pairs"] > 1000 and ref["num_contacts"] > 300
+    got = gpu_run(d, cuda, frames=30, pgs=4)
+    assert_bit_exact(got, ref)
+
+
 def test_config0_pile_bit_exact(cuda):
     """512 bodies (256 boxes + 256 16-segment spheres) + ground, 30 PGS
     iterations, 4 frames."""

@@ -117,7 +117,7 @@ enum seevr_solver {
                                     run in parallel waves: bit-identical to
                                     SEQUENTIAL                               */
     SEEVR_SOLVER_COLORED = 2     /* graph-coloured Gauss-Seidel: a different
-                                    contact order, judged by drift          */
+                                    contact order, assessed by drift        */
 };
 
 enum seevr_flags {

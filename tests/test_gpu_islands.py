@@ -1,7 +1,7 @@
 """Island-parallel PGS (scenes above 1,024 bodies) and the coloured solver.
 
 WAVEFRONT on islands must stay bit-identical to the sequential sweep (the
-FP32 oracle).  COLORED visits contacts in a different order, so it is judged
+FP32 oracle).  COLORED visits contacts in a different order, so it is assessed
 by what it is for: stacks stay up (tower-top drift), and its state stays
 close to the sequential one.
 """

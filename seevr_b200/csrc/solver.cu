@@ -308,9 +308,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
 
     uint32_t* gpass = s.s_lvl_start + c0 + bundle;
     uint32_t maxl = 0, pos = 0, npass = 0;
-    if (mode != 2 && ncb <= 32 * kRegChunks) {
+    if (mode != 2 && ncb <= 32 * kRegChunks && nbs <= 0x10000u) {
         // ---- register path: each lane keeps its contacts (c0 + lane + 32 k)
-        // with their bodies, levels and positions in registers
+        // with their bodies (two 16-bit bundle-local indices, hence at most
+        // 65,536 bodies per bundle), levels and positions in registers
         const uint32_t K = (ncb + 31) / 32;
         uint32_t ab[kRegChunks], lv[kRegChunks], pk[kRegChunks];
 #pragma unroll

@@ -10,7 +10,7 @@ import pytest
 
 import pyoracle
 from helpers import DT, G, assert_bit_exact, gpu_run, max_rel_err
-from seevr_b200 import Caps, Data, SeevrError, SOLVER_SEQUENTIAL, SOLVER_WAVEFRONT
+from seevr_b200 import Caps, Data, SeevrError, SOLVER_SEQUENTIAL, SOLVER_WAVEFRONT, make_params
 
 pytestmark = pytest.mark.gpu
 
@@ -96,6 +96,23 @@ def test_batch_bit_exact_against_oracle(cuda):
     ref = oracle(d, frames=3, pgs=6, threads=8)
     got = gpu_run(d, cuda, frames=3, pgs=6)
     assert_bit_exact(got, ref)
+
+
+@pytest.mark.parametrize("frames", [2, 20])
+def test_bundle_size_does_not_change_results(cuda, frames):
+    """bundle_bodies only changes how scenes are grouped per solver warp:
+    one bundle of every scene (about 68,000 bodies, more than 16-bit
+    bundle-local indices hold; velocities in global memory), the default
+    512 and 64 (one scene per bundle) give the same state bit for bit."""
+    d = Data.batch(num_scenes=300, min_bodies=200, max_bodies=256, seed_base=21)
+    assert d.num_bodies > 65536
+    caps = Caps.for_data(d, pairs_per_body=8.0, contacts_per_body=4.0)
+    runs = [gpu_run(d, cuda, frames=frames, pgs=10, caps=caps, update_verts=False,
+                    params=make_params(pgs_iterations=10, flags=4, bundle_bodies=bb))
+            for bb in (1 << 20, 0, 64)]
+    for r in runs[1:]:
+        for k in ("pos", "quat", "vel", "omega", "lambda"):
+            assert np.array_equal(r[k], runs[0][k]), k
 
 
 def test_scene_in_batch_equals_scene_alone(cuda):

@@ -288,6 +288,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
     const uint32_t c0 = s.bundle_c0[bundle], c1 = s.bundle_c0[bundle + 1];
     if (c0 >= c1) return;
     const uint32_t nbs = b1 - b0, ncb = c1 - c0;
+    // pass entries hold a position in kPassShift bits: a bundle with more
+    // contacts runs the sequential sweep, which has no pass table and gives
+    // the same result bit for bit
+    if (ncb > kPassMask) mode = 0;
 
     float* base = sm + size_t(wid) * warp_smem_words(nbmax);
     const bool in_smem = nbs <= nbmax;

@@ -1,14 +1,15 @@
-// body.cu — per-body stages of physics.comp fused into one kernel:
-// integrate (step 6, physics.comp:586-604) of the previous substep, gravity +
-// damping (step 0, 418-428), the world AABB of the body's hull (steps 9-11,
-// 686-844) and the render-vertex update (step 7, 607-627).
+// body.cu — per-body stages of physics.comp: one kernel fuses integrate
+// (step 6, physics.comp:586-604) of the previous substep, gravity + damping
+// (step 0, 418-428) and the world AABB of the body's hull (steps 9-11,
+// 686-844); the render-vertex update (step 7, 607-627) runs at frame end in
+// its own kernel after the state update.
 //
 // The stage streams every hull vertex once per substep (12 bytes each, the
 // bulk of its HBM traffic).  A block takes 256 consecutive bodies: each
 // thread updates its body's state with coalesced loads and handles a small
-// hull itself; bodies whose hull or render mesh has more than 32 vertices go
-// to a per-block queue that the block's warps then drain, lanes striding
-// over the vertices, so no warp waits on a single lane's state update.
+// hull itself; bodies whose hull has more than 32 vertices go to a
+// per-block queue that the block's warps then drain, lanes striding over
+// the vertices, so no warp waits on a single lane's state update.
 //
 // The reference reduces AABBs with a thread-0 serial loop per 256-vertex
 // workgroup and a multi-launch cascade; min/max are exact in any order, so
@@ -37,8 +38,8 @@ int launch_hull_range_from_geom_data(const float* geom_data, uint32_t* out, uint
 }
 
 constexpr uint32_t kBodyThreads = 256;
-// Hulls (and render meshes) up to this many vertices are transformed by the
-// body's own thread; larger ones by a warp in the block's second phase.
+// Hulls up to this many vertices are transformed by the body's own thread;
+// larger ones by a warp in the block's second phase.
 constexpr uint32_t kSmallVerts = 32;
 // Vertices per lane per round of loads in the warp phase.
 constexpr uint32_t kLaneVerts = 10;
@@ -102,11 +103,10 @@ __device__ __forceinline__ void body_state(const World& w, const Consts& k, uint
     q[3] = qw;
 }
 
-// Phase 1, one thread per body: state update, then the AABB and render
-// vertices of small meshes in vertex order.  Bodies with a large hull or
-// render mesh are queued in shared memory with their pose; phase 2 gives
-// each a warp whose lanes stride over the vertices and reduce with shuffles
-// (min/max are exact in any order).
+// Phase 1, one thread per body: state update, then the AABB of a small hull
+// in vertex order.  Bodies with a large hull are queued in shared memory
+// with their pose; phase 2 gives each a warp whose lanes stride over the
+// vertices and reduce with shuffles (min/max are exact in any order).
 __global__ void __launch_bounds__(kBodyThreads) k_body_stage(World w, Consts k, uint32_t flags,
                                                              float dt, float gx, float gy,
                                                              float gz) {
@@ -119,22 +119,17 @@ __global__ void __launch_bounds__(kBodyThreads) k_body_stage(World w, Consts k, 
     const uint32_t b = blockIdx.x * kBodyThreads + threadIdx.x;
     const float inf = __int_as_float(0x7f800000);
     if (b < w.nb) {
-        uint32_t hs = 0, hc = 0, vs = 0, ve = 0;
+        uint32_t hs = 0, hc = 0;
         if (flags & kAabb) {
             hs = w.hull_range[size_t(b) * 2];
             hc = w.hull_range[size_t(b) * 2 + 1];
         }
-        if (flags & kRenderVerts) {
-            vs = w.vert_start[b];
-            ve = vs + w.vert_count[b];
-            if (ve > w.nv) ve = w.nv;
-            if (ve < vs) ve = vs;
-        }
+
         f3 p;
         float q[4];
         body_state(w, k, flags, b, dt, gx, gy, gz, p, q);
         const m3 R = quat_to_mat(q[0], q[1], q[2], q[3]);
-        const bool big = hc > kSmallVerts || ve - vs > kSmallVerts;
+        const bool big = hc > kSmallVerts;
         if ((flags & kAabb) && hc <= kSmallVerts) {
             f3 mn = mk(inf, inf, inf), mx = mk(-inf, -inf, -inf);
 #pragma unroll 8
@@ -148,10 +143,7 @@ __global__ void __launch_bounds__(kBodyThreads) k_body_stage(World w, Consts k, 
                 st3(w.aabb_max, b, mx);
             }
         }
-        if ((flags & kRenderVerts) && ve - vs <= kSmallVerts) {
-#pragma unroll 4
-            for (uint32_t i = vs; i < ve; ++i) st3(w.verts, i, add(p, mul(R, ld3(w.orig, i))));
-        }
+
         if (big) {
             const uint32_t e = atomicAdd(&sh_n, 1u);
             sh_body[e] = b;
@@ -214,14 +206,38 @@ __global__ void __launch_bounds__(kBodyThreads) k_body_stage(World w, Consts k, 
                 }
             }
         }
-        if (flags & kRenderVerts) {
-            const uint32_t vs = w.vert_start[bb];
-            uint32_t ve = vs + w.vert_count[bb];
-            if (ve > w.nv) ve = w.nv;
-            if (ve > vs && ve - vs > kSmallVerts) {
-#pragma unroll 4
-                for (uint32_t i = vs + lane; i < ve; i += 32)
-                    st3(w.verts, i, add(p, mul(R, ld3(w.orig, i))));
+    }
+}
+
+// Render vertices (step 7, physics.comp:607-627) from the final pose: a warp
+// per body, lanes striding over its vertices, kRenderBatch loads in flight
+// per lane before the stores (the source and destination buffers may
+// alias, so the compiler cannot move a load above an earlier store).  The
+// same arithmetic as the per-body stage: R = quat_to_mat(q), v' = p + R v.
+constexpr uint32_t kRenderBatch = 8;
+constexpr uint32_t kRenderThreads = 256;
+
+__global__ void __launch_bounds__(kRenderThreads) k_render_verts(World w) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t nwarps = gridDim.x * (kRenderThreads / 32);
+    for (uint32_t b = (blockIdx.x * kRenderThreads + threadIdx.x) >> 5; b < w.nb; b += nwarps) {
+        const uint32_t vs = w.vert_start[b];
+        uint32_t ve = vs + w.vert_count[b];
+        if (ve > w.nv) ve = w.nv;
+        if (ve <= vs) continue;
+        const f3 p = ld3(w.pos, b);
+        const m3 R = quat_to_mat(w.quat, b);
+        for (uint32_t c0 = vs; c0 < ve; c0 += 32u * kRenderBatch) {
+            f3 v[kRenderBatch];
+#pragma unroll
+            for (uint32_t j = 0; j < kRenderBatch; ++j) {
+                const uint32_t i = c0 + lane + 32u * j;
+                if (i < ve) v[j] = ld3(w.orig, i);
+            }
+#pragma unroll
+            for (uint32_t j = 0; j < kRenderBatch; ++j) {
+                const uint32_t i = c0 + lane + 32u * j;
+                if (i < ve) st3(w.verts, i, add(p, mul(R, v[j])));
             }
         }
     }
@@ -231,8 +247,14 @@ int launch_body_stage(const World& w, const Consts& k, uint32_t flags, float dt,
                       float gy, float gz, cudaStream_t st) {
     if (w.nb == 0) return 0;
     const uint32_t blocks = (w.nb + kBodyThreads - 1) / kBodyThreads;
-    k_body_stage<<<blocks, kBodyThreads, 0, st>>>(w, k, flags, dt, gx, gy, gz);
-    return 1;
+    // render vertices in their own kernel, after the state update: the
+    // per-body stage keeps its register budget (and occupancy) for the
+    // substep launches
+    k_body_stage<<<blocks, kBodyThreads, 0, st>>>(w, k, flags & ~kRenderVerts, dt, gx, gy, gz);
+    if (!(flags & kRenderVerts)) return 1;
+    const uint32_t rblocks = (w.nb + kRenderThreads / 32 - 1) / (kRenderThreads / 32);
+    k_render_verts<<<rblocks < 148u * 64u ? rblocks : 148u * 64u, kRenderThreads, 0, st>>>(w);
+    return 2;
 }
 
 }  // namespace seevr

@@ -544,8 +544,8 @@ def plain_dropin(a, d, pre_state, dev):
 # roofline.traffic only when the bench runs that workload.
 NCU_TRAFFIC_DEFAULT = {
     "phys/pgs_solve": ("k_solver_warp", 43545792),
-    "phys/narrow_phase": ("k_narrow", 427834701),
-    "phys/aabb": ("k_body_stage", 1021787686),
+    "phys/narrow_phase": ("k_narrow", 805700000),
+    "phys/aabb": ("k_body_stage", 1023200000),
     "phys/broad_phase": ("k_broad_tile (count + write)", 37183770 + 23357722),
 }
 

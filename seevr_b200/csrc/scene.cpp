@@ -858,7 +858,7 @@ int seevr_scene_save(const seevr_scene* s, const char* path) {
     FILE* f = std::fopen(path, "wb");
     if (!f) return 1;
     std::fwrite("SEEVRSC1", 1, 8, f);
-    const uint32_t count = 28;
+    const uint32_t count = 35;
     std::fwrite(&count, 4, 1, f);
     put_vec(f, 0, s->body_pos);
     put_vec(f, 1, s->body_quat);
@@ -889,6 +889,13 @@ int seevr_scene_save(const seevr_scene* s, const char* path) {
     const std::vector<uint32_t> nse{s->num_support_entries};
     put_vec(f, 26, nse);
     put_vec(f, 27, s->hull_range);
+    put_vec(f, 28, s->geom_tri_start);
+    put_vec(f, 29, s->geom_tri_count);
+    put_vec(f, 30, s->mat_albedo);
+    put_vec(f, 31, s->mat_roughness);
+    put_vec(f, 32, s->mat_metallic);
+    put_vec(f, 33, s->mat_emission);
+    put_vec(f, 34, s->mat_ior);
     const int bad = std::ferror(f);
     std::fclose(f);
     return bad ? 1 : 0;
@@ -937,6 +944,13 @@ seevr_scene* seevr_scene_load(const char* path) {
             case 25: ok = get_vec(f, n, s->geom_vert_count); break;
             case 26: ok = get_vec(f, n, nse); break;
             case 27: ok = get_vec(f, n, s->hull_range); break;
+            case 28: ok = get_vec(f, n, s->geom_tri_start); break;
+            case 29: ok = get_vec(f, n, s->geom_tri_count); break;
+            case 30: ok = get_vec(f, n, s->mat_albedo); break;
+            case 31: ok = get_vec(f, n, s->mat_roughness); break;
+            case 32: ok = get_vec(f, n, s->mat_metallic); break;
+            case 33: ok = get_vec(f, n, s->mat_emission); break;
+            case 34: ok = get_vec(f, n, s->mat_ior); break;
             default: ok = std::fseek(f, long(n), SEEK_CUR) == 0; break;
         }
     }
@@ -949,8 +963,12 @@ seevr_scene* seevr_scene_load(const char* path) {
         return nullptr;
     }
     if (!nse.empty()) s->num_support_entries = nse[0];
-    s->geom_tri_start.assign(s->geom_body_idx.size(), 0);
-    s->geom_tri_count.assign(s->geom_body_idx.size(), 0);
+    // files written before records 28-34 existed carry no triangle ranges
+    if (s->geom_tri_start.size() != s->geom_body_idx.size() ||
+        s->geom_tri_count.size() != s->geom_body_idx.size()) {
+        s->geom_tri_start.assign(s->geom_body_idx.size(), 0);
+        s->geom_tri_count.assign(s->geom_body_idx.size(), 0);
+    }
     return s;
 }
 

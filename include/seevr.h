@@ -223,6 +223,29 @@ seevr_status seevr_physics_read_counters(seevr_physics* h, uint32_t out[2]);
  * global-memory path).  Cleared by the call. */
 seevr_status seevr_physics_read_flags(seevr_physics* h, uint32_t* flags);
 
+/* Launch shapes of the batched step (no counterpart in the reference, whose
+ * work-group sizes are fixed in the shader).  None of them changes any
+ * result, only speed; seevr_b200.tune.autotune times candidates on the
+ * caller's workload and sets the fastest.
+ *  - bundle_bodies: solver bundle size (as seevr_params.bundle_bodies;
+ *    0 = 512), at most 2^24;
+ *  - narrow_blocks_per_sm: blocks per SM of the persistent narrowphase grid,
+ *    1 to 7 (0 = 7, the register budget's maximum);
+ *  - broad_tile_rows: rows of a scene per all-pairs broadphase block, 8 to
+ *    2,048 (0 = 64).
+ * get returns the values in use (defaults resolved).  set applies them to
+ * the following steps: a handle with scenes set rebuilds its solver bundles
+ * and broadphase tiles (as seevr_physics_set_scenes does), and a captured
+ * frame graph is recaptured at the next graph step. */
+typedef struct seevr_tuning {
+    uint32_t bundle_bodies;
+    uint32_t narrow_blocks_per_sm;
+    uint32_t broad_tile_rows;
+    uint32_t reserved; /* 0 */
+} seevr_tuning;
+seevr_status seevr_physics_get_tuning(seevr_physics* h, seevr_tuning* out);
+seevr_status seevr_physics_set_tuning(seevr_physics* h, const seevr_tuning* t);
+
 /* Copy the mutable body state between host memory and the bound device
  * buffers (pos, quat, vel, omega of num_bodies bodies), ordered on the
  * handle's stream and synchronous.  Mirrors Data.upload (data.zig:599-611)

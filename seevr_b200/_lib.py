@@ -72,6 +72,12 @@ class Profile(C.Structure):
     _fields_ = [("ms", C.c_float * NUM_STAGES), ("calls", C.c_uint32)]
 
 
+class Tuning(C.Structure):
+    """seevr_tuning: launch shapes of the batched step (results unchanged)."""
+    _fields_ = [("bundle_bodies", C.c_uint32), ("narrow_blocks_per_sm", C.c_uint32),
+                ("broad_tile_rows", C.c_uint32), ("reserved", C.c_uint32)]
+
+
 class AdjointGrads(C.Structure):
     """seevr_adjoint_grads: device pointers of the gradient buffers."""
     _fields_ = [("pos", C.c_void_p), ("quat", C.c_void_p), ("vel", C.c_void_p),
@@ -113,6 +119,8 @@ def _load():
         "seevr_physics_step_async": (I, [P, U32, U32, U32, U32, F, FP, U32, P]),
         "seevr_physics_read_counters": (I, [P, UP]),
         "seevr_physics_read_flags": (I, [P, UP]),
+        "seevr_physics_get_tuning": (I, [P, C.POINTER(Tuning)]),
+        "seevr_physics_set_tuning": (I, [P, C.POINTER(Tuning)]),
         "seevr_physics_upload_state": (I, [P, U32, P, P, P, P]),
         "seevr_physics_download_state": (I, [P, U32, P, P, P, P]),
         "seevr_physics_destroy": (None, [P]),

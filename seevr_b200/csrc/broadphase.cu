@@ -15,8 +15,9 @@
 // reads the words back instead of re-testing.
 //
 // Scenes of at most kTileBodies bodies (k_broad_tile): each of a scene's
-// blocks (one per kTileRows rows) stages the scene's AABBs and static flags
-// in shared memory, so a column test reads shared memory only.  The count
+// blocks (one per kTileRows rows, or the tuned row count) stages the
+// scene's AABBs and static flags in shared memory, so a column test reads
+// shared memory only.  The count
 // pass deals groups of kRowGroup consecutive rows to the warps of the
 // scene's blocks in turn (row work shrinks with the row index); a warp reads
 // 32 columns and tests them against every row of its group.  Its overlap
@@ -215,9 +216,10 @@ int launch_broadphase_n2(const World& w, const Scratch& s, uint32_t max_scene_bo
                          cudaStream_t st) {
     if (w.nb == 0) return 0;
     if (max_scene_bodies <= kTileBodies && w.ns > 0) {
-        // one block per kTileRows rows of each scene (the tile table), or
+        // one block per `rows` rows of each scene (the tile table), or
         // without a table the largest scene's block count for every scene
-        const uint32_t slices = max(1u, (max_scene_bodies + kTileRows - 1) / kTileRows);
+        const uint32_t rows = s.bp_tile_rows ? s.bp_tile_rows : kTileRows;
+        const uint32_t slices = max(1u, (max_scene_bodies + rows - 1) / rows);
         const uint2* tiles = s.bp_ntiles ? s.bp_tiles : nullptr;
         const uint32_t blocks = tiles ? s.bp_ntiles : w.ns * slices;
         const size_t smem = size_t(7) * max_scene_bodies * sizeof(float);

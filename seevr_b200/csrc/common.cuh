@@ -126,6 +126,9 @@ struct Scratch {
     // (NULL: every scene gets the slices of the largest)
     uint2* bp_tiles;
     uint32_t bp_ntiles;
+    // launch shapes (seevr_physics_set_tuning; 0 = the built-in default)
+    uint32_t narrow_blocks;  // persistent narrowphase grid, in blocks
+    uint32_t bp_tile_rows;   // all-pairs broadphase rows per block
     IslandScratch isl;
 };
 
@@ -155,6 +158,9 @@ cudaError_t init_broadphase();
 // bodies, one block per kTileRows rows of a scene
 constexpr uint32_t kTileBodies = 2048;
 constexpr uint32_t kTileRows = 64;
+// narrowphase: resident blocks per SM of the persistent grid (its register
+// cap; measured best of 4 to 8)
+constexpr uint32_t kNarrowBlocksPerSm = 7;
 int launch_narrowphase(const World& w, const Consts& k, const Scratch& s, cudaStream_t st);
 // Narrowphase that also tapes the supporting hull vertices of each contact's
 // final portal (2 uint4 per pair / contact) for the adjoint.

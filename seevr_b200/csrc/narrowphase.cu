@@ -151,7 +151,6 @@ __device__ __forceinline__ void finish(float4* res0, float4* res1, uint32_t* fla
 }
 
 constexpr uint32_t kNarrowThreads = 128;
-constexpr uint32_t kNarrowBlocksPerSm = 7;  // resident blocks per SM of the persistent grid (measured best of 4-8)
 
 // kTape: also record, per pair, which hull vertices support the final
 // portal (tape[2p] = {case, m1.ia, m1.ib, m2.ia}, tape[2p+1] = {m2.ib,
@@ -381,7 +380,8 @@ int launch_narrowphase_taped(const World& w, const Consts& k, const Scratch& s, 
     // persistent grid: a few resident blocks per SM; the pair ticket lives
     // in status[1] and is cleared here
     cudaMemsetAsync(&s.status[1], 0, sizeof(uint32_t), st);
-    const uint32_t blocks = grid_for(w.max_pairs, kNarrowThreads, 148 * kNarrowBlocksPerSm);
+    const uint32_t blocks = grid_for(w.max_pairs, kNarrowThreads,
+                                     s.narrow_blocks ? s.narrow_blocks : 148 * kNarrowBlocksPerSm);
     if (pair_tape)
         k_narrow<true><<<blocks, kNarrowThreads, 0, st>>>(w, k, s.pair_res0, s.pair_res1,
                                                           s.pair_flag, &s.status[1], pair_tape);

@@ -113,6 +113,11 @@ struct seevr_physics {
     size_t bp_mask_cap = 0;
     // broadphase tile table (s.bp_tiles) capacity, in tiles
     uint32_t bp_tiles_cap = 0;
+    // streaming multiprocessors of the device (launch shapes are per SM)
+    int sm_count = 148;
+    uint32_t narrow_blocks_per_sm = kNarrowBlocksPerSm;
+    // the caller's scene layout, kept to rebuild bundles and tiles on retuning
+    std::vector<uint32_t> scene_offsets_host;
 };
 
 namespace {
@@ -370,7 +375,8 @@ seevr_status set_bp_tiles(seevr_physics* h, const uint32_t* body_offset, uint32_
     std::vector<uint2> tiles;
     for (uint32_t s = 0; s < num_scenes; ++s) {
         const uint32_t n = body_offset[s + 1] - body_offset[s];
-        const uint32_t k = std::max(1u, (n + kTileRows - 1) / kTileRows);
+        const uint32_t rows = h->s.bp_tile_rows ? h->s.bp_tile_rows : kTileRows;
+        const uint32_t k = std::max(1u, (n + rows - 1) / rows);
         for (uint32_t j = 0; j < k; ++j) tiles.push_back(make_uint2(s, j | (k << 16)));
     }
     if (tiles.size() > h->bp_tiles_cap) {
@@ -564,6 +570,14 @@ seevr_status seevr_physics_create(const seevr_bindings* b, const seevr_caps* cap
         st = fail(SEEVR_ERR_CUDA, "cudaMemset failed");
     if (st == SEEVR_OK && init_solver() != cudaSuccess)
         st = fail(SEEVR_ERR_CUDA, "cudaFuncSetAttribute for the solver failed");
+    if (st == SEEVR_OK) {
+        int sms = 0;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device) == cudaSuccess &&
+            sms > 0)
+            h->sm_count = sms;
+        h->s.narrow_blocks = uint32_t(h->sm_count) * h->narrow_blocks_per_sm;
+        h->s.bp_tile_rows = kTileRows;
+    }
     if (st == SEEVR_OK && init_broadphase() != cudaSuccess)
         st = fail(SEEVR_ERR_CUDA, "cudaFuncSetAttribute for the broadphase failed");
     if (st != SEEVR_OK) {
@@ -593,6 +607,7 @@ seevr_status seevr_physics_set_scenes(seevr_physics* h, const uint32_t* body_off
     const uint32_t nb = body_offset[num_scenes];
     if (nb > h->caps.max_bodies)
         return fail(SEEVR_ERR_INVALID_ARGUMENT, "scenes hold more bodies than caps.max_bodies");
+    h->scene_offsets_host.assign(body_offset, body_offset + num_scenes + 1);
     std::vector<uint32_t> bs(nb ? nb : 1, 0);
     for (uint32_t s = 0; s < num_scenes; ++s)
         for (uint32_t i = body_offset[s]; i < body_offset[s + 1]; ++i) bs[i] = s;
@@ -712,6 +727,44 @@ seevr_status seevr_physics_read_flags(seevr_physics* h, uint32_t* flags) {
     *flags = h->host_flags;
     h->host_flags = 0;
     return st;
+}
+
+seevr_status seevr_physics_get_tuning(seevr_physics* h, seevr_tuning* out) {
+    if (!h || !out) return fail(SEEVR_ERR_INVALID_ARGUMENT, "handle or out is NULL");
+    out->bundle_bodies = h->params.bundle_bodies ? h->params.bundle_bodies : 512u;
+    out->narrow_blocks_per_sm = h->narrow_blocks_per_sm;
+    out->broad_tile_rows = h->s.bp_tile_rows ? h->s.bp_tile_rows : kTileRows;
+    out->reserved = 0;
+    return SEEVR_OK;
+}
+
+seevr_status seevr_physics_set_tuning(seevr_physics* h, const seevr_tuning* t) {
+    if (!h || !t) return fail(SEEVR_ERR_INVALID_ARGUMENT, "handle or tuning is NULL");
+    const uint32_t nbps = t->narrow_blocks_per_sm ? t->narrow_blocks_per_sm : kNarrowBlocksPerSm;
+    const uint32_t rows = t->broad_tile_rows ? t->broad_tile_rows : kTileRows;
+    if (nbps > kNarrowBlocksPerSm)
+        return fail(SEEVR_ERR_INVALID_ARGUMENT, "narrow_blocks_per_sm above " +
+                                                    std::to_string(kNarrowBlocksPerSm) +
+                                                    " (the blocks that fit on an SM)");
+    if (rows < 8 || rows > kTileBodies)
+        return fail(SEEVR_ERR_INVALID_ARGUMENT, "broad_tile_rows outside [8, " +
+                                                    std::to_string(kTileBodies) + "]");
+    if (t->bundle_bodies > (1u << 24))
+        return fail(SEEVR_ERR_INVALID_ARGUMENT, "bundle_bodies above 2^24");
+    SEEVR_CUDA(cudaSetDevice(h->device));
+    h->narrow_blocks_per_sm = nbps;
+    h->s.narrow_blocks = uint32_t(h->sm_count) * nbps;
+    h->s.bp_tile_rows = rows;
+    h->params.bundle_bodies = t->bundle_bodies;
+    if (h->graph_exec) {
+        cudaGraphExecDestroy(h->graph_exec);
+        h->graph_exec = nullptr;
+    }
+    if (h->scenes_set) {  // rebuild the bundles and the broadphase tiles
+        const std::vector<uint32_t> off = h->scene_offsets_host;
+        return seevr_physics_set_scenes(h, off.data(), uint32_t(off.size() - 1));
+    }
+    return SEEVR_OK;
 }
 
 seevr_status seevr_physics_upload_state(seevr_physics* h, uint32_t nb, const float* pos,

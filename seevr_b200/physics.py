@@ -84,6 +84,19 @@ class Physics:
         L.check(L.lib.seevr_physics_read_flags(self._h, C.byref(f)))
         return int(f.value)
 
+    def get_tuning(self) -> dict:
+        """The launch shapes in use (seevr_physics_get_tuning)."""
+        t = L.Tuning()
+        L.check(L.lib.seevr_physics_get_tuning(self._h, C.byref(t)))
+        return {"bundle_bodies": t.bundle_bodies, "narrow_blocks_per_sm": t.narrow_blocks_per_sm,
+                "broad_tile_rows": t.broad_tile_rows}
+
+    def set_tuning(self, bundle_bodies: int = 0, narrow_blocks_per_sm: int = 0,
+                   broad_tile_rows: int = 0) -> None:
+        """seevr_physics_set_tuning: results are unchanged, only speed (0 = default)."""
+        t = L.Tuning(bundle_bodies, narrow_blocks_per_sm, broad_tile_rows, 0)
+        L.check(L.lib.seevr_physics_set_tuning(self._h, C.byref(t)))
+
     def upload_state(self, num_bodies: int, pos=None, quat=None, vel=None, omega=None) -> None:
         ptr = lambda a: None if a is None else C.c_void_p(a.ctypes.data if isinstance(a, np.ndarray) else a.data_ptr())
         L.check(L.lib.seevr_physics_upload_state(self._h, num_bodies, ptr(pos), ptr(quat),

@@ -115,6 +115,26 @@ def test_bundle_size_does_not_change_results(cuda, frames):
             assert np.array_equal(r[k], runs[0][k]), k
 
 
+def test_golden_fixtures_bit_exact(cuda):
+    """The CUDA path reproduces the committed golden fixtures (tests/golden)
+    bit for bit: body state, pairs, contacts and impulses."""
+    import sys
+    from pathlib import Path
+
+    sys.path.insert(0, str(Path(__file__).resolve().parent / "golden"))
+    import make_golden
+
+    for name, (make, frames, pgs) in sorted(make_golden.CASES.items()):
+        z = np.load(Path(__file__).resolve().parent / "golden" / f"{name}.npz")
+        d = make(Data)
+        assert make_golden.scene_digest(d.arrays()) == str(z["scene_sha256"]), name
+        got = gpu_run(d, cuda, frames=frames, pgs=pgs)
+        assert got["num_pairs"] == int(z["num_pairs"]), name
+        assert got["num_contacts"] == int(z["num_contacts"]), name
+        for k in make_golden.KEYS:
+            assert np.array_equal(np.asarray(got[k]).view(np.uint8), z[k].view(np.uint8)), (name, k)
+
+
 def test_scene_in_batch_equals_scene_alone(cuda):
     batch = Data.batch(num_scenes=16, min_bodies=8, max_bodies=64, seed_base=100)
     off = batch.scene_body_offset()

@@ -504,7 +504,8 @@ __global__ void k_lbvh_write(World w, LbvhView t, const uint32_t* __restrict__ r
     while (remaining > 0 && slot < w.max_pairs) {
         uint32_t buf[kRowBuf];
         uint32_t nbuf = 0;
-        // keep the kRowBuf smallest j > lo, sorted ascending
+        // keep the kRowBuf smallest j > lo, sorted ascending (buf[kRowBuf - 1]
+        // is read only once nbuf == kRowBuf, i.e. after every entry is set)
         traverse(w, t, i, lo, err, [&](uint32_t j) {
             if (nbuf == kRowBuf && j >= buf[kRowBuf - 1]) return;
             uint32_t pos = nbuf < kRowBuf ? nbuf++ : kRowBuf - 1;

@@ -9,6 +9,13 @@ whole batch.  The scenes are pre-rolled (--preroll frames, untimed) so the
 timed frames contain a settling pile rather than free fall.  Under torchrun
 each rank runs its own 4,096 scenes (weak scaling, no collective in the
 step); rank 0 prints one JSON line.
+
+Besides the headline the line carries: the whole-step and per-stage
+roofline, the CPU oracle on a sample of the same scenes and state with the
+GPU's results on that sample compared bit for bit, the plain drop-in, the
+512-body drop-in scene (120 frames at 4 and 30 PGS iterations), the
+32,768-body scene with the LBVH and all-pairs broadphases, the
+differentiable rollout, and the stacked towers.
 """
 from __future__ import annotations
 
@@ -31,6 +38,8 @@ METRIC = ("body-substeps/s batched vs plain step, same B200, ≤1e-4 state err; 
 UNIT = "body-substeps/s"
 DT = 1.0 / 60.0
 G = (0.0, -9.81, 0.0)
+STATE = (("pos", "body_pos", 3), ("quat", "body_quat", 4), ("vel", "body_vel", 3),
+         ("omega", "body_omega", 3))
 
 
 def parse():
@@ -46,9 +55,10 @@ def parse():
     ap.add_argument("--substeps", type=int, default=10)
     ap.add_argument("--pgs", type=int, default=30)
     ap.add_argument("--preroll", type=int, default=90)
+    ap.add_argument("--sample-stride", type=int, default=16,
+                    help="CPU legs run every n-th scene of the batch (same histogram)")
     ap.add_argument("--plain-scenes", type=int, default=32)
-    ap.add_argument("--e2e-steps", type=int, default=3)
-    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--adjoint-scenes", type=int, default=1024)
     ap.add_argument("--adjoint-bodies", type=int, default=64)
@@ -57,7 +67,13 @@ def parse():
     ap.add_argument("--towers", type=int, default=1024)
     ap.add_argument("--tower-height", type=int, default=256)
     ap.add_argument("--tower-frames", type=int, default=20)
+    ap.add_argument("--tower-overlap", type=float, default=0.002)
     ap.add_argument("--no-towers", action="store_true")
+    ap.add_argument("--no-config0", action="store_true")
+    ap.add_argument("--config0-frames", type=int, default=120)
+    ap.add_argument("--no-config1", action="store_true")
+    ap.add_argument("--config1-bodies", type=int, default=32768)
+    ap.add_argument("--config1-frames", type=int, default=60)
     ap.add_argument("--prof-frames", type=int, default=3)
     ap.add_argument("--bundle-bodies", type=int, default=0,
                     help="solver bundle size in bodies (0: the library default)")
@@ -66,18 +82,21 @@ def parse():
     return ap.parse_args()
 
 
-def workload_config(a, nb, ndyn, nhv, nv):
+def workload_config(a, world):
+    """The workload both arms report (identical keys and values)."""
     return {
         "workload": (f"batched scenes: {a.scenes} independent scenes per GPU, dynamic bodies "
                      f"log-uniform {a.min_bodies}-{a.max_bodies} (half boxes with half-extents "
                      f"U(0.2,0.6) m, half {a.segments}-segment UV spheres r U(0.2,0.5) m) on a "
                      f"static ground box, {a.substeps} substeps x {a.pgs} PGS iterations per "
                      f"60 Hz frame, after {a.preroll} untimed frames of settling"),
-        "scenes": a.scenes, "bodies": nb, "dynamic_bodies": ndyn, "hull_verts": nhv,
-        "render_verts": nv, "substeps": a.substeps, "pgs_iterations": a.pgs,
-        "preroll_frames": a.preroll, "dt": DT,
-        "l2": f"inputs larger than L2: {nhv * 12 / 1e6:.0f} MB of hull vertices read per substep",
+        "scenes": a.scenes, "min_bodies": a.min_bodies, "max_bodies": a.max_bodies,
+        "sphere_segments": a.segments, "substeps": a.substeps, "pgs_iterations": a.pgs,
+        "preroll_frames": a.preroll, "dt": DT, "seed": "scene s of rank r: seed r*scenes+s",
+        "l2": "inputs larger than L2: the hull vertices (888 MB at 4,096 scenes) are read "
+              "every substep, no flush needed",
         "broadphase": "all-pairs per scene", "solver": "wavefront (bit-identical to sequential)",
+        "parallelism": f"scenes sharded x{world}",
     }
 
 
@@ -150,76 +169,85 @@ def measured_peaks():
 
 
 # ---------------------------------------------------------------------------
-def oracle_sample(arrays, scenes, frames, a, threads):
-    """Run the CPU oracle on the first `scenes` scenes for `frames` frames;
-    returns (dynamic body-substeps, seconds, out)."""
+# the sample of scenes the CPU legs run
+def sample_seeds(a, rank):
+    """Every `sample_stride`-th scene of this rank's batch: the body-count
+    histogram of the sample follows the batch's."""
+    stride = max(1, a.sample_stride)
+    return [rank * a.scenes + s for s in range(0, a.scenes, stride)]
+
+
+def sample_data(a, rank):
+    from seevr_b200 import Data
+
+    return Data.batch_seeds(sample_seeds(a, rank), min_bodies=a.min_bodies,
+                            max_bodies=a.max_bodies, segments=a.segments)
+
+
+def sample_state(a, full_off, state, rank):
+    """Rows of `state` (per-body arrays of the full batch) that belong to the
+    sampled scenes, concatenated in sample order."""
+    rows = np.concatenate([np.arange(full_off[s - rank * a.scenes],
+                                     full_off[s - rank * a.scenes + 1])
+                           for s in sample_seeds(a, rank)])
+    return {k: v[rows] for k, v in state.items()}
+
+
+def oracle_frames(arrays, state, frames, a, threads):
+    """The CPU oracle: `frames` frames of the scenes in `arrays` from
+    `state`; returns (dynamic body-substeps, seconds, out)."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import pyoracle
 
-    off = arrays["scene_body_offset"]
-    b1 = int(off[scenes])
-    hr = arrays["hull_range"]
-    h0, h1 = 0, int(hr[b1 - 1][0] + hr[b1 - 1][1])
-    vs, vc = arrays["body_vert_start"], arrays["body_vert_count"]
-    v1 = int(vs[b1 - 1] + vc[b1 - 1])
-    sub = {}
-    for k, v in arrays.items():
-        if k in ("hull_verts",):
-            sub[k] = v[h0:h1]
-        elif k in ("orig_vertices", "vertices", "colors"):
-            sub[k] = v[:v1]
-        elif k in ("support_lookup", "indices"):
-            sub[k] = v
-        elif k == "scene_body_offset":
-            sub[k] = off[: scenes + 1]
-        elif len(v) == len(arrays["body_inv_mass"]):
-            sub[k] = v[:b1]
-        else:
-            sub[k] = v
-    ndyn = int((sub["body_inv_mass"] > 0).sum())
+    arr = dict(arrays)
+    if state is not None:
+        for key, name, _ in STATE:
+            arr[name] = np.ascontiguousarray(state[key], dtype=np.float32)
+    nb = len(arr["body_inv_mass"])
+    ndyn = int((arr["body_inv_mass"] > 0).sum())
     t0 = time.perf_counter()
-    out = pyoracle.run(sub, frames=frames, substeps=a.substeps, dt=DT, gravity=G,
-                       pgs_iterations=a.pgs, max_pairs=max(16 * b1, 10000),
-                       max_contacts=max(8 * b1, 4000), threads=threads)
-    dt = time.perf_counter() - t0
-    return ndyn * a.substeps * frames, dt, out
+    out = pyoracle.run(arr, frames=frames, substeps=a.substeps, dt=DT, gravity=G,
+                       pgs_iterations=a.pgs, max_pairs=max(8 * nb, 10000),
+                       max_contacts=max(4 * nb, 4000), threads=threads)
+    secs = time.perf_counter() - t0
+    return ndyn * a.substeps * frames, secs, out
 
 
 def reference_arm(a, rank, world):
     """The reference's path on the host cores: the CPU restatement of
-    physics.comp (the reference's own Vulkan/GLSL step cannot run here)."""
+    physics.comp (the reference's own Vulkan/GLSL step cannot run here), on
+    every `sample_stride`-th scene of the batch, pre-rolled on the CPU like
+    the GPU arm's batch, then `warmup` + `steps` frames timed per step."""
     if rank != 0:
         return 0
-    from seevr_b200 import Data
-
     threads = os.cpu_count() or 1
-    d = Data.batch(num_scenes=a.scenes, min_bodies=a.min_bodies, max_bodies=a.max_bodies,
-                   segments=a.segments, seed_base=0)
+    d = sample_data(a, rank)
     arrays = d.arrays()
-    scenes = max(8, min(a.scenes, 2 * threads))
-    # pre-roll the sample like the GPU arm, then time `steps` frames
-    _, _, out = oracle_sample(arrays, scenes, a.preroll, a, threads)
-    st = dict(arrays)
-    b1 = int(arrays["scene_body_offset"][scenes])
-    for key, name in (("pos", "body_pos"), ("quat", "body_quat"), ("vel", "body_vel"),
-                      ("omega", "body_omega")):
-        x = arrays[name].copy()
-        x[:b1] = out[key].astype(np.float32)
-        st[name] = x
+    _, _, out = oracle_frames(arrays, None, a.preroll, a, threads)
+    st = {k: out[k].astype(np.float32) for k, _, _ in STATE}
     for _ in range(a.warmup):
-        oracle_sample(st, scenes, 1, a, threads)
-    work, secs, _ = oracle_sample(st, scenes, a.steps, a, threads)
+        _, _, out = oracle_frames(arrays, st, 1, a, threads)
+        st = {k: out[k].astype(np.float32) for k, _, _ in STATE}
+    work, secs = 0, 0.0
+    for _ in range(a.steps):
+        w_, s_, out = oracle_frames(arrays, st, 1, a, threads)
+        st = {k: out[k].astype(np.float32) for k, _, _ in STATE}
+        work += w_
+        secs += s_
     value = work / secs
-    nb = d.num_bodies
+    n = np.diff(d.scene_body_offset())
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": secs / a.steps * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "impl": "reference",
-        "config": workload_config(a, nb, d.num_dynamic, d.num_hull_verts, d.num_vertices),
+        "config": workload_config(a, world),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"first {scenes} of {a.scenes} scenes, {a.steps} frames after "
-                                   f"{a.preroll} pre-roll frames, one OpenMP thread per scene"},
+                         "sample": f"every {a.sample_stride}th of the {a.scenes} scenes "
+                                   f"({len(n)} scenes, mean {n.mean():.1f} bodies per scene "
+                                   f"against {d_batch_mean(a):.1f} in the batch), pre-rolled "
+                                   f"{a.preroll} frames on the CPU, {a.steps} frames timed, "
+                                   f"OpenMP over scenes"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": ("reference GLSL/Vulkan step unavailable on this box (no graphics stack, no Zig "
                  "toolchain); timed its CPU restatement"),
@@ -228,7 +256,19 @@ def reference_arm(a, rank, world):
     return 0
 
 
+def d_batch_mean(a):
+    from seevr_b200 import Data
+
+    d = Data.batch(num_scenes=a.scenes, min_bodies=a.min_bodies, max_bodies=a.max_bodies,
+                   segments=a.segments, seed_base=0)
+    return float(np.diff(d.scene_body_offset()).mean())
+
+
 # ---------------------------------------------------------------------------
+def read_state(buf, nb):
+    return {k: buf[n][: nb * c].cpu().numpy().reshape(nb, c).copy() for k, n, c in STATE}
+
+
 def ours(a, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -241,9 +281,11 @@ def ours(a, rank, world, local_rank):
     d = Data.batch(num_scenes=a.scenes, min_bodies=a.min_bodies, max_bodies=a.max_bodies,
                    segments=a.segments, seed_base=rank * a.scenes)
     nb, nhv, nv, ndyn = d.num_bodies, d.num_hull_verts, d.num_vertices, d.num_dynamic
+    off = d.scene_body_offset()
     caps = Caps.for_data(d, pairs_per_body=8.0, contacts_per_body=4.0)
     buf = d.upload(dev, caps)
-    ph = Physics(buf, make_params(pgs_iterations=a.pgs, flags=FLAG_CUDA_GRAPH, bundle_bodies=a.bundle_bodies))
+    ph = Physics(buf, make_params(pgs_iterations=a.pgs, flags=FLAG_CUDA_GRAPH,
+                                  bundle_bodies=a.bundle_bodies))
     stream = torch.cuda.Stream(dev)
 
     def frames(n):
@@ -256,11 +298,9 @@ def ours(a, rank, world, local_rank):
     if a.autotune:  # launch shapes timed on the settled state (restored afterwards)
         from seevr_b200.tune import autotune
         autotune(ph, buf, a.substeps, DT, G, frames=2, repeats=2)
-    pre_state = {k: buf[n][: nb * c].cpu().numpy().reshape(nb, c) for k, n, c in (
-        ("pos", "body_pos", 3), ("quat", "body_quat", 4), ("vel", "body_vel", 3),
-        ("omega", "body_omega", 3))}
     frames(a.warmup)
     stream.synchronize()
+    t0_state = read_state(buf, nb)  # the state the timed region starts from
 
     # ---- timed region: K graph replays, CUDA events on the launching stream
     if world > 1:
@@ -278,6 +318,7 @@ def ours(a, rank, world, local_rank):
         dist.barrier()
     ms = e0.elapsed_time(e1)
     launches = ph.kernel_launches - launches0
+    flags = ph.read_flags()
     t = torch.tensor([ms], dtype=torch.float64, device=dev)
     work = torch.tensor([float(ndyn)], dtype=torch.float64, device=dev)
     if world > 1:
@@ -287,55 +328,56 @@ def ours(a, rank, world, local_rank):
     total_dyn = float(work.item())
     value = total_dyn * a.substeps * a.steps / (ms_max / 1e3)
     ms_per_step = ms_max / a.steps
-    counters = ph.read_counters()
+    pairs, contacts = ph.read_counters()
+    end_state = read_state(buf, nb)
 
-    # ---- per-stage device times of one frame (profiling mode)
+    # ---- e2e: the same K frames from the same state through the C ABI,
+    # the state copied in from pinned host memory and back out every frame
+    host = {k: torch.from_numpy(np.ascontiguousarray(v, dtype=np.float32)).pin_memory()
+            for k, v in t0_state.items()}
+    h2d = d2h = sum(host[k].numel() * 4 for k in host)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    tw = time.perf_counter()
+    for _ in range(a.steps):
+        ph.upload_state(nb, host["pos"], host["quat"], host["vel"], host["omega"])
+        ph.step_async(nb, nv, nhv, a.substeps, DT, G, frames=1)
+        ph.download_state(nb, host["pos"], host["quat"], host["vel"], host["omega"])
+    e2e_s = time.perf_counter() - tw
+    et = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(et, op=dist.ReduceOp.MAX)
+    e2e_value = total_dyn * a.substeps * a.steps / float(et.item())
+    e2e_same = all(np.array_equal(host[k].numpy(), end_state[k]) for k in host)
+
+    # ---- per-stage device times of one frame (profiling mode, separate
+    # handle; the state continues from the end of the e2e frames)
     ph_prof = Physics(buf, make_params(pgs_iterations=a.pgs, bundle_bodies=a.bundle_bodies))
     prof = Profile()
     for _ in range(a.prof_frames):
         ph_prof.step(nb, nv, nhv, a.substeps, DT, G, prof)
-    pairs, contacts = ph_prof.read_counters()
     ph_prof.deinit()
     stage_ms = {STAGE_NAMES[i]: prof.ms[i] / a.prof_frames for i in range(len(STAGE_NAMES))}
+    tuning = ph.get_tuning()
+    ph.deinit()
 
-    # ---- e2e: host state in pinned memory -> device, frame, device -> host
-    host = {k: torch.from_numpy(np.ascontiguousarray(v, dtype=np.float32)).pin_memory()
-            for k, v in pre_state.items()}
-    ph_e2e = Physics(buf, make_params(pgs_iterations=a.pgs, flags=FLAG_CUDA_GRAPH, bundle_bodies=a.bundle_bodies))
-    ph_e2e.set_tuning(**ph.get_tuning())  # the same launch shapes as the timed handle
-    h2d = d2h = nb * (12 + 16 + 12 + 12)
-    ph_e2e.upload_state(nb, host["pos"], host["quat"], host["vel"], host["omega"])
-    ph_e2e.step_async(nb, nv, nhv, a.substeps, DT, G, frames=1)  # capture
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    t0 = time.perf_counter()
-    for _ in range(a.e2e_steps):
-        ph_e2e.upload_state(nb, host["pos"], host["quat"], host["vel"], host["omega"])
-        ph_e2e.step_async(nb, nv, nhv, a.substeps, DT, G, frames=1)
-        ph_e2e.download_state(nb, host["pos"], host["quat"], host["vel"], host["omega"])
-    e2e_s = time.perf_counter() - t0
-    et = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(et, op=dist.ReduceOp.MAX)
-    e2e_value = total_dyn * a.substeps * a.e2e_steps / float(et.item())
-    ph_e2e.deinit()
-
-    # ---- plain drop-in: one handle per scene, synchronous Physics.step,
-    # looped over a sample of scenes from the same pre-rolled state
-    plain = None
-    if rank == 0 and a.plain_scenes > 0:
-        plain = plain_dropin(a, d, pre_state, dev)
-
-    # ---- roofline of the dominant stage kernel
     peak, peak_kind = measured_peaks()
-    roof = roofline(stage_ms, nb, nhv, nv, pairs, contacts, a.substeps, peak, peak_kind,
-                    NCU_TRAFFIC_DEFAULT if default_workload(a) else None)
+    roof = roofline(stage_ms, ms_per_step, nb, nhv, nv, pairs, contacts, a.substeps, peak,
+                    peak_kind, a)
 
-    cpu = None
-    if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        cpu = cpu_baseline(a, d, pre_state)
-
+    extras = {}
+    if rank == 0:
+        if a.plain_scenes > 0:
+            extras["plain"] = plain_dropin(a, d, t0_state, dev)
+        if world == 1 and not a.no_cpu_baseline:
+            extras["cpu_baseline"], extras["parity"] = cpu_baseline(a, off, t0_state, dev, rank)
+        if world == 1 and not a.no_config0:
+            extras["config0"] = config0_leg(a, dev)
+        if world == 1 and not a.no_config1:
+            extras["config1"] = config1_leg(a, dev)
+    del buf
+    torch.cuda.empty_cache()
     adj = None if a.no_adjoint else adjoint_leg(a, rank, world, dev)
     tow = None if a.no_towers or world > 1 else towers_leg(a, rank, world, dev)
 
@@ -345,23 +387,30 @@ def ours(a, rank, world, local_rank):
             "warmup": a.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded splitmix64 scenes)",
-            "config": workload_config(a, nb, ndyn, nhv, nv) | {"parallelism": f"scenes x{world}",
-                                                               "tuning": ph.get_tuning(),
-                                                               "autotuned": bool(a.autotune)},
+            "config": workload_config(a, world),
+            "tuning": tuning | {"autotuned": bool(a.autotune)},
+            "bodies": nb, "dynamic_bodies": ndyn, "hull_verts": nhv, "render_verts": nv,
             "clocks": clk.summary(),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h},
+                    "d2h_bytes_per_step": d2h,
+                    "how": ("the timed region's frames from its starting state, through "
+                            "seevr_physics_upload_state / step_async / download_state with "
+                            "pinned host arrays, wall clock, max over ranks"),
+                    "same_final_state_as_timed_region": e2e_same},
             "gpu_launches": launches,
+            "device_flags": flags,
             "roofline": roof,
-            "cpu_baseline": cpu,
-            "plain": plain,
+            "cpu_baseline": extras.get("cpu_baseline"),
+            "parity": extras.get("parity"),
+            "plain": extras.get("plain"),
+            "config0": extras.get("config0"),
+            "config1": extras.get("config1"),
             "adjoint": adj,
             "towers": tow,
             "stage_ms_per_frame": stage_ms,
             "last_substep": {"pairs": pairs, "contacts": contacts},
         }
         print(json.dumps(line))
-    ph.deinit()
     return 0
 
 
@@ -392,9 +441,7 @@ def adjoint_leg(a, rank, world, dev):
     target = torch.tensor(rng.uniform(-1.0, 1.0, (a.adjoint_scenes, 3)) + [0.0, 1.0, 0.0],
                           dtype=torch.float32, device=dev)
     t = buf.tensors
-    init = {k: t[n][: nb * c].clone().reshape(nb, c) for k, n, c in (
-        ("pos", "body_pos", 3), ("quat", "body_quat", 4), ("vel", "body_vel", 3),
-        ("omega", "body_omega", 3))}
+    init = {k: t[n][: nb * c].clone().reshape(nb, c) for k, n, c in STATE}
     fr0 = t["geom_friction"][:nb].clone()
 
     def one(frames):
@@ -441,17 +488,19 @@ def adjoint_leg(a, rank, world, dev):
 
 def towers_leg(a, rank, world, dev):
     """Stacked boxes: --towers towers of --tower-height unit boxes (jitter
-    N(0, 0.01) m, friction 0.6, no restitution) on one static ground, one
-    scene, LBVH broadphase, island-parallel PGS, --tower-frames frames of 10
-    substeps x 30 iterations.  Coloured vs wavefront (= sequential) order:
-    throughput and the tower tops' drift at the end."""
+    N(0, 0.01) m, friction 0.6, no restitution, each box sunk
+    --tower-overlap m into the one below so that every stack contact exists
+    from the first substep) on one static ground, one scene, LBVH
+    broadphase, island-parallel PGS, --tower-frames frames of 10 substeps x
+    30 iterations.  Coloured vs wavefront (= sequential) order: throughput,
+    contacts per substep and the tower tops' drift."""
     import torch
 
     from seevr_b200 import (BROADPHASE_LBVH, FLAG_CUDA_GRAPH, FLAG_SKIP_RENDER_VERTS, Caps, Data,
                             Physics, SOLVER_COLORED, SOLVER_WAVEFRONT, make_params)
 
     h = a.tower_height
-    d = Data.towers(seed=rank, towers=a.towers, height=h, spacing=2.0)
+    d = Data.towers(seed=rank, towers=a.towers, height=h, spacing=2.0, overlap=a.tower_overlap)
     nb, nhv = d.num_bodies, d.num_hull_verts
     caps = Caps.for_data(d, pairs_per_body=4.0, contacts_per_body=4.0)
     buf = d.upload(dev, caps)
@@ -467,28 +516,39 @@ def towers_leg(a, rank, world, dev):
                                       broadphase=BROADPHASE_LBVH,
                                       flags=FLAG_CUDA_GRAPH | FLAG_SKIP_RENDER_VERTS))
         torch.cuda.synchronize()
+        ph.step_async(nb, 0, nhv, a.substeps, DT, G, frames=1, stream=stream)  # capture
+        stream.synchronize()
+        c_first = ph.read_counters()[1]
+        for k, v in init.items():
+            buf.tensors[k].copy_(v)
+        torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        with torch.cuda.stream(stream):
-            e0.record(stream)
-            ph.step_async(nb, 0, nhv, a.substeps, DT, G, frames=a.tower_frames, stream=stream)
-            e1.record(stream)
+        e0.record(stream)
+        ph.step_async(nb, 0, nhv, a.substeps, DT, G, frames=a.tower_frames, stream=stream)
+        e1.record(stream)
         e1.synchronize()
         ms = e0.elapsed_time(e1)
         flags = ph.read_flags()
+        c_last = ph.read_counters()[1]
         top = buf.tensors["body_pos"][: nb * 3].reshape(-1, 3)[tops, 1]
         drift = (top - top0).abs()
         out[name] = {"value": (nb - 1) * a.substeps * a.tower_frames / (ms / 1e3),
                      "ms_per_frame": ms / a.tower_frames,
-                     "top_drift_mean_m": float(drift.mean()), "top_drift_max_m": float(drift.max()),
+                     "contacts_first_frame": c_first, "contacts_last_substep": c_last,
+                     "top_drift_mean_m": float(drift.mean()),
+                     "top_drift_max_m": float(drift.max()),
+                     "towers_standing": int((drift < 0.5).sum()),
                      "finite": bool(torch.isfinite(buf.tensors["body_pos"][: nb * 3]).all()),
                      "device_flags": flags}
         ph.deinit()
     return {"unit": UNIT, "bodies": nb, "towers": a.towers, "height": h,
-            "frames": a.tower_frames, "substeps": a.substeps, "pgs_iterations": a.pgs,
-            "broadphase": "LBVH", "solver_work": "islands (one per tower)", **out}
+            "overlap_m": a.tower_overlap, "frames": a.tower_frames, "substeps": a.substeps,
+            "pgs_iterations": a.pgs, "broadphase": "LBVH",
+            "solver_work": "islands (one per tower while the towers stand)",
+            "contact_model": "one MPR contact per touching pair (physics.comp:475-491)", **out}
 
 
-def plain_dropin(a, d, pre_state, dev):
+def plain_dropin(a, d, state, dev):
     """Plain single-scene step (the Physics.step drop-in, synchronous) looped
     over the first scenes; also the state error of the batched step against
     it after one frame from the same state."""
@@ -498,14 +558,13 @@ def plain_dropin(a, d, pre_state, dev):
 
     off = d.scene_body_offset()
     n = min(a.plain_scenes, a.scenes)
-    # the batched step over the same scenes for one frame, from pre_state
+    # the batched step over the same scenes for one frame, from `state`
     sub_batch = Data.batch(num_scenes=n, min_bodies=a.min_bodies, max_bodies=a.max_bodies,
                            segments=a.segments, seed_base=0)
     b1 = int(off[n])
     bbuf = sub_batch.upload(dev)
-    for key, name, c in (("pos", "body_pos", 3), ("quat", "body_quat", 4), ("vel", "body_vel", 3),
-                         ("omega", "body_omega", 3)):
-        bbuf[name][: b1 * c].copy_(torch.from_numpy(pre_state[key][:b1].reshape(-1)))
+    for key, name, c in STATE:
+        bbuf[name][: b1 * c].copy_(torch.from_numpy(state[key][:b1].reshape(-1)))
     bph = Physics(bbuf, make_params(pgs_iterations=a.pgs))
     bph.step(b1, sub_batch.num_vertices, sub_batch.num_hull_verts, a.substeps, DT, G)
     batched_pos = bbuf["body_pos"][: b1 * 3].cpu().numpy().reshape(-1, 3)
@@ -519,14 +578,12 @@ def plain_dropin(a, d, pre_state, dev):
                          segments=a.segments, seed_base=s)
         lo, hi = int(off[s]), int(off[s + 1])
         buf = one.upload(dev, Caps.for_data(one))
-        for key, name, c in (("pos", "body_pos", 3), ("quat", "body_quat", 4),
-                             ("vel", "body_vel", 3), ("omega", "body_omega", 3)):
-            buf[name][: (hi - lo) * c].copy_(torch.from_numpy(pre_state[key][lo:hi].reshape(-1)))
+        for key, name, c in STATE:
+            buf[name][: (hi - lo) * c].copy_(torch.from_numpy(state[key][lo:hi].reshape(-1)))
         ph = Physics(buf, make_params(pgs_iterations=a.pgs))
         ph.step(hi - lo, one.num_vertices, one.num_hull_verts, a.substeps, DT, G)  # warm
-        for key, name, c in (("pos", "body_pos", 3), ("quat", "body_quat", 4),
-                             ("vel", "body_vel", 3), ("omega", "body_omega", 3)):
-            buf[name][: (hi - lo) * c].copy_(torch.from_numpy(pre_state[key][lo:hi].reshape(-1)))
+        for key, name, c in STATE:
+            buf[name][: (hi - lo) * c].copy_(torch.from_numpy(state[key][lo:hi].reshape(-1)))
         torch.cuda.synchronize()
         e0.record(torch.cuda.current_stream())
         ph.step(hi - lo, one.num_vertices, one.num_hull_verts, a.substeps, DT, G)
@@ -545,17 +602,64 @@ def plain_dropin(a, d, pre_state, dev):
             "batched_vs_plain_max_rel_state_err": err}
 
 
-# DRAM bytes (read + write) per substep launch of each stage's main kernel,
-# from one ncu capture of the default workload (4,096 scenes, bodies 8-512,
-# 16-segment spheres, 10 substeps x 30 PGS iterations, 20 substeps after the
-# 90-frame pre-roll: profiles/launches_batched4096.md).  Reported as
-# roofline.traffic only when the bench runs that workload.
-NCU_TRAFFIC_DEFAULT = {
-    "phys/pgs_solve": ("k_solver_warp", 43545792),
-    "phys/narrow_phase": ("k_narrow", 805700000),
-    "phys/aabb": ("k_body_stage", 1023200000),
-    "phys/broad_phase": ("k_broad_tile (count + write)", 37183770 + 23357722),
-}
+# Figures of single-kernel ncu captures (not measured by this run): per
+# main kernel of each stage, DRAM bytes per launch and issue/warp
+# utilisation, captured on a 1,024-scene batch (same distributions, 0.25x the
+# bodies) and scaled to this workload by bodies (body stage, broadphase,
+# solver) or pairs (narrowphase).  The command is given with each entry.
+NCU_CAPTURE = {}
+
+
+def roofline(stage_ms, ms_per_step, nb, nhv, nv, pairs, contacts, substeps, peak, peak_kind, a):
+    """Whole-step HBM roofline (algorithmic bytes per frame over the timed
+    frame) and one entry per stage with the bound that limits it.
+
+    Algorithmic bytes per substep (the minimum traffic of each stage as the
+    reference sequence moves it; pairs and contacts of the last substep):
+      body stage  = integrate 84N + gravity 52N + AABB 60N + 12 per hull vertex
+      broadphase  = 28N + 8P;  narrowphase = 64P + 36C;  impulse clear = 4C;
+      solver      = 100N + 44C;  and per frame the render vertices 28N + 24V.
+    """
+    per_substep = {
+        "phys/aabb": ("k_body_stage", "hbm", 196 * nb + 12 * nhv),
+        "phys/broad_phase": ("k_broad_tile (count, scan, write)", "issue: compare pipe",
+                             28 * nb + 8 * pairs),
+        "phys/narrow_phase": ("k_narrow (+ scan, scatter)", "latency: dependent gathers, "
+                              "divergence", 64 * pairs + 36 * contacts),
+        "phys/clear_impulse": ("memset", "hbm", 4 * contacts),
+        "phys/pgs_solve": ("k_solver_warp", "latency: dependent chain of the largest bundle",
+                           100 * nb + 44 * contacts),
+    }
+    once = {"phys/render_verts": ("k_render_verts", "hbm", 28 * nb + 24 * nv)}
+    frame_bytes = substeps * (324 * nb + 12 * nhv + 72 * pairs + 84 * contacts) + \
+        28 * nb + 24 * nv
+    achieved = frame_bytes / (ms_per_step / 1e3) / 1e9
+    total_stage = max(sum(stage_ms.values()), 1e-9)
+    stages = []
+    for k, ms in sorted(stage_ms.items(), key=lambda kv: -kv[1]):
+        if ms <= 0:
+            continue
+        kern, bound, algo = per_substep.get(k) or once.get(k) or ("", "", 0)
+        launch_ms = ms / (substeps if k in per_substep else 1)
+        gbs = algo / (launch_ms / 1e3) / 1e9 if launch_ms > 0 else 0.0
+        e = {"stage": k, "kernel": kern, "bound": bound, "share": ms / total_stage,
+             "launch_ms": launch_ms, "algorithmic_bytes_per_launch": algo,
+             "achieved_gbs": gbs, "hbm_frac": gbs / peak}
+        if k in NCU_CAPTURE and default_workload(a):
+            e["ncu"] = NCU_CAPTURE[k]
+        stages.append(e)
+    traffic = None
+    if default_workload(a) and all(k in NCU_CAPTURE for k in per_substep if k != "phys/clear_impulse"):
+        traffic = sum(substeps * NCU_CAPTURE[k]["dram_bytes_per_launch"]
+                      for k in per_substep if k != "phys/clear_impulse")
+    return {"bound": "hbm", "kernel": f"whole frame ({substeps} substeps + render vertices)",
+            "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "peak_source": peak_kind, "traffic": traffic,
+            "traffic_source": ("sum over the stage kernels of their ncu-captured DRAM bytes "
+                               "per launch (stages[].ncu)") if traffic else None,
+            "algorithmic_bytes_per_frame": frame_bytes,
+            "dominant_stage": stages[0]["stage"] if stages else None,
+            "stages": stages}
 
 
 def default_workload(a):
@@ -563,48 +667,172 @@ def default_workload(a):
         (4096, 8, 512, 16, 10, 30, 90)
 
 
-def roofline(stage_ms, nb, nhv, nv, pairs, contacts, substeps, peak, peak_kind, traffic_table=None):
-    """Algorithmic bytes per launch of each stage kernel (last-substep pair and
-    contact counts) over its measured time; the dominant stage is reported."""
-    per_substep = {
-        "phys/aabb": 196 * nb + 12 * nhv,          # integrate 84N + gravity 52N + AABB 60N+12V
-        "phys/broad_phase": 28 * nb + 8 * pairs,
-        "phys/narrow_phase": 64 * pairs + 36 * contacts,
-        "phys/pgs_solve": 100 * nb + 44 * contacts,
-        "phys/clear_impulse": 4 * contacts,
-    }
-    once = {"phys/render_verts": 28 * nb + 24 * nv}
-    best = max(stage_ms, key=lambda k: stage_ms[k])
-    t_launch = stage_ms[best] / (substeps if best in per_substep else 1)
-    algo = per_substep.get(best, once.get(best, 0))
-    achieved = algo / (t_launch / 1e3) / 1e9 if t_launch > 0 else 0.0
-    measured = (traffic_table or {}).get(best)
-    return {"bound": "hbm", "kernel": best, "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "peak_source": peak_kind,
-            "traffic": measured[1] if measured else None,
-            "traffic_kernel": measured[0] if measured else None,
-            "algorithmic_bytes_per_launch": algo, "launch_ms": t_launch,
-            "note": "stage share of the frame: " + ", ".join(
-                f"{k.split('/')[1]} {v / max(sum(stage_ms.values()), 1e-9):.0%}"
-                for k, v in sorted(stage_ms.items(), key=lambda kv: -kv[1]) if v > 0)}
+def cpu_baseline(a, full_off, state, dev, rank):
+    """The CPU oracle on every `sample_stride`-th scene of the batch from the
+    state the timed region starts from, and the CUDA path on the same scenes
+    from the same state for the same frames, compared bit for bit."""
+    import torch
 
-
-def cpu_baseline(a, d, pre_state):
-    """The CPU oracle on a bounded sample of the same workload and state."""
     threads = os.cpu_count() or 1
+    d = sample_data(a, rank)
     arrays = d.arrays()
-    for key, name in (("pos", "body_pos"), ("quat", "body_quat"), ("vel", "body_vel"),
-                      ("omega", "body_omega")):
-        arrays[name] = pre_state[key].astype(np.float32)
-    scenes = max(8, min(a.scenes, 2 * threads))
-    work, secs, _ = oracle_sample(arrays, scenes, 1, a, threads)
+    st = sample_state(a, full_off, state, rank)
+    work, secs, out = oracle_frames(arrays, st, 1, a, threads)
     frames = 1
-    if secs < a.cpu_seconds / 4:
-        frames = max(1, min(10, int(a.cpu_seconds / max(secs, 1e-3))))
-        work, secs, _ = oracle_sample(arrays, scenes, frames, a, threads)
-    return {"value": work / secs, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"first {scenes} of {a.scenes} scenes, {frames} frame(s) from the same "
-                      f"pre-rolled state, OpenMP over scenes"}
+    if secs < a.cpu_seconds / 2:
+        frames = max(1, min(a.steps, int(a.cpu_seconds / max(secs, 1e-3))))
+        work, secs, out = oracle_frames(arrays, st, frames, a, threads)
+    n = np.diff(d.scene_body_offset())
+    cpu = {"value": work / secs, "unit": UNIT, "cores": threads, "kind": "port",
+           "sample": f"every {a.sample_stride}th of the {a.scenes} scenes ({len(n)} scenes, "
+                     f"{n.sum()} bodies, {n.max()} in the largest), {frames} frame(s) from the "
+                     f"state the timed region starts from, OpenMP over scenes"}
+    got = gpu_frames(d, st, frames, a, dev)
+    keys = ("pos", "quat", "vel", "omega", "pairs", "c_a", "c_b", "c_pos", "c_normal", "c_pen",
+            "lambda")
+    same = {k: bool(np.array_equal(got[k], np.asarray(out[k]).astype(got[k].dtype)))
+            for k in keys}
+    parity = {"scenes": int(len(n)), "bodies": int(n.sum()), "largest_scene": int(n.max()),
+              "scenes_over_256_bodies": int((n > 256).sum()), "frames": frames,
+              "pairs": int(out["num_pairs"]), "contacts": int(out["num_contacts"]),
+              "counters_equal": (got["num_pairs"], got["num_contacts"]) ==
+                                (int(out["num_pairs"]), int(out["num_contacts"])),
+              "bit_exact": all(same.values()) and (got["num_pairs"], got["num_contacts"]) ==
+                           (int(out["num_pairs"]), int(out["num_contacts"])),
+              "keys": same,
+              "against": "FP32 CPU oracle, same scenes, same starting state, same frames; "
+                         "the GPU runs them as one batched CUDA-graph handle"}
+    del got
+    torch.cuda.empty_cache()
+    return cpu, parity
+
+
+def gpu_frames(d, state, frames, a, dev):
+    """The batched CUDA-graph step on the scenes of `d` from `state` for
+    `frames` frames; the outputs the oracle also returns."""
+    import torch
+
+    from seevr_b200 import FLAG_CUDA_GRAPH, FLAG_SKIP_RENDER_VERTS, Caps, Physics, make_params
+
+    nb = d.num_bodies
+    caps = Caps(nb, max(d.num_hull_verts, 1), max(d.num_vertices, 1), max(8 * nb, 10000),
+                max(4 * nb, 4000), max(d.num_scenes, 1))
+    buf = d.upload(dev, caps)
+    for key, name, c in STATE:
+        buf[name][: nb * c].copy_(torch.from_numpy(np.ascontiguousarray(state[key]).reshape(-1)))
+    ph = Physics(buf, make_params(pgs_iterations=a.pgs, bundle_bodies=a.bundle_bodies,
+                                  flags=FLAG_CUDA_GRAPH | FLAG_SKIP_RENDER_VERTS))
+    ph.step_async(nb, 0, d.num_hull_verts, a.substeps, DT, G, frames=frames)
+    torch.cuda.synchronize()
+    ph.deinit()
+    t = buf.tensors
+    cnt = t["counters"][:2].cpu().numpy().view(np.uint32)
+    npairs, nc = int(min(cnt[0], caps.max_pairs)), int(min(cnt[1], caps.max_contacts))
+    out = read_state(buf, nb)
+    out.update({
+        "num_pairs": int(cnt[0]), "num_contacts": int(cnt[1]),
+        "pairs": t["collision_pairs"][: npairs * 2].cpu().numpy().view(np.uint32).reshape(-1, 2),
+        "c_pos": t["contact_pos"][: nc * 3].cpu().numpy().reshape(-1, 3),
+        "c_normal": t["contact_normal"][: nc * 3].cpu().numpy().reshape(-1, 3),
+        "c_pen": t["contact_pen"][:nc].cpu().numpy(),
+        "lambda": t["lambda_n"][:nc].cpu().numpy(),
+        "c_a": t["contact_geom_a"][:nc].cpu().numpy().view(np.uint32),
+        "c_b": t["contact_geom_b"][:nc].cpu().numpy().view(np.uint32),
+    })
+    return out
+
+
+def config0_leg(a, dev):
+    """The plain drop-in scene: 256 boxes + 256 16-segment spheres on the
+    ground (seed 0), 120 frames of synchronous Physics.step at the
+    reference's 4 and at 30 PGS iterations, beside the single-threaded CPU
+    oracle over the same frames; the final states are compared."""
+    import torch
+
+    from seevr_b200 import Caps, Data, Physics, make_params
+
+    out = {"scene": "256 boxes + 256 spheres (16 segments), seed 0, ground box",
+           "frames": a.config0_frames, "how": "synchronous Physics.step per frame (the drop-in)"}
+    d = Data.pile(seed=0)
+    caps = Caps.for_data(d)
+    for pgs in (4, 30):
+        buf = d.upload(dev, caps)
+        nb, nv, nhv = buf.num_bodies, buf.num_vertices, buf.num_hull_verts
+        ph = Physics(buf, make_params(pgs_iterations=pgs))
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(a.config0_frames):
+            ph.step(nb, nv, nhv, a.substeps, DT, G)
+        e1.record()
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        pairs, contacts = ph.read_counters()
+        gpu_state = read_state(buf, nb)
+        ph.deinit()
+        b = dict(a.__dict__)
+        b["pgs"] = pgs
+        work, secs, ref = oracle_frames(d.arrays(), None, a.config0_frames,
+                                        argparse.Namespace(**b), 1)
+        exact = all(np.array_equal(gpu_state[k], ref[k].astype(np.float32)) for k, _, _ in STATE)
+        out[f"pgs{pgs}"] = {"gpu": work / (ms / 1e3), "gpu_ms_per_frame": ms / a.config0_frames,
+                            "cpu_oracle_1_thread": work / secs, "unit": UNIT,
+                            "pairs_last_substep": pairs, "contacts_last_substep": contacts,
+                            "final_state_bit_exact": bool(exact)}
+        del buf
+    return out
+
+
+def config1_leg(a, dev):
+    """The large scene: --config1-bodies bodies (40% boxes, 40% spheres, 20%
+    hulls of 16-32 points) in a 64 m cube with velocities N(0,1), stepped
+    --config1-frames frames with the LBVH broadphase and with the all-pairs
+    broadphase from the same state: time per frame and per stage, and the
+    final pair lists and states compared."""
+    import torch
+
+    from seevr_b200 import (BROADPHASE_LBVH, BROADPHASE_N2, FLAG_CUDA_GRAPH, Caps, Data, Physics,
+                            Profile, STAGE_NAMES, make_params)
+
+    d = Data.large(seed=0, n_bodies=a.config1_bodies)
+    caps = Caps.for_data(d, pairs_per_body=8.0, contacts_per_body=4.0)
+    out = {"bodies": d.num_bodies, "frames": a.config1_frames,
+           "scene": "40% boxes, 40% 16-segment spheres, 20% hulls of 16-32 points, 64 m cube, "
+                    "v N(0,1), seed 0"}
+    res = {}
+    for name, bp in (("lbvh", BROADPHASE_LBVH), ("all_pairs", BROADPHASE_N2)):
+        buf = d.upload(dev, caps)
+        nb, nv, nhv = buf.num_bodies, buf.num_vertices, buf.num_hull_verts
+        ph = Physics(buf, make_params(pgs_iterations=a.pgs, broadphase=bp, flags=FLAG_CUDA_GRAPH))
+        stream = torch.cuda.Stream(dev)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ph.step_async(nb, nv, nhv, a.substeps, DT, G, frames=a.config1_frames, stream=stream)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)  # includes the graph capture of the first frame
+        pairs, contacts = ph.read_counters()
+        st = read_state(buf, nb)
+        pl = buf["collision_pairs"][: min(pairs, caps.max_pairs) * 2].cpu().numpy().copy()
+        ph.deinit()
+        # per-stage times of one more frame in profiling mode
+        php = Physics(buf, make_params(pgs_iterations=a.pgs, broadphase=bp))
+        prof = Profile()
+        php.step(nb, nv, nhv, a.substeps, DT, G, prof)
+        php.deinit()
+        res[name] = (st, pl)
+        out[name] = {"value": d.num_dynamic * a.substeps * a.config1_frames / (ms / 1e3),
+                     "unit": UNIT, "ms_per_frame": ms / a.config1_frames,
+                     "pairs_last_substep": pairs, "contacts_last_substep": contacts,
+                     "stage_ms_next_frame": {STAGE_NAMES[i]: prof.ms[i]
+                                             for i in range(len(STAGE_NAMES)) if prof.ms[i] > 0}}
+        del buf
+        torch.cuda.empty_cache()
+    out["pair_lists_equal"] = bool(np.array_equal(res["lbvh"][1], res["all_pairs"][1]))
+    out["states_equal"] = all(np.array_equal(res["lbvh"][0][k], res["all_pairs"][0][k])
+                              for k, _, _ in STATE)
+    return out
 
 
 def main():

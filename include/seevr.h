@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define SEEVR_ABI_VERSION 1
+#define SEEVR_ABI_VERSION 2
 
 typedef enum seevr_status {
     SEEVR_OK = 0,
@@ -220,7 +220,9 @@ seevr_status seevr_physics_read_counters(seevr_physics* h, uint32_t out[2]);
 /* Overflow and error flags accumulated since the last call (bit 0: pairs
  * overflowed, bit 1: contacts overflowed, bit 2: a device wait timed out,
  * bit 3: a scene exceeded the solver's per-scene limits and took the
- * global-memory path).  Cleared by the call. */
+ * global-memory path, bit 4: a bounds check failed (SEEVR_CHECK=1), bit 5:
+ * in the coloured mode, islands of more than 4,096 contacts were solved by
+ * the whole grid).  Cleared by the call. */
 seevr_status seevr_physics_read_flags(seevr_physics* h, uint32_t* flags);
 
 /* Launch shapes of the batched step (no counterpart in the reference, whose
@@ -232,19 +234,54 @@ seevr_status seevr_physics_read_flags(seevr_physics* h, uint32_t* flags);
  *  - narrow_blocks_per_sm: blocks per SM of the persistent narrowphase grid,
  *    1 to 7 (0 = 7, the register budget's maximum);
  *  - broad_tile_rows: rows of a scene per all-pairs broadphase block, 8 to
- *    2,048 (0 = 64).
+ *    2,048 (0 = 64);
+ *  - scene_groups: 1 to 8 (0 = 1).  With more than one, the scenes are split
+ *    into that many contiguous ranges of about equal bodies, each stepped
+ *    through the whole frame on its own stream (one branch of the captured
+ *    frame graph), so that one range's solver, whose time is its largest
+ *    scene's dependent chain, overlaps the other ranges' collision stages.
+ *    Each range keeps its own pair and contact lists (the handle's
+ *    capacities each); they are merged into the bound buffers in canonical
+ *    order at the end of every frame, so pairs, contacts, impulses, state
+ *    and counters are bit for bit those of one group.  Needs scenes set,
+ *    the all-pairs broadphase, no bounds-check mode, and every geom's body
+ *    inside its own scene (geom_body_idx is read when the groups are
+ *    built).  Which contacts a step that overflowed a cap keeps may differ;
+ *  - giant_island_contacts: in the coloured mode, islands of more contacts
+ *    than this are coloured and swept by the whole GPU (one cooperative
+ *    launch, a grid barrier between colours) instead of by one warp; 0 =
+ *    4,096.  Their colouring differs from the one-warp greedy colouring
+ *    (it is computed in parallel), so this setting changes the coloured
+ *    mode's results, never the sequential and wavefront modes'.
  * get returns the values in use (defaults resolved).  set applies them to
- * the following steps: a handle with scenes set rebuilds its solver bundles
- * and broadphase tiles (as seevr_physics_set_scenes does), and a captured
- * frame graph is recaptured at the next graph step. */
+ * the following steps: a handle with scenes set rebuilds its solver bundles,
+ * broadphase tiles and scene groups (as seevr_physics_set_scenes does), and
+ * a captured frame graph is recaptured at the next graph step. */
 typedef struct seevr_tuning {
     uint32_t bundle_bodies;
     uint32_t narrow_blocks_per_sm;
     uint32_t broad_tile_rows;
-    uint32_t reserved; /* 0 */
+    uint32_t scene_groups;
+    uint32_t giant_island_contacts;
 } seevr_tuning;
 seevr_status seevr_physics_get_tuning(seevr_physics* h, seevr_tuning* out);
 seevr_status seevr_physics_set_tuning(seevr_physics* h, const seevr_tuning* t);
+
+/* No counterpart in the reference, whose waits cannot fail.  Every bounded
+ * device-side wait of this handle (the decoupled look-back of its scans and
+ * radix sorts) gives up after `polls` polls of a tile that has not yet
+ * published, raises the timeout bit and lets the step finish; the step then
+ * returns SEEVR_ERR_TIMEOUT (seevr_physics_step) or reports bit 2 in
+ * seevr_physics_read_flags (async steps; the bit stays set, and the stages
+ * that consume scan or sort results stay skipped, until it is read).  A step
+ * that timed out has advanced only the body state (gravity, damping,
+ * integration) and wrote nothing outside its buffers; its pairs and contacts
+ * are unspecified.  The default, 4,194,304 polls, is reached only if the GPU
+ * stops scheduling a tile.  Small values exist so that tests can exercise
+ * the error path without hanging or faulting the GPU (0: give up at the
+ * first poll of an unpublished tile).  A captured frame graph is recaptured
+ * at the next graph step. */
+seevr_status seevr_physics_set_wait_limit(seevr_physics* h, uint32_t polls);
 
 /* Copy the mutable body state between host memory and the bound device
  * buffers (pos, quat, vel, omega of num_bodies bodies), ordered on the
@@ -276,7 +313,11 @@ void seevr_physics_destroy(seevr_physics* h);
  *    values return SEEVR_ERR_INVALID_ARGUMENT with a message.
  *  - All-pairs broadphase, sequential or wavefront solver.
  *  - Ordered on `stream` (a cudaStream_t, NULL = default stream) on the
- *    current device; synchronous unless params->flags has NO_SYNC.
+ *    current device; synchronous unless params->flags has NO_SYNC.  To
+ *    enqueue the step while `stream` is being captured, set NO_SYNC: the
+ *    synchronous mode reads the status word back and waits, which capture
+ *    forbids.  With NO_SYNC no status is reported: capacity overflow and
+ *    timeouts are not returned, and the next call clears the status word.
  *  - The first call on a device looks up the scratch array's device address
  *    (cudaGetSymbolAddress) and configures the solver and broadphase
  *    kernels; make that first call before any stream capture.

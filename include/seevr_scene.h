@@ -127,11 +127,26 @@ void seevr_scene_gen_large(seevr_scene* s, uint64_t seed, uint32_t n_bodies,
 void seevr_scene_gen_batch(seevr_scene* s, uint32_t num_scenes,
                            uint32_t min_bodies, uint32_t max_bodies,
                            uint32_t segments, uint64_t seed_base);
+/* The scenes of seevr_scene_gen_batch whose seeds are listed: seeds
+ * {k0, k1, ...} give scenes k0, k1, ... of the batch generated with
+ * seed_base 0 (each scene has its own stream, seeded with its number). */
+void seevr_scene_gen_batch_seeds(seevr_scene* s, const uint64_t* seeds,
+                                 uint32_t num_scenes, uint32_t min_bodies,
+                                 uint32_t max_bodies, uint32_t segments);
 void seevr_scene_gen_rollout(seevr_scene* s, uint32_t num_scenes,
                              uint32_t bodies, uint32_t segments,
                              uint64_t seed_base);
 void seevr_scene_gen_towers(seevr_scene* s, uint64_t seed, uint32_t towers,
                             uint32_t height, float spacing);
+/* Towers of unit boxes (half-extent 0.5) on a static ground: `towers`
+ * stacks of `height` boxes on a square grid `spacing` apart, x and z
+ * jittered N(0, 0.01) m, friction 0.6, no restitution.  Each box sinks
+ * `overlap` metres into the one below (the lowest into the ground), so every
+ * stack contact exists from the first substep; overlap 0 gives boxes that
+ * just touch (seevr_scene_gen_towers), whose contacts appear only as the
+ * boxes below settle. */
+void seevr_scene_gen_towers_stacked(seevr_scene* s, uint64_t seed, uint32_t towers,
+                                    uint32_t height, float spacing, float overlap);
 
 /* Views of the staging arrays (valid until the next add/gen call). */
 void* seevr_scene_array(seevr_scene* s, int array_id);

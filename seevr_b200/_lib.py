@@ -27,7 +27,8 @@ SOLVER_SEQUENTIAL, SOLVER_WAVEFRONT, SOLVER_COLORED = 0, 1, 2
 FLAG_NO_SYNC, FLAG_CUDA_GRAPH, FLAG_SKIP_RENDER_VERTS = 1, 2, 4
 # bits of seevr_physics_read_flags
 DEVICE_FLAG_PAIR_OVERFLOW, DEVICE_FLAG_CONTACT_OVERFLOW, DEVICE_FLAG_TIMEOUT, \
-    DEVICE_FLAG_SOLVER_GLOBAL = 1, 2, 4, 8
+    DEVICE_FLAG_SOLVER_GLOBAL, DEVICE_FLAG_CHECK_FAILED, DEVICE_FLAG_GIANT_ISLANDS = \
+    1, 2, 4, 8, 16, 32
 
 # binding indices (physics.comp:16-57 + extension 30)
 (B_BODY_POS, B_BODY_QUAT, B_BODY_VEL, B_BODY_OMEGA, B_BODY_INV_MASS, B_BODY_INV_INERTIA,
@@ -75,7 +76,8 @@ class Profile(C.Structure):
 class Tuning(C.Structure):
     """seevr_tuning: launch shapes of the batched step (results unchanged)."""
     _fields_ = [("bundle_bodies", C.c_uint32), ("narrow_blocks_per_sm", C.c_uint32),
-                ("broad_tile_rows", C.c_uint32), ("reserved", C.c_uint32)]
+                ("broad_tile_rows", C.c_uint32), ("scene_groups", C.c_uint32),
+                ("giant_island_contacts", C.c_uint32)]
 
 
 class AdjointGrads(C.Structure):
@@ -121,6 +123,7 @@ def _load():
         "seevr_physics_read_flags": (I, [P, UP]),
         "seevr_physics_get_tuning": (I, [P, C.POINTER(Tuning)]),
         "seevr_physics_set_tuning": (I, [P, C.POINTER(Tuning)]),
+        "seevr_physics_set_wait_limit": (I, [P, U32]),
         "seevr_physics_upload_state": (I, [P, U32, P, P, P, P]),
         "seevr_physics_download_state": (I, [P, U32, P, P, P, P]),
         "seevr_physics_destroy": (None, [P]),
@@ -154,6 +157,8 @@ def _load():
         "seevr_scene_gen_batch": (None, [P, U32, U32, U32, U32, U64]),
         "seevr_scene_gen_rollout": (None, [P, U32, U32, U32, U64]),
         "seevr_scene_gen_towers": (None, [P, U64, U32, U32, F]),
+        "seevr_scene_gen_towers_stacked": (None, [P, U64, U32, U32, F, F]),
+        "seevr_scene_gen_batch_seeds": (None, [P, C.POINTER(C.c_uint64), U32, U32, U32, U32]),
         "seevr_scene_array": (P, [P, I]),
         "seevr_scene_count": (U64, [P, I]),
         "seevr_scene_save": (I, [P, C.c_char_p]),

@@ -503,6 +503,7 @@ __device__ __forceinline__ void fix_addR(double* f, const dm3& g) {
 
 __global__ void __launch_bounds__(kAdjWarps * 32)
     k_adjoint(World w, Consts k, Scratch s, AdjScratch a, Grads g, float dt) {
+    if (halted(w.status)) return;  // the recomputed contacts are not valid
     const unsigned full = 0xFFFFFFFFu;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t bundle = blockIdx.x * kAdjWarps + (threadIdx.x >> 5);

@@ -39,6 +39,7 @@ template <bool kWrite>
 __global__ void __launch_bounds__(256) k_broad_n2(World w, const uint32_t* __restrict__ row_off,
                                                   uint32_t* __restrict__ row_count,
                                                   uint32_t* __restrict__ mask, uint32_t stride) {
+    if (kWrite && halted(w.status)) return;  // row offsets from a scan that gave up
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (i >= w.nb) return;
@@ -92,6 +93,7 @@ __global__ void __launch_bounds__(kTileThreads)
                  const uint32_t* __restrict__ row_off, uint32_t* __restrict__ row_count,
                  uint32_t* __restrict__ mask, uint32_t stride) {
     extern __shared__ float sm[];
+    if (kWrite && halted(w.status)) return;  // row offsets from a scan that gave up
     uint32_t scene, slice, slices;
     if (tiles) {
         const uint2 t = tiles[blockIdx.x];

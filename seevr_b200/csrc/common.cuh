@@ -16,10 +16,25 @@ enum : uint32_t {
     kFlagContactOverflow = 1u << 1,
     kFlagTimeout = 1u << 2,
     kFlagSolverGlobal = 1u << 3,
+    kFlagCheckFailed = 1u << 4,  // bounds-check mode found a bad index (check.cu)
+    kFlagGiantIslands = 1u << 5,  // islands were solved grid-wide (giant.cu)
 };
 
-// Bounded spin for decoupled look-back: after this many polls a wait gives
-// up, raises kFlagTimeout and proceeds, so no kernel can hang.
+// Checks of the bounds-check mode; the failing one is kept in status[2]
+// and its body, pair or contact index in status[3].
+enum : uint32_t {
+    kCheckHullRange = 1,
+    kCheckRenderRange = 2,
+    kCheckLookup = 3,
+    kCheckGeomBody = 4,
+    kCheckPairs = 5,
+    kCheckContacts = 6,
+};
+
+// Bounded spin for decoupled look-back: after this many polls of an
+// unpublished tile a wait gives up, raises kFlagTimeout and proceeds, so no
+// kernel can hang.  The default of Scratch::wait_limit (per handle,
+// seevr_physics_set_wait_limit).
 constexpr uint32_t kSpinLimit = 1u << 22;
 
 constexpr uint32_t kNone = 0xFFFFFFFFu;
@@ -47,6 +62,9 @@ struct World {
     uint32_t* c_b;
     float* lambda;
     uint32_t* counters;
+    // library status word (Scratch::status): kernels that consume scan or
+    // sort results read its timeout bit first (timed_out)
+    uint32_t* status;
     float* aabb_min;
     float* aabb_max;
     uint32_t* pairs;
@@ -70,6 +88,23 @@ struct Consts {
     uint32_t pgs_iterations, mpr_iterations, discover_trials;
 };
 
+// Grid-wide coloured solve of giant islands (giant.cu); list == NULL: not
+// allocated.  Indexed by contact position in island order (i) or body.
+struct GiantScratch {
+    uint32_t* list;    // [max_contacts] positions of the giant islands' contacts
+    uint32_t* colour;  // [max_contacts] colour per position
+    uint32_t* order;   // [max_contacts] positions grouped by colour
+    uint64_t* used;    // [max_bodies] colours taken at each body (bit mask)
+    uint64_t* prio;    // [max_bodies] highest priority of an uncoloured contact
+    uint32_t* hist;    // [kGiantMaxColours] contacts per colour, then cursors
+    uint32_t* first;   // [kGiantMaxColours + 1] first slot of each colour
+    uint32_t* ctr;     // [8] barrier, counts
+};
+constexpr uint32_t kGiantMaxColours = 64 + 1024;
+// Islands of more contacts than this are solved grid-wide in the coloured
+// mode (launch_solver_giant).
+constexpr uint32_t kGiantContacts = 4096;
+
 // Island solver work arrays (islands.cu); parent == NULL: not allocated.
 struct IslandScratch {
     uint32_t* parent;       // [max_bodies] union-find links
@@ -86,6 +121,7 @@ struct IslandScratch {
     uint32_t* lvl;          // [2 * max_contacts + 2] level boundaries per island
     uint32_t* sort_hist;    // [4 * 256]
     uint32_t* sort_status;  // look-back words of the sort
+    GiantScratch giant;
 };
 
 // Library-owned scratch (device).
@@ -98,7 +134,10 @@ struct Scratch {
     float4* pair_res0;      // [max_pairs] contact point xyz, depth
     float4* pair_res1;      // [max_pairs] normal xyz, found flag
     uint32_t* pair_flag;    // [max_pairs] 1 if the pair makes a contact
-    uint32_t* pair_coff;    // [max_pairs] exclusive scan of pair_flag
+    uint32_t* pair_coff;    // [max_pairs] exclusive scan of pair_flag (before it:
+                            // the narrowphase's pair order)
+    uint32_t* pair_class;   // [8] pairs per support-path class and cursors
+                            // (NULL: pairs taken in index order)
     // solver, per contact
     float* s_ra;            // [max_contacts*3]
     float* s_rb;            // [max_contacts*3]
@@ -126,11 +165,35 @@ struct Scratch {
     // (NULL: every scene gets the slices of the largest)
     uint2* bp_tiles;
     uint32_t bp_ntiles;
+    // polls of an unpublished tile before a look-back gives up (kSpinLimit)
+    uint32_t wait_limit;
+    // coloured mode: islands above this many contacts are solved grid-wide
+    // (0: kGiantContacts)
+    uint32_t giant_min;
     // launch shapes (seevr_physics_set_tuning; 0 = the built-in default)
     uint32_t narrow_blocks;  // persistent narrowphase grid, in blocks
+    uint32_t narrow_per_sm;  // of which per SM (selects the register budget)
     uint32_t bp_tile_rows;   // all-pairs broadphase rows per block
     IslandScratch isl;
 };
+
+// True once a bounded wait of the running step gave up or a bounds check
+// failed.  Every kernel that consumes a scan's offsets or a sort's order
+// returns at once when it is set: offsets from a look-back that gave up are
+// too small, and the lists they would index (pairs, contacts, bundle
+// ranges, tree nodes) are then neither complete nor ordered.  A step that
+// timed out therefore only advances the body state and stays within every
+// buffer.  The bits stay set until the host reads and clears the status
+// word.
+__device__ __forceinline__ bool halted(const uint32_t* status) {
+    return (*reinterpret_cast<const volatile uint32_t*>(status) &
+            (kFlagTimeout | kFlagCheckFailed)) != 0u;
+}
+// True once a bounds check failed: then the per-body stages stop as well,
+// since the inputs they index are not valid.
+__device__ __forceinline__ bool check_failed(const uint32_t* status) {
+    return (*reinterpret_cast<const volatile uint32_t*>(status) & kFlagCheckFailed) != 0u;
+}
 
 // ---- launchers (one translation unit each) ------------------------------
 enum BodyStageFlags : uint32_t {
@@ -180,8 +243,41 @@ int launch_solver(const World& w, const Consts& k, const Scratch& s, uint32_t mo
 // sequential, 1 wavefront, 2 coloured.
 int launch_solver_islands(const World& w, const Consts& k, const Scratch& s, uint32_t mode,
                           float dt, cudaStream_t st);
+// Grid-wide coloured solve of the islands above kGiantContacts contacts (a
+// cooperative launch); returns 0 without launching when not available.
+int launch_solver_giant(const World& w, const Consts& k, const Scratch& s, float dt,
+                        cudaStream_t st);
 // Scenes above this many bodies are solved by islands (when allocated).
 constexpr uint32_t kWarpMaxBodies = 1024;
 constexpr uint32_t kRecWords = 8;  // float4 words of a warp-solver contact record
+
+// One scene group's outputs, merged into the bound buffers at frame end
+// (physics.cu): its counters and status word, its pair and contact lists in
+// group-local body and geom indices, and its first body.
+struct GroupOut {
+    const uint32_t* counters;
+    uint32_t* status;
+    const uint32_t* pairs;
+    const float* c_pos;
+    const float* c_normal;
+    const float* c_pen;
+    const uint32_t* c_a;
+    const uint32_t* c_b;
+    const float* lambda;
+    uint32_t b0;
+};
+constexpr uint32_t kMaxGroups = 8;
+struct GroupTable {
+    GroupOut g[kMaxGroups];
+    uint32_t n;
+};
+
+// Bounds-check mode (check.cu): validation of the caller's index arrays
+// (lut_words: entries of the support-lookup binding) and of each substep's
+// pair and contact lists; check_name describes a status[2] code.
+int launch_check_inputs(const World& w, uint32_t lut_words, cudaStream_t st);
+int launch_check_pairs(const World& w, cudaStream_t st);
+int launch_check_contacts(const World& w, cudaStream_t st);
+const char* check_name(uint32_t code);
 
 }  // namespace seevr

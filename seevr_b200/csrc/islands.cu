@@ -51,7 +51,10 @@ __device__ __forceinline__ uint32_t find_root(uint32_t* parent, uint32_t x) {
     return cur;
 }
 
+// Every island kernel runs on contacts from the narrowphase's scan (and the
+// later ones on the island sort): none runs after a wait gave up.
 __global__ void k_island_prep(World w, Scratch s) {
+    if (halted(w.status)) return;
     for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < w.nb; b += gridDim.x * blockDim.x) {
         s.isl.parent[b] = b;
         s.s_last[b] = 0;
@@ -62,6 +65,7 @@ __global__ void k_island_prep(World w, Scratch s) {
 // Hook the roots of a contact's two dynamic bodies: a failed CAS returns a
 // smaller root, so every retry makes progress.
 __global__ void k_island_union(World w, Scratch s) {
+    if (halted(w.status)) return;
     const uint32_t nc = min(w.counters[1], w.max_contacts);
     for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
         const uint32_t a = w.geom_body[w.c_a[c]], b = w.geom_body[w.c_b[c]];
@@ -82,6 +86,7 @@ __global__ void k_island_union(World w, Scratch s) {
 }
 
 __global__ void k_island_keys(World w, Scratch s) {
+    if (halted(w.status)) return;
     const uint32_t nc = min(w.counters[1], w.max_contacts);
     for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < w.max_contacts;
          c += gridDim.x * blockDim.x) {
@@ -97,6 +102,7 @@ __global__ void k_island_keys(World w, Scratch s) {
 }
 
 __global__ void k_island_heads(World w, Scratch s) {
+    if (halted(w.status)) return;
     const uint32_t* k = s.isl.keys_out;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < w.max_contacts;
          i += gridDim.x * blockDim.x)
@@ -104,6 +110,7 @@ __global__ void k_island_heads(World w, Scratch s) {
 }
 
 __global__ void k_island_starts(World w, Scratch s) {
+    if (halted(w.status)) return;
     const uint32_t* k = s.isl.keys_out;
     const uint32_t n = w.max_contacts;
     const uint32_t count = *s.isl.count;
@@ -117,7 +124,8 @@ __global__ void k_island_starts(World w, Scratch s) {
 // Warp per island (persistent).  Positions p in [start, start+1) index the
 // island's contacts in index order (perm[p] = contact).
 __global__ void __launch_bounds__(kIslandThreads)
-    k_solver_island(World w, Consts k, Scratch s, uint32_t mode, float dt) {
+    k_solver_island(World w, Consts k, Scratch s, uint32_t mode, float dt, uint32_t giant) {
+    if (halted(w.status)) return;
     const unsigned full = 0xFFFFFFFFu;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -127,6 +135,7 @@ __global__ void __launch_bounds__(kIslandThreads)
     uint32_t* last = s.s_last;
     for (uint32_t isl = gwarp; isl < count; isl += nwarps) {
         const uint32_t p0 = s.isl.start[isl], p1 = s.isl.start[isl + 1];
+        if (p1 - p0 > giant) continue;  // solved grid-wide (giant.cu)
         for (uint32_t i = p0 + lane; i < p1; i += 32) {
             const uint32_t c = perm[i];
             s.s_ab[size_t(i) * 2] = w.geom_body[w.c_a[c]];
@@ -284,6 +293,7 @@ int launch_solver_islands(const World& w, const Consts& k, const Scratch& s, uin
     LbvhScratch ls{};
     ls.hist = s.isl.sort_hist;
     ls.status = s.isl.sort_status;
+    ls.wait_limit = s.wait_limit;
     int n = 3 + lbvh_sort(s.isl.keys_in, s.isl.vals_in, s.isl.keys_tmp, s.isl.vals_tmp,
                           s.isl.keys_out, s.isl.perm, w.max_contacts, ls, &s.status[0], st);
     k_island_heads<<<ncb, 256, 0, st>>>(w, s);
@@ -298,8 +308,12 @@ int launch_solver_islands(const World& w, const Consts& k, const Scratch& s, uin
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    k_solver_island<<<uint32_t(sms) * uint32_t(per_sm), kIslandThreads, 0, st>>>(w, k, s, mode, dt);
-    return n + 2;
+    // coloured mode: islands above kGiantContacts contacts are solved by the
+    // whole grid, the others by a warp each
+    const int giant = mode == 2 ? launch_solver_giant(w, k, s, dt, st) : 0;
+    k_solver_island<<<uint32_t(sms) * uint32_t(per_sm), kIslandThreads, 0, st>>>(
+        w, k, s, mode, dt, giant ? (s.giant_min ? s.giant_min : kGiantContacts) : 0xFFFFFFFFu);
+    return n + 2 + giant;
 }
 
 }  // namespace seevr

@@ -181,7 +181,7 @@ __global__ void __launch_bounds__(kSortThreads)
     k_sort_onesweep(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
                     uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, uint32_t n,
                     uint32_t shift, const uint32_t* __restrict__ bin_start, uint32_t* status,
-                    uint32_t* err) {
+                    uint32_t* err, uint32_t wait_limit) {
     __shared__ uint32_t s_tile;
     __shared__ uint32_t s_warp_hist[kSortWarps][kRadix];
     __shared__ uint32_t s_bin_off[kRadix];
@@ -244,7 +244,7 @@ __global__ void __launch_bounds__(kSortThreads)
                 const uint32_t s = *reinterpret_cast<volatile uint32_t*>(&st[size_t(p) * kRadix + d]);
                 const uint32_t f = s >> 30;
                 if (f == 0u) {
-                    if (++spins > kSpinLimit) {
+                    if (++spins > wait_limit) {
                         atomicOr(err, kFlagTimeout);
                         break;
                     }
@@ -281,7 +281,8 @@ __device__ __forceinline__ int delta(const uint32_t* m, int i, int j, int n) {
 
 __global__ void k_karras(const uint32_t* __restrict__ m, uint32_t n, uint32_t* __restrict__ left,
                          uint32_t* __restrict__ right, uint32_t* __restrict__ parent,
-                         uint32_t* __restrict__ count) {
+                         uint32_t* __restrict__ count, const uint32_t* err) {
+    if (halted(err)) return;  // the sort gave up: the keys are not ordered
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) {
         left[n - 1 + i] = i;
@@ -323,7 +324,8 @@ __global__ void k_karras(const uint32_t* __restrict__ m, uint32_t n, uint32_t* _
 __global__ void k_leaves_bodies(const float* __restrict__ aabb_min, const float* __restrict__ aabb_max,
                                 const uint32_t* __restrict__ sorted_vals, uint32_t n,
                                 float* __restrict__ node_min, float* __restrict__ node_max,
-                                uint32_t* __restrict__ flags) {
+                                uint32_t* __restrict__ flags, const uint32_t* err) {
+    if (halted(err)) return;  // slots of the sorted order may be unwritten
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i + 1 < n) flags[i] = 0;
     if (i >= n) return;
@@ -335,7 +337,9 @@ __global__ void k_leaves_bodies(const float* __restrict__ aabb_min, const float*
 __global__ void k_leaves_tris(const float* __restrict__ verts, const uint32_t* __restrict__ idx,
                               const uint32_t* __restrict__ sorted_vals, uint32_t n,
                               float* __restrict__ node_min, float* __restrict__ node_max,
-                              uint32_t* __restrict__ prim_idx, uint32_t* __restrict__ flags) {
+                              uint32_t* __restrict__ prim_idx, uint32_t* __restrict__ flags,
+                              const uint32_t* err) {
+    if (halted(err)) return;  // slots of the sorted order may be unwritten
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i + 1 < n) flags[i] = 0;
     if (i >= n) return;
@@ -350,7 +354,8 @@ __global__ void k_leaves_tris(const float* __restrict__ verts, const uint32_t* _
 // Bottom-up: the second child to arrive at a node computes its box.
 __global__ void k_refit(uint32_t n, const uint32_t* __restrict__ left,
                         const uint32_t* __restrict__ right, const uint32_t* __restrict__ parent,
-                        float* node_min, float* node_max, uint32_t* flags) {
+                        float* node_min, float* node_max, uint32_t* flags, const uint32_t* err) {
+    if (halted(err)) return;  // no valid hierarchy to refit
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n || n < 2) return;
     uint32_t p = parent[n - 1 + i];
@@ -410,6 +415,7 @@ __device__ __forceinline__ void traverse(const World& w, const LbvhView& t, uint
 // listed here.
 __global__ void k_lbvh_count(World w, LbvhView t, uint32_t* __restrict__ row_count, uint32_t* err,
                              uint32_t* static_list, uint32_t* static_count) {
+    if (halted(err)) return;  // the tree was not built
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= w.nb) return;
     if (w.inv_mass[i] <= 0.0f) {
@@ -431,6 +437,7 @@ __global__ void __launch_bounds__(256)
     k_lbvh_static_rows(World w, LbvhView t, uint32_t* row_count, const uint32_t* row_off,
                        const uint32_t* static_list, const uint32_t* static_count, uint32_t* bfs) {
     __shared__ uint32_t sh_next, sh_found, sh_cur;
+    if (halted(w.status)) return;  // the tree (or the row offsets) are not valid
     const uint32_t n = w.nb;
     if (n < 2) return;
     uint32_t* fa = bfs + size_t(blockIdx.x) * 3 * 2 * n;
@@ -496,6 +503,7 @@ __global__ void __launch_bounds__(256)
 // chunks of up to kRowBuf smallest remaining j, one traversal per chunk.
 __global__ void k_lbvh_write(World w, LbvhView t, const uint32_t* __restrict__ row_count,
                              const uint32_t* __restrict__ row_off, uint32_t* err) {
+    if (halted(err)) return;  // the tree or the row offsets are not valid
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= w.nb || w.inv_mass[i] <= 0.0f) return;  // static rows: k_lbvh_static_rows
     uint32_t remaining = row_count[i];
@@ -548,7 +556,8 @@ int lbvh_sort(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_t
         uint32_t* vo = (p % 2 == 0) ? vals_tmp : vals_out;
         cudaMemsetAsync(s.status, 0, sizeof(uint32_t) * (1 + size_t(tiles) * kRadix), st);
         k_sort_onesweep<<<tiles ? tiles : 1, kSortThreads, 0, st>>>(ki, vi, ko, vo, n, 8u * p,
-                                                                   s.hist + p * kRadix, s.status, err);
+                                                                   s.hist + p * kRadix, s.status, err,
+                                                                   s.wait_limit);
         ki = ko;
         vi = vo;
         ++launches;
@@ -568,11 +577,11 @@ int lbvh_build_bodies(const World& w, const LbvhScratch& s, uint32_t* err, cudaS
     int k = 2 + lbvh_sort(s.keys_a, s.vals_a, s.keys_b, s.vals_b, s.keys_sorted, s.vals_sorted, n,
                           s, err, st);
     k_karras<<<blocks_for(n, 256), 256, 0, st>>>(s.keys_sorted, n, s.left, s.right, s.parent,
-                                                 nullptr);
+                                                 nullptr, err);
     k_leaves_bodies<<<blocks_for(n, 256), 256, 0, st>>>(w.aabb_min, w.aabb_max, s.vals_sorted, n,
-                                                        s.node_min, s.node_max, s.flags);
+                                                        s.node_min, s.node_max, s.flags, err);
     k_refit<<<blocks_for(n, 256), 256, 0, st>>>(n, s.left, s.right, s.parent, s.node_min,
-                                                s.node_max, s.flags);
+                                                s.node_max, s.flags, err);
     return k + 3;
 }
 
@@ -605,11 +614,12 @@ int lbvh_build_triangles(const float* verts, const uint32_t* idx, uint32_t n, co
                                                  o.scene_bounds);
     int k = 2 + lbvh_sort(s.keys_a, s.vals_a, s.keys_b, s.vals_b, o.morton, o.sort_idx, n, s, err,
                           st);
-    k_karras<<<blocks_for(n, 256), 256, 0, st>>>(o.morton, n, o.left, o.right, o.parent, o.count);
+    k_karras<<<blocks_for(n, 256), 256, 0, st>>>(o.morton, n, o.left, o.right, o.parent, o.count,
+                                                 err);
     k_leaves_tris<<<blocks_for(n, 256), 256, 0, st>>>(verts, idx, o.sort_idx, n, o.node_min,
-                                                      o.node_max, o.prim_idx, o.flags);
+                                                      o.node_max, o.prim_idx, o.flags, err);
     k_refit<<<blocks_for(n, 256), 256, 0, st>>>(n, o.left, o.right, o.parent, o.node_min,
-                                                o.node_max, o.flags);
+                                                o.node_max, o.flags, err);
     return k + 3;
 }
 

@@ -29,6 +29,8 @@ struct LbvhScratch {
     uint32_t* static_list;   // [cap]
     uint32_t* static_count;  // [1]
     uint32_t* bfs;
+    // polls of an unpublished sort tile before a look-back gives up
+    uint32_t wait_limit = kSpinLimit;
 };
 
 // Blocks that traverse static bodies' rows.

@@ -25,20 +25,38 @@
 
 namespace seevr {
 
+constexpr uint32_t kNarrowThreads = 128;
+constexpr uint32_t kNarrowThreadsW = kNarrowThreads;  // witness slots per thread row
+
+// A pair's two shapes: hull range and lookup offset in registers; rotation
+// and position in shared memory (Pose), read at each support call, so that
+// the state a lane carries from step to step fits its register budget.
 struct Shape {
-    m3 R;
-    f3 p;
     uint32_t vs, vc, lk;
 };
 
-__device__ __forceinline__ Shape load_shape(const World& w, uint32_t b) {
-    Shape s;
-    s.R = quat_to_mat(w.quat, b);
-    s.p = ld3(w.pos, b);
-    s.vs = w.hull_range[size_t(b) * 2];
-    s.vc = w.hull_range[size_t(b) * 2 + 1];
-    s.lk = w.sup_off[b];
-    return s;
+struct Pose {
+    float (*q)[12][kNarrowThreadsW];  // [shape][R by columns, p][thread]
+    uint32_t t;
+    __device__ __forceinline__ void put(uint32_t i, const m3& R, f3 p) const {
+        q[i][0][t] = R.c0.x; q[i][1][t] = R.c0.y; q[i][2][t] = R.c0.z;
+        q[i][3][t] = R.c1.x; q[i][4][t] = R.c1.y; q[i][5][t] = R.c1.z;
+        q[i][6][t] = R.c2.x; q[i][7][t] = R.c2.y; q[i][8][t] = R.c2.z;
+        q[i][9][t] = p.x; q[i][10][t] = p.y; q[i][11][t] = p.z;
+    }
+    __device__ __forceinline__ m3 R(uint32_t i) const {
+        m3 m;
+        m.c0 = mk(q[i][0][t], q[i][1][t], q[i][2][t]);
+        m.c1 = mk(q[i][3][t], q[i][4][t], q[i][5][t]);
+        m.c2 = mk(q[i][6][t], q[i][7][t], q[i][8][t]);
+        return m;
+    }
+    __device__ __forceinline__ f3 p(uint32_t i) const { return mk(q[i][9][t], q[i][10][t], q[i][11][t]); }
+};
+
+__device__ __forceinline__ Shape load_shape(const World& w, uint32_t b, const Pose& P, uint32_t i) {
+    P.put(i, quat_to_mat(w.quat, b), ld3(w.pos, b));
+    return Shape{w.hull_range[size_t(b) * 2], w.hull_range[size_t(b) * 2 + 1], w.sup_off[b]};
 }
 
 // support (physics.comp:107-162).  Both paths of the reference visit a list
@@ -46,8 +64,10 @@ __device__ __forceinline__ Shape load_shape(const World& w, uint32_t b) {
 // hull vertices when lk == 0 (brute force), else for each of the 3 axes the
 // two lookup bins around the direction's angle.  One loop over candidates
 // serves both, so lanes of a warp holding boxes and spheres share it.
-__device__ __forceinline__ f3 support(const World& w, const Shape& s, f3 d, uint32_t& chosen) {
-    const f3 ld = mulT(s.R, d);
+__device__ __forceinline__ f3 support(const World& w, const Shape& s, const Pose& P, uint32_t i,
+                                      f3 d, uint32_t& chosen) {
+    const m3 R = P.R(i);
+    const f3 ld = mulT(R, d);
     const bool lut = s.lk != 0;
     float a0 = 0.f, a1 = 0.f, a2 = 0.f;
     if (lut) {
@@ -80,15 +100,57 @@ __device__ __forceinline__ f3 support(const World& w, const Shape& s, f3 d, uint
             chosen = idx;
         }
     }
-    return add(s.p, mul(s.R, bv));
+    return add(P.p(i), mul(R, bv));
 }
 
-// Minkowski support point and the supporting points on A and B
-// (mink_support_pts, physics.comp:165-169)
+// A Minkowski support point (mink_support_pts, physics.comp:165-169): its
+// value v = sa - sb stays in registers, while the supporting points sa, sb
+// (and, for the adjoint's tape, the hull-relative indices of the supporting
+// vertices) are kept in one of four shared-memory slots per lane, named by
+// `slot`.  The portal's three points and the step's fresh point always hold
+// four different slots, so a point entering the portal frees the slot of
+// the one it replaces.  Only the contact point (find_pos) and the segment
+// case read sa and sb, so keeping them out of registers costs one store per
+// support call and lets the lane's state fit the register budget of seven
+// resident blocks per SM.
 struct Mink {
-    f3 v, sa, sb;
-    uint32_t ia, ib;  // hull-relative indices of the supporting vertices
+    f3 v;
+    uint32_t slot;
 };
+
+template <bool kTape>
+struct Witness {
+    static constexpr uint32_t kWords = kTape ? 8 : 6;  // sa xyz, sb xyz (, ia, ib)
+    float (*w)[kWords][kNarrowThreadsW];               // [slot][word][thread]
+    uint32_t t;
+    __device__ __forceinline__ void put(uint32_t slot, f3 sa, f3 sb, uint32_t ia, uint32_t ib) const {
+        w[slot][0][t] = sa.x; w[slot][1][t] = sa.y; w[slot][2][t] = sa.z;
+        w[slot][3][t] = sb.x; w[slot][4][t] = sb.y; w[slot][5][t] = sb.z;
+        if (kTape) {
+            w[slot][kWords - 2][t] = __uint_as_float(ia);
+            w[slot][kWords - 1][t] = __uint_as_float(ib);
+        }
+    }
+    __device__ __forceinline__ f3 sa(uint32_t slot) const {
+        return mk(w[slot][0][t], w[slot][1][t], w[slot][2][t]);
+    }
+    __device__ __forceinline__ f3 sb(uint32_t slot) const {
+        return mk(w[slot][3][t], w[slot][4][t], w[slot][5][t]);
+    }
+    __device__ __forceinline__ uint32_t ia(uint32_t slot) const {
+        return __float_as_uint(w[slot][kWords - 2][t]);
+    }
+    __device__ __forceinline__ uint32_t ib(uint32_t slot) const {
+        return __float_as_uint(w[slot][kWords - 1][t]);
+    }
+};
+
+// dst takes the fresh point m (held in slot `free`): dst's old slot becomes
+// the free one.
+__device__ __forceinline__ void take(Mink& dst, const Mink& m, uint32_t& free) {
+    free = dst.slot;
+    dst = m;
+}
 
 __device__ __forceinline__ f3 portal_dir(f3 v1, f3 v2, f3 v3) {
     return normalize(cross(sub(v2, v1), sub(v3, v1)));
@@ -100,23 +162,25 @@ __device__ __forceinline__ bool reach_tol(const Consts& k, f3 v1, f3 v2, f3 v3, 
 }
 
 // mpr_expand_portal (physics.comp:200-221)
-__device__ __forceinline__ void expand(const f3& v0, Mink& m1, Mink& m2, Mink& m3, const Mink& m4) {
+__device__ __forceinline__ void expand(const f3& v0, Mink& m1, Mink& m2, Mink& m3, const Mink& m4,
+                                       uint32_t& free) {
     const f3 v4v0 = cross(m4.v, v0);
     float d = dot(m1.v, v4v0);
     if (d > 0.0f) {
         d = dot(m2.v, v4v0);
-        if (d > 0.0f) m1 = m4;
-        else m3 = m4;
+        if (d > 0.0f) take(m1, m4, free);
+        else take(m3, m4, free);
     } else {
         d = dot(m3.v, v4v0);
-        if (d > 0.0f) m2 = m4;
-        else m1 = m4;
+        if (d > 0.0f) take(m2, m4, free);
+        else take(m1, m4, free);
     }
 }
 
 // mpr_find_pos (physics.comp:224-247); s0a, s0b are the body positions
+template <bool kTape>
 __device__ f3 find_pos(const Consts& k, f3 v0, f3 s0a, f3 s0b, const Mink& m1, const Mink& m2,
-                       const Mink& m3) {
+                       const Mink& m3, const Witness<kTape>& W) {
     const f3 v1 = m1.v, v2 = m2.v, v3 = m3.v;
     float b0 = dot(cross(v1, v2), v3);
     float b1 = -dot(cross(v0, v2), v3);
@@ -131,8 +195,10 @@ __device__ f3 find_pos(const Consts& k, f3 v0, f3 s0a, f3 s0b, const Mink& m1, c
         b3 = dot(cross(v1, v2), dir);
         sum = b0 + b1 + b2 + b3;
     }
-    const f3 p1 = add(add(add(scale(b0, s0a), scale(b1, m1.sa)), scale(b2, m2.sa)), scale(b3, m3.sa));
-    const f3 p2 = add(add(add(scale(b0, s0b), scale(b1, m1.sb)), scale(b2, m2.sb)), scale(b3, m3.sb));
+    const f3 p1 = add(add(add(scale(b0, s0a), scale(b1, W.sa(m1.slot))), scale(b2, W.sa(m2.slot))),
+                      scale(b3, W.sa(m3.slot)));
+    const f3 p2 = add(add(add(scale(b0, s0b), scale(b1, W.sb(m1.slot))), scale(b2, W.sb(m2.slot))),
+                      scale(b3, W.sb(m3.slot)));
     return scale(0.5f / sum, add(p1, p2));
 }
 
@@ -150,26 +216,32 @@ __device__ __forceinline__ void finish(float4* res0, float4* res1, uint32_t* fla
     }
 }
 
-constexpr uint32_t kNarrowThreads = 128;
-
 // kTape: also record, per pair, which hull vertices support the final
 // portal (tape[2p] = {case, m1.ia, m1.ib, m2.ia}, tape[2p+1] = {m2.ib,
 // m3.ia, m3.ib, 0}; case 1 = penetration portal, 2 = the segment case of
 // physics.comp:267-271), from which the adjoint differentiates the contact.
-template <bool kTape>
-__global__ void __launch_bounds__(kNarrowThreads, kNarrowBlocksPerSm)
+// kMinBlocks: resident blocks per SM the register allocation is capped for
+// (7: 72 registers with a few spilled values; 6: about 80, no spills).
+template <bool kTape, uint32_t kMinBlocks>
+__global__ void __launch_bounds__(kNarrowThreads, kMinBlocks)
     k_narrow(World w, Consts k, float4* __restrict__ res0, float4* __restrict__ res1,
              uint32_t* __restrict__ flag, uint32_t* __restrict__ ticket,
-             uint4* __restrict__ tape) {
+             uint4* __restrict__ tape, const uint32_t* __restrict__ order) {
+    __shared__ float wit[4][Witness<kTape>::kWords][kNarrowThreadsW];
+    __shared__ float pose[2][12][kNarrowThreadsW];
+    if (halted(w.status)) return;  // pairs from a scan that gave up
     const uint32_t np = min(w.counters[0], w.max_pairs);
     const uint32_t lane = threadIdx.x & 31u;
     const unsigned full = 0xFFFFFFFFu;
+    const Witness<kTape> W{wit, threadIdx.x};
+    const Pose P{pose, threadIdx.x};
 
     bool active = false, drained = false;
     uint32_t p = 0, state = kD1, iter = 0;
     Shape A, B;
     f3 v0 = mk(0, 0, 0), dir = mk(0, 0, 0);
-    Mink m1{}, m2{}, m3{};
+    Mink m1{mk(0, 0, 0), 0}, m2{mk(0, 0, 0), 1}, m3{mk(0, 0, 0), 2};
+    uint32_t free = 3;
 
     while (true) {
         // ---- refill idle lanes with the next pairs ----
@@ -184,11 +256,11 @@ __global__ void __launch_bounds__(kNarrowThreads, kNarrowBlocksPerSm)
                 if (!active) {
                     const uint32_t q = base + __popc(need & ((1u << lane) - 1u));
                     if (q < np) {
-                        p = q;
+                        p = order ? order[q] : q;
                         const uint32_t a = w.pairs[size_t(p) * 2], b = w.pairs[size_t(p) * 2 + 1];
-                        A = load_shape(w, a);
-                        B = load_shape(w, b);
-                        v0 = sub(A.p, B.p);  // s0a - s0b (physics.comp:254-258)
+                        A = load_shape(w, a, P, 0);
+                        B = load_shape(w, b, P, 1);
+                        v0 = sub(ld3(w.pos, a), ld3(w.pos, b));  // s0a - s0b (physics.comp:254-258)
                         if (fabsf(v0.x) < k.eps && fabsf(v0.y) < k.eps && fabsf(v0.z) < k.eps)
                             v0.x += 10.0f * k.eps;
                         dir = normalize(neg(v0));
@@ -220,9 +292,14 @@ __global__ void __launch_bounds__(kNarrowThreads, kNarrowBlocksPerSm)
 
         // ---- the one Minkowski support call of the step ----
         Mink m;
-        m.sa = support(w, A, dir, m.ia);
-        m.sb = support(w, B, neg(dir), m.ib);
-        m.v = sub(m.sa, m.sb);
+        {
+            uint32_t ia, ib;
+            const f3 sa = support(w, A, P, 0, dir, ia);
+            const f3 sb = support(w, B, P, 1, neg(dir), ib);
+            m.v = sub(sa, sb);
+            m.slot = free;
+            W.put(free, sa, sb, ia, ib);
+        }
 
         // ---- postlude ----
         switch (state) {
@@ -232,7 +309,7 @@ __global__ void __launch_bounds__(kNarrowThreads, kNarrowBlocksPerSm)
                     active = false;
                     break;
                 }
-                m1 = m;
+                take(m1, m, free);
                 const f3 c = cross(v0, m1.v);
                 if (dot(c, c) < k.eps) {
                     const f3 v1 = m1.v;
@@ -246,10 +323,11 @@ __global__ void __launch_bounds__(kNarrowThreads, kNarrowBlocksPerSm)
                         n = normalize(v1);
                     }
                     if (kTape) {
-                        tape[size_t(p) * 2] = make_uint4(2u, m1.ia, m1.ib, 0u);
+                        tape[size_t(p) * 2] = make_uint4(2u, W.ia(m1.slot), W.ib(m1.slot), 0u);
                         tape[size_t(p) * 2 + 1] = make_uint4(0u, 0u, 0u, 0u);
                     }
-                    finish(res0, res1, flag, p, true, scale(0.5f, add(m1.sa, m1.sb)), n, depth);
+                    finish(res0, res1, flag, p, true,
+                           scale(0.5f, add(W.sa(m1.slot), W.sb(m1.slot))), n, depth);
                     active = false;
                     break;
                 }
@@ -263,7 +341,7 @@ __global__ void __launch_bounds__(kNarrowThreads, kNarrowBlocksPerSm)
                     active = false;
                     break;
                 }
-                m2 = m;
+                take(m2, m, free);
                 dir = normalize(cross(sub(m1.v, v0), sub(m2.v, v0)));
                 if (dot(dir, v0) > 0.0f) {
                     const Mink t = m1;
@@ -287,10 +365,10 @@ __global__ void __launch_bounds__(kNarrowThreads, kNarrowBlocksPerSm)
                 }
                 bool retry = false;
                 if (dot(cross(m1.v, m.v), v0) < -k.eps) {
-                    m2 = m;
+                    take(m2, m, free);
                     retry = true;
                 } else if (dot(cross(m.v, m2.v), v0) < -k.eps) {
-                    m1 = m;
+                    take(m1, m, free);
                     retry = true;
                 }
                 if (retry) {
@@ -301,7 +379,7 @@ __global__ void __launch_bounds__(kNarrowThreads, kNarrowBlocksPerSm)
                     }
                     break;
                 }
-                m3 = m;  // portal found: refine
+                take(m3, m, free);  // portal found: refine
                 iter = 0;
                 state = kR;
                 if (k.mpr_iterations == 0) {  // refine returns 1, penetration finds nothing
@@ -316,7 +394,7 @@ __global__ void __launch_bounds__(kNarrowThreads, kNarrowBlocksPerSm)
                     active = false;
                     break;
                 }
-                expand(v0, m1, m2, m3, m);
+                expand(v0, m1, m2, m3, m, free);
                 if (++iter >= k.mpr_iterations) {  // refine returns 1: go on to penetration
                     iter = 0;
                     state = kP;
@@ -327,17 +405,61 @@ __global__ void __launch_bounds__(kNarrowThreads, kNarrowBlocksPerSm)
                 if (reach_tol(k, m1.v, m2.v, m3.v, m.v, dir) || iter >= k.mpr_iterations - 1) {
                     const float depth = dot(dir, m1.v);
                     if (kTape) {
-                        tape[size_t(p) * 2] = make_uint4(1u, m1.ia, m1.ib, m2.ia);
-                        tape[size_t(p) * 2 + 1] = make_uint4(m2.ib, m3.ia, m3.ib, 0u);
+                        tape[size_t(p) * 2] =
+                            make_uint4(1u, W.ia(m1.slot), W.ib(m1.slot), W.ia(m2.slot));
+                        tape[size_t(p) * 2 + 1] =
+                            make_uint4(W.ib(m2.slot), W.ia(m3.slot), W.ib(m3.slot), 0u);
                     }
-                    finish(res0, res1, flag, p, true, find_pos(k, v0, A.p, B.p, m1, m2, m3), dir,
-                           depth);
+                    finish(res0, res1, flag, p, true,
+                           find_pos(k, v0, P.p(0), P.p(1), m1, m2, m3, W), dir, depth);
                     active = false;
                     break;
                 }
-                expand(v0, m1, m2, m3, m);
+                expand(v0, m1, m2, m3, m, free);
                 ++iter;
                 break;
+            }
+        }
+    }
+}
+
+// ---- pair order by support path ---------------------------------------------
+// A warp's lanes run their pairs' support calls together; a shape with a
+// support lookup (lk != 0) takes three arctangents and six candidates, one
+// without walks all its hull vertices.  Taking the pairs grouped by the two
+// shapes' paths (4 classes) keeps a warp's lanes on one path.  Each pair's
+// result is staged at its own index, so the order changes no result.
+__device__ __forceinline__ uint32_t pair_class(const World& w, uint32_t p) {
+    const uint32_t a = w.pairs[size_t(p) * 2], b = w.pairs[size_t(p) * 2 + 1];
+    return (w.sup_off[a] != 0u ? 2u : 0u) | (w.sup_off[b] != 0u ? 1u : 0u);
+}
+
+// cls[0..3]: pairs per class; cls[4..7]: placement cursors (zeroed before)
+template <bool kScatter>
+__global__ void k_pair_classes(World w, uint32_t* __restrict__ cls, uint32_t* __restrict__ order) {
+    if (halted(w.status)) return;
+    const uint32_t np = min(w.counters[0], w.max_pairs);
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t pre[4] = {0, 0, 0, 0};
+    if (kScatter) {
+        pre[1] = cls[0];
+        pre[2] = pre[1] + cls[1];
+        pre[3] = pre[2] + cls[2];
+    }
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t p0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); p0 < np; p0 += stride) {
+        const uint32_t p = p0 + lane;
+        const uint32_t c = p < np ? pair_class(w, p) : 4u;
+#pragma unroll
+        for (uint32_t k = 0; k < 4; ++k) {
+            const unsigned m = __ballot_sync(0xFFFFFFFFu, c == k);
+            if (!m) continue;
+            const uint32_t leader = __ffs(m) - 1;
+            uint32_t base = 0;
+            if (lane == leader) base = atomicAdd(&cls[kScatter ? 4 + k : k], uint32_t(__popc(m)));
+            if (kScatter) {
+                base = __shfl_sync(0xFFFFFFFFu, base, leader);
+                if (c == k) order[pre[k] + base + __popc(m & ((1u << lane) - 1u))] = p;
             }
         }
     }
@@ -350,6 +472,7 @@ __global__ void k_contact_scatter(World w, const float4* __restrict__ res0,
                                   const uint32_t* __restrict__ coff,
                                   const uint4* __restrict__ pair_tape,
                                   uint4* __restrict__ contact_tape) {
+    if (halted(w.status)) return;  // offsets from a scan that gave up
     const uint32_t np = min(w.counters[0], w.max_pairs);
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < np; p += gridDim.x * blockDim.x) {
         if (!flag[p]) continue;
@@ -382,18 +505,41 @@ int launch_narrowphase_taped(const World& w, const Consts& k, const Scratch& s, 
     cudaMemsetAsync(&s.status[1], 0, sizeof(uint32_t), st);
     const uint32_t blocks = grid_for(w.max_pairs, kNarrowThreads,
                                      s.narrow_blocks ? s.narrow_blocks : 148 * kNarrowBlocksPerSm);
-    if (pair_tape)
-        k_narrow<true><<<blocks, kNarrowThreads, 0, st>>>(w, k, s.pair_res0, s.pair_res1,
-                                                          s.pair_flag, &s.status[1], pair_tape);
-    else
-        k_narrow<false><<<blocks, kNarrowThreads, 0, st>>>(w, k, s.pair_res0, s.pair_res1,
-                                                           s.pair_flag, &s.status[1], nullptr);
+    // the register budget of seven blocks per SM when that many are resident,
+    // else the larger one of six
+    const bool seven = (s.narrow_per_sm ? s.narrow_per_sm : kNarrowBlocksPerSm) >= 7;
+    // pair order by support path, in pair_coff (free until the scan below)
+    const uint32_t* order = nullptr;
+    int n = 3;
+    if (s.pair_class) {
+        cudaMemsetAsync(s.pair_class, 0, 8 * sizeof(uint32_t), st);
+        const uint32_t cb = grid_for(w.max_pairs, 256, 148 * 8);
+        k_pair_classes<false><<<cb, 256, 0, st>>>(w, s.pair_class, nullptr);
+        k_pair_classes<true><<<cb, 256, 0, st>>>(w, s.pair_class, s.pair_coff);
+        order = s.pair_coff;
+        n += 2;
+    }
+    if (pair_tape) {
+        if (seven)
+            k_narrow<true, 7><<<blocks, kNarrowThreads, 0, st>>>(
+                w, k, s.pair_res0, s.pair_res1, s.pair_flag, &s.status[1], pair_tape, order);
+        else
+            k_narrow<true, 6><<<blocks, kNarrowThreads, 0, st>>>(
+                w, k, s.pair_res0, s.pair_res1, s.pair_flag, &s.status[1], pair_tape, order);
+    } else {
+        if (seven)
+            k_narrow<false, 7><<<blocks, kNarrowThreads, 0, st>>>(
+                w, k, s.pair_res0, s.pair_res1, s.pair_flag, &s.status[1], nullptr, order);
+        else
+            k_narrow<false, 6><<<blocks, kNarrowThreads, 0, st>>>(
+                w, k, s.pair_res0, s.pair_res1, s.pair_flag, &s.status[1], nullptr, order);
+    }
     launch_exclusive_scan(s.pair_flag, s.pair_coff, &w.counters[0], w.max_pairs,
                           &w.counters[1], w.max_contacts, kFlagContactOverflow, s, st);
     k_contact_scatter<<<grid_for(w.max_pairs, 256, 148 * 16), 256, 0, st>>>(
         w, s.pair_res0, s.pair_res1, s.pair_flag, s.pair_coff, pair_tape,
         pair_tape ? contact_tape : nullptr);
-    return 3;
+    return n;
 }
 
 int launch_narrowphase(const World& w, const Consts& k, const Scratch& s, cudaStream_t st) {

@@ -10,8 +10,8 @@
 // entry point runs the same kernels on scratch carved from one file-scope
 // device array, so the caller provides only the bound buffers and a stream.
 //
-// The array holds SEEVR_NOALLOC_SCRATCH_BYTES (2.9 MB) on every device that loads the
-// library, until the process exits.  All calls share it: calls whose GPU
+// The array holds SEEVR_NOALLOC_SCRATCH_BYTES (4,965,632 bytes, about 5.0 MB)
+// on every device that loads the library, until the process exits.  All calls share it: calls whose GPU
 // work overlaps (different streams, or different host threads on one
 // device) race on it and must be serialised by the caller.  Each call
 // clears the parts that must start at zero (the status word, scan and
@@ -73,14 +73,19 @@ constexpr int kMaxDevices = 64;
 std::once_flag g_once[kMaxDevices];
 unsigned char* g_dev_ptr[kMaxDevices] = {};
 cudaError_t g_setup_err[kMaxDevices] = {};
+uint32_t g_narrow_blocks[kMaxDevices] = {};
 
 // Once per device, with that device current: the device address of the
-// scratch array, and the solver's shared-memory opt-in.
+// scratch array, the solver's shared-memory opt-in and the persistent
+// narrowphase grid for this device's SM count (as seevr_physics_create).
 void setup_device(int dev) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e == cudaSuccess) e = init_solver();
     if (e == cudaSuccess) e = init_broadphase();
+    int sms = 0;
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    g_narrow_blocks[dev] = uint32_t(sms > 0 ? sms : 1) * kNarrowBlocksPerSm;
     g_setup_err[dev] = e;
     g_dev_ptr[dev] = e == cudaSuccess ? static_cast<unsigned char*>(p) : nullptr;
 }
@@ -179,6 +184,9 @@ extern "C" seevr_status seevr_physics_step_noalloc(
     s.row_off = reinterpret_cast<uint32_t*>(at(kOffRowOff));
     s.scan_tiles = reinterpret_cast<unsigned long long*>(at(kOffScanTiles));
     s.scan_tiles_cap = kNaScanTiles;
+    s.wait_limit = kSpinLimit;
+    s.narrow_blocks = g_narrow_blocks[dev];
+    s.narrow_per_sm = kNarrowBlocksPerSm;
     s.pair_res0 = reinterpret_cast<float4*>(at(kOffRes0));
     s.pair_res1 = reinterpret_cast<float4*>(at(kOffRes1));
     s.pair_flag = reinterpret_cast<uint32_t*>(at(kOffFlag));
@@ -226,6 +234,7 @@ extern "C" seevr_status seevr_physics_step_noalloc(
     w.c_b = static_cast<uint32_t*>(P(SEEVR_B_CONTACT_GEOM_B));
     w.lambda = static_cast<float*>(P(SEEVR_B_LAMBDA_N));
     w.counters = static_cast<uint32_t*>(P(SEEVR_B_COUNTERS));
+    w.status = s.status;
     w.aabb_min = static_cast<float*>(P(SEEVR_B_BODY_AABB_MIN));
     w.aabb_max = static_cast<float*>(P(SEEVR_B_BODY_AABB_MAX));
     w.pairs = static_cast<uint32_t*>(P(SEEVR_B_COLLISION_PAIRS));

@@ -12,9 +12,11 @@
 // device memory, so a frame needs no host round trip and can be captured
 // into a CUDA graph.
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -98,6 +100,8 @@ struct seevr_physics {
     std::vector<void*> allocations;
     uint64_t launches = 0;
     uint32_t host_flags = 0;
+    // bounds-check mode: SEEVR_CHECK=1 in the environment at creation
+    bool check = false;
     // CUDA graph of one frame
     cudaGraphExec_t graph_exec = nullptr;
     GraphKey graph_key{};
@@ -118,6 +122,21 @@ struct seevr_physics {
     uint32_t narrow_blocks_per_sm = kNarrowBlocksPerSm;
     // the caller's scene layout, kept to rebuild bundles and tiles on retuning
     std::vector<uint32_t> scene_offsets_host;
+    // Scene groups (seevr_tuning.scene_groups > 1): sub-handles over
+    // contiguous scene ranges, each stepping its scenes on its own stream
+    // with its own pair and contact lists, merged into the bound buffers at
+    // the end of every frame.
+    struct Group {
+        seevr_physics* h = nullptr;
+        uint32_t b0 = 0, nb = 0;
+        cudaStream_t stream = nullptr;
+        cudaEvent_t done = nullptr;
+        std::vector<void*> allocs;  // the group's own pair/contact lists
+        GroupOut out{};
+    };
+    std::vector<Group> groups;
+    uint32_t scene_groups = 1;
+    cudaEvent_t fork = nullptr;
 };
 
 namespace {
@@ -135,7 +154,20 @@ seevr_status dev_alloc(seevr_physics* h, T** p, size_t count) {
     return SEEVR_OK;
 }
 
+void free_groups(seevr_physics* h) {
+    for (auto& g : h->groups) {
+        if (g.stream) cudaStreamSynchronize(g.stream);
+        if (g.h) seevr_physics_destroy(g.h);
+        for (void* p : g.allocs) cudaFree(p);
+        if (g.done) cudaEventDestroy(g.done);
+        if (g.stream) cudaStreamDestroy(g.stream);
+    }
+    h->groups.clear();
+}
+
 void free_all(seevr_physics* h) {
+    free_groups(h);
+    if (h->fork) cudaEventDestroy(h->fork);
     if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
     if (h->s.bp_mask) cudaFree(h->s.bp_mask);
     h->s.bp_mask = nullptr;
@@ -197,6 +229,7 @@ void setup_world(seevr_physics* h) {
     w.c_b = static_cast<uint32_t*>(P(SEEVR_B_CONTACT_GEOM_B));
     w.lambda = static_cast<float*>(P(SEEVR_B_LAMBDA_N));
     w.counters = static_cast<uint32_t*>(P(SEEVR_B_COUNTERS));
+    w.status = h->s.status;
     w.aabb_min = static_cast<float*>(P(SEEVR_B_BODY_AABB_MIN));
     w.aabb_max = static_cast<float*>(P(SEEVR_B_BODY_AABB_MAX));
     w.pairs = static_cast<uint32_t*>(P(SEEVR_B_COLLISION_PAIRS));
@@ -271,6 +304,13 @@ struct StageTimer {
     }
 };
 
+// NVTX range of one stage, named as the reference's profiler sections
+// (Physics.step_names, physics.zig:22-32); free when no tool is attached.
+struct Range {
+    explicit Range(const char* name) { nvtxRangePushA(name); }
+    ~Range() { nvtxRangePop(); }
+};
+
 // Issue one frame (Physics.step body) on stream st; returns kernels launched.
 uint64_t issue_frame(seevr_physics* h, uint32_t nb, uint32_t nv, uint32_t nhv, uint32_t substeps,
                      float dt, const float g[3], cudaStream_t st, seevr_profile* prof) {
@@ -282,37 +322,290 @@ uint64_t issue_frame(seevr_physics* h, uint32_t nb, uint32_t nv, uint32_t nhv, u
     w.nbundles = h->num_bundles;
     uint64_t n = 0;
     StageTimer T{h, prof, st};
+    const Range frame("phys/step");
     const float sub_dt = dt / float(substeps);  // physics.zig:90
+    const bool render = nv > 0 && !(h->params.flags & SEEVR_FLAG_SKIP_RENDER_VERTS);
     if (!h->b.ptr[SEEVR_B_HULL_RANGE])
         n += launch_hull_range_from_geom_data(static_cast<const float*>(h->b.ptr[SEEVR_B_GEOM_DATA]),
                                               h->s.derived_hull_range, nb, st);
+    if (h->check) {  // bounds-check mode: the caller's index arrays first
+        const Range r("phys/check_inputs");
+        World wc = w;
+        wc.nv = render ? nv : 0u;
+        n += launch_check_inputs(wc, uint32_t(h->b.bytes[SEEVR_B_SUPPORT_LOOKUP] / 4), st);
+    }
     for (uint32_t s = 0; s < substeps; ++s) {
         T.begin();
-        n += launch_body_stage(w, h->k, (s > 0 ? kIntegrate : 0u) | kGravity | kAabb, sub_dt, g[0],
-                               g[1], g[2], st);
+        {
+            const Range r("phys/aabb");  // with integrate and gravity
+            n += launch_body_stage(w, h->k, (s > 0 ? kIntegrate : 0u) | kGravity | kAabb, sub_dt,
+                                   g[0], g[1], g[2], st);
+        }
         T.end(kStAabb);
         T.begin();
-        n += h->params.broadphase == SEEVR_BROADPHASE_LBVH
-                 ? launch_broadphase_lbvh(w, h->s, h->lb, st)
-                 : launch_broadphase_n2(w, h->s, h->max_scene_bodies, st);
+        {
+            const Range r("phys/broad_phase");
+            n += h->params.broadphase == SEEVR_BROADPHASE_LBVH
+                     ? launch_broadphase_lbvh(w, h->s, h->lb, st)
+                     : launch_broadphase_n2(w, h->s, h->max_scene_bodies, st);
+            if (h->check) n += launch_check_pairs(w, st);
+        }
         T.end(kStBroad);
         T.begin();
-        n += launch_narrowphase(w, h->k, h->s, st);
+        {
+            const Range r("phys/narrow_phase");
+            n += launch_narrowphase(w, h->k, h->s, st);
+            if (h->check) n += launch_check_contacts(w, st);
+        }
         T.end(kStNarrow);
         T.begin();
-        cudaMemsetAsync(w.lambda, 0, sizeof(float) * w.max_contacts, st);  // step 4
+        {
+            const Range r("phys/clear_impulse");
+            cudaMemsetAsync(w.lambda, 0, sizeof(float) * w.max_contacts, st);  // step 4
+        }
         T.end(kStClear);
         T.begin();
-        n += launch_solver(w, h->k, h->s, h->params.solver,
-                           sub_dt, h->max_bundle_bodies, h->smem_bundle_bodies, st);
+        {
+            const Range r("phys/pgs_solve");
+            n += launch_solver(w, h->k, h->s, h->params.solver, sub_dt, h->max_bundle_bodies,
+                               h->smem_bundle_bodies, st);
+        }
         T.end(kStSolve);
     }
-    const bool render = nv > 0 && !(h->params.flags & SEEVR_FLAG_SKIP_RENDER_VERTS);
     T.begin();
-    n += launch_body_stage(w, h->k, kIntegrate | (render ? kRenderVerts : 0u), sub_dt, g[0], g[1],
-                           g[2], st);
+    {
+        const Range r(render ? "phys/render_verts" : "phys/integrate");
+        n += launch_body_stage(w, h->k, kIntegrate | (render ? kRenderVerts : 0u), sub_dt, g[0],
+                               g[1], g[2], st);
+    }
     T.end(render ? kStRender : kStIntegrate);
     return n;
+}
+
+// ---- scene groups --------------------------------------------------------
+// The groups' lists concatenated in group order are the canonical lists of
+// the whole batch (a group's bodies all come after the previous group's), so
+// the merge copies group g's entry i to the group's prefix + i, adding the
+// group's first body to every body and geom index.  Counters are the true
+// totals; entries beyond the caps are dropped and the overflow bit raised, as
+// in the ungrouped step.  Each group's status bits are moved into the
+// handle's status word.
+__global__ void k_merge_groups(World w, GroupTable t) {
+    uint32_t pp[kMaxGroups + 1], cp[kMaxGroups + 1];
+    pp[0] = cp[0] = 0;
+    for (uint32_t g = 0; g < t.n; ++g) {
+        pp[g + 1] = pp[g] + t.g[g].counters[0];
+        cp[g + 1] = cp[g] + t.g[g].counters[1];
+    }
+    const uint32_t np = min(pp[t.n], w.max_pairs), nc = min(cp[t.n], w.max_contacts);
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+    for (uint32_t d = tid; d < np; d += stride) {
+        uint32_t g = 0;
+        while (g + 1 < t.n && pp[g + 1] <= d) ++g;
+        const GroupOut& o = t.g[g];
+        const uint32_t i = d - pp[g];
+        w.pairs[size_t(d) * 2] = o.pairs[size_t(i) * 2] + o.b0;
+        w.pairs[size_t(d) * 2 + 1] = o.pairs[size_t(i) * 2 + 1] + o.b0;
+    }
+    for (uint32_t d = tid; d < nc; d += stride) {
+        uint32_t g = 0;
+        while (g + 1 < t.n && cp[g + 1] <= d) ++g;
+        const GroupOut& o = t.g[g];
+        const uint32_t i = d - cp[g];
+        st3(w.c_pos, d, ld3(o.c_pos, i));
+        st3(w.c_normal, d, ld3(o.c_normal, i));
+        w.c_pen[d] = o.c_pen[i];
+        w.c_a[d] = o.c_a[i] + o.b0;
+        w.c_b[d] = o.c_b[i] + o.b0;
+        w.lambda[d] = o.lambda[i];
+    }
+    if (tid == 0) {
+        uint32_t f = 0;
+        for (uint32_t g = 0; g < t.n; ++g) {
+            f |= t.g[g].status[0];
+            t.g[g].status[0] = 0u;
+        }
+        if (pp[t.n] > w.max_pairs) f |= kFlagPairOverflow;
+        if (cp[t.n] > w.max_contacts) f |= kFlagContactOverflow;
+        if (f) atomicOr(&w.status[0], f);
+        w.counters[0] = pp[t.n];
+        w.counters[1] = cp[t.n];
+    }
+}
+
+// One frame of every group: forked from `st` onto the groups' streams (or,
+// with per-stage profiling, group after group on `st`), joined back, merged.
+uint64_t issue_frame_groups(seevr_physics* h, uint32_t nv, uint32_t nhv, uint32_t substeps,
+                            float dt, const float g[3], cudaStream_t st, seevr_profile* prof) {
+    uint64_t n = 0;
+    if (prof) {
+        for (auto& G : h->groups)
+            if (G.h) n += issue_frame(G.h, G.nb, nv, nhv, substeps, dt, g, st, prof);
+    } else {
+        cudaEventRecord(h->fork, st);
+        for (auto& G : h->groups) {
+            if (!G.h) continue;  // a group of empty scenes
+            cudaStreamWaitEvent(G.stream, h->fork, 0);
+            n += issue_frame(G.h, G.nb, nv, nhv, substeps, dt, g, G.stream, nullptr);
+            cudaEventRecord(G.done, G.stream);
+        }
+        for (auto& G : h->groups)
+            if (G.h) cudaStreamWaitEvent(st, G.done, 0);
+    }
+    GroupTable t{};
+    t.n = uint32_t(h->groups.size());
+    for (uint32_t i = 0; i < t.n; ++i) t.g[i] = h->groups[i].out;
+    const uint32_t cap = std::max(h->caps.max_pairs, h->caps.max_contacts);
+    const uint32_t blocks = std::min((cap + 255) / 256, uint32_t(h->sm_count) * 8u);
+    k_merge_groups<<<std::max(blocks, 1u), 256, 0, st>>>(h->w, t);
+    return n + 1;
+}
+
+__global__ void k_local_geom_body(const uint32_t* __restrict__ geom_body, uint32_t b0, uint32_t n,
+                                  uint32_t* __restrict__ out, uint32_t* bad) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t b = geom_body[b0 + i];
+    const bool inside = b >= b0 && b - b0 < n;
+    out[i] = inside ? b - b0 : i;
+    if (!inside) atomicOr(bad, 1u);
+}
+
+// Split the scenes into h->scene_groups contiguous ranges of about equal
+// bodies and create one sub-handle per range: bound to the handle's arrays
+// at the range's offset (state, masses, geoms, AABBs, render and hull
+// ranges), to the shared hull vertices, lookup table and render vertices,
+// and to its own pair and contact lists and geom -> body map in local
+// indices.  Each group keeps the handle's capacities, so no group overflows
+// where the whole batch would not.
+seevr_status build_groups(seevr_physics* h) {
+    free_groups(h);
+    const std::vector<uint32_t>& off = h->scene_offsets_host;
+    const uint32_t ns = h->num_scenes, G = std::min(h->scene_groups, ns);
+    if (G <= 1) return SEEVR_OK;
+    if (h->params.broadphase != SEEVR_BROADPHASE_N2 || h->check)
+        return fail(SEEVR_ERR_NOT_SUPPORTED,
+                    "scene groups need the all-pairs broadphase and no bounds-check mode");
+    if (!h->fork && cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming) != cudaSuccess)
+        return fail(SEEVR_ERR_CUDA, "cudaEventCreate failed");
+    const uint32_t nb = off[ns];
+    std::vector<uint32_t> cut{0};
+    for (uint32_t s = 1, k = 1; s < ns && k < G; ++s)
+        if (uint64_t(off[s]) * G >= uint64_t(nb) * k) {
+            cut.push_back(s);
+            ++k;
+        }
+    cut.push_back(ns);
+    const seevr_caps& pc = h->caps;
+    uint32_t* bad = nullptr;
+    if (cudaMalloc(&bad, sizeof(uint32_t)) != cudaSuccess || cudaMemset(bad, 0, 4) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(SEEVR_ERR_OUT_OF_MEMORY, "cudaMalloc failed");
+    }
+    seevr_status st = SEEVR_OK;
+    for (size_t gi = 0; gi + 1 < cut.size() && st == SEEVR_OK; ++gi) {
+        h->groups.emplace_back();
+        auto& g = h->groups.back();
+        const uint32_t s0 = cut[gi], s1 = cut[gi + 1];
+        g.b0 = off[s0];
+        g.nb = off[s1] - off[s0];
+        auto alloc = [&](size_t bytes) -> void* {
+            void* p = nullptr;
+            if (st != SEEVR_OK) return nullptr;
+            if (cudaMalloc(&p, bytes ? bytes : 16) != cudaSuccess) {
+                cudaGetLastError();
+                st = fail(SEEVR_ERR_OUT_OF_MEMORY, "cudaMalloc of a scene group's lists failed");
+                return nullptr;
+            }
+            g.allocs.push_back(p);
+            return p;
+        };
+        seevr_bindings b = h->b;
+        auto shift = [&](int i, size_t elem) {
+            if (!b.ptr[i]) return;
+            b.ptr[i] = static_cast<char*>(h->b.ptr[i]) + size_t(g.b0) * elem;
+            b.bytes[i] = size_t(g.nb) * elem;
+        };
+        shift(SEEVR_B_BODY_POS, 12);
+        shift(SEEVR_B_BODY_QUAT, 16);
+        shift(SEEVR_B_BODY_VEL, 12);
+        shift(SEEVR_B_BODY_OMEGA, 12);
+        shift(SEEVR_B_BODY_INV_MASS, 4);
+        shift(SEEVR_B_BODY_INV_INERTIA, 12);
+        shift(SEEVR_B_BODY_VERT_START, 4);
+        shift(SEEVR_B_BODY_VERT_COUNT, 4);
+        shift(SEEVR_B_GEOM_DATA, 32);
+        shift(SEEVR_B_GEOM_FRICTION, 4);
+        shift(SEEVR_B_GEOM_RESTITUTION, 4);
+        shift(SEEVR_B_BODY_AABB_MIN, 12);
+        shift(SEEVR_B_BODY_AABB_MAX, 12);
+        shift(SEEVR_B_SUPPORT_OFFSET, 4);
+        shift(SEEVR_B_HULL_RANGE, 8);
+        const size_t P = pc.max_pairs, C = pc.max_contacts;
+        auto own = [&](int i, size_t bytes) {
+            b.ptr[i] = alloc(bytes);
+            b.bytes[i] = bytes;
+        };
+        own(SEEVR_B_GEOM_BODY_IDX, size_t(g.nb) * 4);
+        own(SEEVR_B_COLLISION_PAIRS, P * 8);
+        own(SEEVR_B_CONTACT_POS, C * 12);
+        own(SEEVR_B_CONTACT_NORMAL, C * 12);
+        own(SEEVR_B_CONTACT_PEN, C * 4);
+        own(SEEVR_B_CONTACT_GEOM_A, C * 4);
+        own(SEEVR_B_CONTACT_GEOM_B, C * 4);
+        own(SEEVR_B_LAMBDA_N, C * 4);
+        own(SEEVR_B_COUNTERS, 16);
+        if (st != SEEVR_OK) break;
+        cudaMemset(b.ptr[SEEVR_B_COUNTERS], 0, 16);
+        g.out = GroupOut{static_cast<const uint32_t*>(b.ptr[SEEVR_B_COUNTERS]), nullptr,
+                         static_cast<const uint32_t*>(b.ptr[SEEVR_B_COLLISION_PAIRS]),
+                         static_cast<const float*>(b.ptr[SEEVR_B_CONTACT_POS]),
+                         static_cast<const float*>(b.ptr[SEEVR_B_CONTACT_NORMAL]),
+                         static_cast<const float*>(b.ptr[SEEVR_B_CONTACT_PEN]),
+                         static_cast<const uint32_t*>(b.ptr[SEEVR_B_CONTACT_GEOM_A]),
+                         static_cast<const uint32_t*>(b.ptr[SEEVR_B_CONTACT_GEOM_B]),
+                         static_cast<const float*>(b.ptr[SEEVR_B_LAMBDA_N]), g.b0};
+        if (g.nb == 0) {  // empty scenes only: nothing to step, counters stay 0
+            uint32_t* word = static_cast<uint32_t*>(alloc(16));
+            if (word) cudaMemset(word, 0, 16);
+            g.out.status = word;
+            continue;
+        }
+        const uint32_t n = g.nb;
+        k_local_geom_body<<<(n + 255) / 256, 256>>>(
+            static_cast<const uint32_t*>(h->b.ptr[SEEVR_B_GEOM_BODY_IDX]), g.b0, g.nb,
+            static_cast<uint32_t*>(b.ptr[SEEVR_B_GEOM_BODY_IDX]), bad);
+        seevr_caps c = pc;
+        c.max_bodies = n;
+        c.max_scenes = s1 - s0;
+        seevr_params p = h->params;
+        p.flags &= ~uint32_t(SEEVR_FLAG_NO_SYNC | SEEVR_FLAG_CUDA_GRAPH);
+        st = seevr_physics_create(&b, &c, &p, &g.h);
+        if (st != SEEVR_OK) break;
+        std::vector<uint32_t> lo(s1 - s0 + 1);
+        for (uint32_t s = s0; s <= s1; ++s) lo[s - s0] = off[s] - g.b0;
+        g.h->narrow_blocks_per_sm = h->narrow_blocks_per_sm;
+        g.h->s.narrow_blocks = h->s.narrow_blocks;
+        g.h->s.narrow_per_sm = h->s.narrow_per_sm;
+        g.h->s.bp_tile_rows = h->s.bp_tile_rows;
+        g.h->s.wait_limit = h->s.wait_limit;
+        g.h->s.giant_min = h->s.giant_min;
+        st = seevr_physics_set_scenes(g.h, lo.data(), s1 - s0);
+        if (st != SEEVR_OK) break;
+        if (cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming) != cudaSuccess)
+            st = fail(SEEVR_ERR_CUDA, "cudaStreamCreate for a scene group failed");
+        g.out.status = g.h->s.status;
+    }
+    uint32_t bad_host = 0;
+    if (st == SEEVR_OK && cudaMemcpy(&bad_host, bad, 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+        st = fail(SEEVR_ERR_CUDA, "cudaMemcpy failed");
+    cudaFree(bad);
+    if (st == SEEVR_OK && bad_host)
+        st = fail(SEEVR_ERR_INVALID_ARGUMENT,
+                  "scene groups need every geom's body inside its own scene (geom_body_idx)");
+    if (st != SEEVR_OK) free_groups(h);
+    return st;
 }
 
 seevr_status check_step_args(seevr_physics* h, uint32_t nb, uint32_t nv, uint32_t nhv) {
@@ -416,13 +709,17 @@ seevr_status ensure_single_scene(seevr_physics* h, uint32_t nb, cudaStream_t st)
 }
 
 seevr_status collect_flags(seevr_physics* h, cudaStream_t st, bool* overflow) {
-    uint32_t f = 0;
-    SEEVR_CUDA(cudaMemcpyAsync(&f, h->s.status, sizeof f, cudaMemcpyDeviceToHost, st));
+    uint32_t f[4] = {0, 0, 0, 0};
+    SEEVR_CUDA(cudaMemcpyAsync(f, h->s.status, sizeof f, cudaMemcpyDeviceToHost, st));
     SEEVR_CUDA(cudaMemsetAsync(h->s.status, 0, sizeof(uint32_t), st));
+    SEEVR_CUDA(cudaMemsetAsync(h->s.status + 2, 0, 2 * sizeof(uint32_t), st));
     SEEVR_CUDA(cudaStreamSynchronize(st));
-    h->host_flags |= f;
-    *overflow = (f & (kFlagPairOverflow | kFlagContactOverflow)) != 0;
-    if (f & kFlagTimeout) return fail(SEEVR_ERR_TIMEOUT, "a device-side wait exceeded its limit");
+    h->host_flags |= f[0];
+    *overflow = (f[0] & (kFlagPairOverflow | kFlagContactOverflow)) != 0;
+    if (f[0] & kFlagCheckFailed)
+        return fail(SEEVR_ERR_INVALID_ARGUMENT, std::string("bounds check: ") + check_name(f[2]) +
+                                                    " (index " + std::to_string(f[3]) + ")");
+    if (f[0] & kFlagTimeout) return fail(SEEVR_ERR_TIMEOUT, "a device-side wait exceeded its limit");
     return SEEVR_OK;
 }
 
@@ -486,6 +783,9 @@ seevr_status seevr_physics_create(const seevr_bindings* b, const seevr_caps* cap
     const seevr_caps& c = h->caps;
     const uint32_t scan_n = std::max(std::max(std::max(c.max_bodies, c.max_pairs), c.max_contacts), 1u);
     h->s.scan_tiles_cap = (scan_n + 2047) / 2048 + 2;
+    h->s.wait_limit = kSpinLimit;
+    h->lb.wait_limit = kSpinLimit;
+    if (const char* e = std::getenv("SEEVR_CHECK")) h->check = std::strcmp(e, "1") == 0;
 #define ALLOC(ptr, n)                                   \
     if (st == SEEVR_OK) st = dev_alloc(h, &(ptr), (n));
     ALLOC(h->s.status, 4);
@@ -496,6 +796,7 @@ seevr_status seevr_physics_create(const seevr_bindings* b, const seevr_caps* cap
     ALLOC(h->s.pair_res1, c.max_pairs);
     ALLOC(h->s.pair_flag, c.max_pairs);
     ALLOC(h->s.pair_coff, c.max_pairs);
+    ALLOC(h->s.pair_class, 8);
     ALLOC(h->s.s_ra, size_t(c.max_contacts) * 3);
     ALLOC(h->s.s_rb, size_t(c.max_contacts) * 3);
     ALLOC(h->s.s_bias, c.max_contacts);
@@ -534,6 +835,15 @@ seevr_status seevr_physics_create(const seevr_bindings* b, const seevr_caps* cap
         ALLOC(is.lvl, 2 * nc + 2);
         ALLOC(is.sort_hist, 4 * 256);
         ALLOC(is.sort_status, lbvh_status_words(c.max_contacts));
+        GiantScratch& gs = is.giant;
+        ALLOC(gs.list, nc);
+        ALLOC(gs.colour, nc);
+        ALLOC(gs.order, nc);
+        ALLOC(gs.used, c.max_bodies);
+        ALLOC(gs.prio, c.max_bodies);
+        ALLOC(gs.hist, kGiantMaxColours);
+        ALLOC(gs.first, kGiantMaxColours + 1);
+        ALLOC(gs.ctr, 8);
     }
     if (p.broadphase == SEEVR_BROADPHASE_LBVH) {
         LbvhScratch& lb = h->lb;
@@ -576,6 +886,7 @@ seevr_status seevr_physics_create(const seevr_bindings* b, const seevr_caps* cap
             sms > 0)
             h->sm_count = sms;
         h->s.narrow_blocks = uint32_t(h->sm_count) * h->narrow_blocks_per_sm;
+        h->s.narrow_per_sm = h->narrow_blocks_per_sm;
         h->s.bp_tile_rows = kTileRows;
     }
     if (st == SEEVR_OK && init_broadphase() != cudaSuccess)
@@ -642,6 +953,7 @@ seevr_status seevr_physics_set_scenes(seevr_physics* h, const uint32_t* body_off
         cudaGraphExecDestroy(h->graph_exec);
         h->graph_exec = nullptr;
     }
+    if (h->scene_groups > 1 || !h->groups.empty()) return build_groups(h);
     return SEEVR_OK;
 }
 
@@ -658,8 +970,11 @@ seevr_status seevr_physics_step(seevr_physics* h, uint32_t num_bodies, uint32_t 
     if (prof) {
         prof->calls += 1;
     }
-    h->launches += issue_frame(h, num_bodies, num_vertices, num_hull_verts, substeps, dt, gravity,
-                               h->stream, prof);
+    h->launches += h->groups.empty()
+                       ? issue_frame(h, num_bodies, num_vertices, num_hull_verts, substeps, dt,
+                                     gravity, h->stream, prof)
+                       : issue_frame_groups(h, num_vertices, num_hull_verts, substeps, dt, gravity,
+                                            h->stream, prof);
     SEEVR_CUDA(cudaGetLastError());
     if (h->params.flags & SEEVR_FLAG_NO_SYNC) return SEEVR_OK;
     bool overflow = false;
@@ -682,8 +997,11 @@ seevr_status seevr_physics_step_async(seevr_physics* h, uint32_t num_bodies, uin
     if (st != SEEVR_OK) return st;
     if (!(h->params.flags & SEEVR_FLAG_CUDA_GRAPH)) {
         for (uint32_t f = 0; f < frames; ++f)
-            h->launches += issue_frame(h, num_bodies, num_vertices, num_hull_verts, substeps, dt,
-                                       gravity, s, nullptr);
+            h->launches += h->groups.empty()
+                               ? issue_frame(h, num_bodies, num_vertices, num_hull_verts, substeps,
+                                             dt, gravity, s, nullptr)
+                               : issue_frame_groups(h, num_vertices, num_hull_verts, substeps, dt,
+                                                    gravity, s, nullptr);
         SEEVR_CUDA(cudaGetLastError());
         return SEEVR_OK;
     }
@@ -696,8 +1014,11 @@ seevr_status seevr_physics_step_async(seevr_physics* h, uint32_t num_bodies, uin
         }
         cudaGraph_t g = nullptr;
         SEEVR_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-        const uint64_t n = issue_frame(h, num_bodies, num_vertices, num_hull_verts, substeps, dt,
-                                       gravity, s, nullptr);
+        const uint64_t n = h->groups.empty()
+                               ? issue_frame(h, num_bodies, num_vertices, num_hull_verts, substeps,
+                                             dt, gravity, s, nullptr)
+                               : issue_frame_groups(h, num_vertices, num_hull_verts, substeps, dt,
+                                                    gravity, s, nullptr);
         cudaError_t e = cudaStreamEndCapture(s, &g);
         if (e != cudaSuccess) return fail(SEEVR_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
         e = cudaGraphInstantiate(&h->graph_exec, g, 0);
@@ -734,7 +1055,8 @@ seevr_status seevr_physics_get_tuning(seevr_physics* h, seevr_tuning* out) {
     out->bundle_bodies = h->params.bundle_bodies ? h->params.bundle_bodies : 512u;
     out->narrow_blocks_per_sm = h->narrow_blocks_per_sm;
     out->broad_tile_rows = h->s.bp_tile_rows ? h->s.bp_tile_rows : kTileRows;
-    out->reserved = 0;
+    out->scene_groups = h->scene_groups;
+    out->giant_island_contacts = h->s.giant_min ? h->s.giant_min : kGiantContacts;
     return SEEVR_OK;
 }
 
@@ -751,11 +1073,16 @@ seevr_status seevr_physics_set_tuning(seevr_physics* h, const seevr_tuning* t) {
                                                     std::to_string(kTileBodies) + "]");
     if (t->bundle_bodies > (1u << 24))
         return fail(SEEVR_ERR_INVALID_ARGUMENT, "bundle_bodies above 2^24");
+    if (t->scene_groups > kMaxGroups)
+        return fail(SEEVR_ERR_INVALID_ARGUMENT, "scene_groups above " + std::to_string(kMaxGroups));
     SEEVR_CUDA(cudaSetDevice(h->device));
     h->narrow_blocks_per_sm = nbps;
     h->s.narrow_blocks = uint32_t(h->sm_count) * nbps;
+    h->s.narrow_per_sm = nbps;
     h->s.bp_tile_rows = rows;
     h->params.bundle_bodies = t->bundle_bodies;
+    h->scene_groups = t->scene_groups ? t->scene_groups : 1u;
+    h->s.giant_min = t->giant_island_contacts;
     if (h->graph_exec) {
         cudaGraphExecDestroy(h->graph_exec);
         h->graph_exec = nullptr;
@@ -763,6 +1090,19 @@ seevr_status seevr_physics_set_tuning(seevr_physics* h, const seevr_tuning* t) {
     if (h->scenes_set) {  // rebuild the bundles and the broadphase tiles
         const std::vector<uint32_t> off = h->scene_offsets_host;
         return seevr_physics_set_scenes(h, off.data(), uint32_t(off.size() - 1));
+    }
+    return SEEVR_OK;
+}
+
+seevr_status seevr_physics_set_wait_limit(seevr_physics* h, uint32_t polls) {
+    if (!h) return fail(SEEVR_ERR_INVALID_ARGUMENT, "handle is NULL");
+    h->s.wait_limit = polls;
+    h->lb.wait_limit = polls;
+    for (auto& g : h->groups)
+        if (g.h) seevr_physics_set_wait_limit(g.h, polls);
+    if (h->graph_exec) {  // kernel arguments are baked into a captured frame
+        cudaGraphExecDestroy(h->graph_exec);
+        h->graph_exec = nullptr;
     }
     return SEEVR_OK;
 }

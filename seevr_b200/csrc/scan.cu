@@ -4,8 +4,11 @@
 // physics.comp:465; contacts, physics.comp:404): counting, scanning and
 // writing at the scanned offsets gives the same totals in a deterministic
 // canonical order.  Tiles take tickets from an atomic counter so every tile
-// a block waits on has already started; each wait is bounded (kSpinLimit)
-// and raises kFlagTimeout instead of hanging.
+// a block waits on has already started; each wait is bounded (the handle's
+// wait limit, kSpinLimit polls by default) and raises kFlagTimeout instead
+// of hanging.  Offsets written after a wait gave up are too small but stay
+// within `out`; the kernels that would use them see the timeout bit and
+// return (timed_out).
 #include "common.cuh"
 
 namespace seevr {
@@ -21,7 +24,7 @@ __device__ __forceinline__ unsigned long long ld_volatile(const unsigned long lo
 __global__ void __launch_bounds__(kScanThreads)
     k_scan(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, const uint32_t* n_dev,
            uint32_t n_cap, uint32_t* total_out, uint32_t total_cap, uint32_t overflow_bit,
-           unsigned long long* tiles, uint32_t* status) {
+           unsigned long long* tiles, uint32_t* status, uint32_t wait_limit) {
     __shared__ uint32_t s_tile, s_excl;
     __shared__ uint32_t s_warp[kScanThreads / 32];
     const uint32_t n = n_dev ? min(*n_dev, n_cap) : n_cap;
@@ -75,7 +78,7 @@ __global__ void __launch_bounds__(kScanThreads)
                     const unsigned long long s = ld_volatile(&st[p]);
                     const uint32_t f = uint32_t(s >> 32);
                     if (f == 0u) {
-                        if (++spins > kSpinLimit) {
+                        if (++spins > wait_limit) {
                             atomicOr(status, kFlagTimeout);
                             break;
                         }
@@ -111,7 +114,7 @@ int launch_exclusive_scan(const uint32_t* in, uint32_t* out, const uint32_t* n_d
     const uint32_t blocks = tiles > 0 ? tiles : 1;
     cudaMemsetAsync(s.scan_tiles, 0, sizeof(unsigned long long) * (blocks + 1), st);
     k_scan<<<blocks, kScanThreads, 0, st>>>(in, out, n_dev, n_cap, total_out, total_cap,
-                                            overflow_bit, s.scan_tiles, s.status);
+                                            overflow_bit, s.scan_tiles, s.status, s.wait_limit);
     return 1;
 }
 

@@ -711,14 +711,14 @@ void seevr_scene_gen_large(seevr_scene* s, uint64_t seed, uint32_t n_bodies, uin
 // the result does not depend on the thread count.
 static void gen_many(seevr_scene* s, uint32_t num_scenes, uint64_t seed_base,
                      uint32_t min_bodies, uint32_t max_bodies, uint32_t segments,
-                     bool rollout) {
+                     bool rollout, const uint64_t* seeds = nullptr) {
     const Mats m = default_materials(s);
     std::vector<seevr_scene> parts(num_scenes);
 #pragma omp parallel for schedule(dynamic, 8)
     for (int64_t sc = 0; sc < int64_t(num_scenes); ++sc) {
         seevr_scene& p = parts[size_t(sc)];
         default_materials(&p);
-        SplitMix64 rng(seed_base + uint64_t(sc));
+        SplitMix64 rng(seeds ? seeds[sc] : seed_base + uint64_t(sc));
         uint32_t n = max_bodies;
         if (!rollout) {
             const double lo = std::log(double(min_bodies)), hi = std::log(double(max_bodies));
@@ -739,6 +739,12 @@ void seevr_scene_gen_batch(seevr_scene* s, uint32_t num_scenes, uint32_t min_bod
     gen_many(s, num_scenes, seed_base, min_bodies, max_bodies, segments, false);
 }
 
+void seevr_scene_gen_batch_seeds(seevr_scene* s, const uint64_t* seeds, uint32_t num_scenes,
+                                 uint32_t min_bodies, uint32_t max_bodies, uint32_t segments) {
+    if (!seeds || num_scenes == 0) return;
+    gen_many(s, num_scenes, 0, min_bodies, max_bodies, segments, false, seeds);
+}
+
 void seevr_scene_gen_rollout(seevr_scene* s, uint32_t num_scenes, uint32_t bodies,
                              uint32_t segments, uint64_t seed_base) {
     gen_many(s, num_scenes, seed_base, bodies, bodies, segments, true);
@@ -746,6 +752,11 @@ void seevr_scene_gen_rollout(seevr_scene* s, uint32_t num_scenes, uint32_t bodie
 
 void seevr_scene_gen_towers(seevr_scene* s, uint64_t seed, uint32_t towers, uint32_t height,
                             float spacing) {
+    seevr_scene_gen_towers_stacked(s, seed, towers, height, spacing, 0.0f);
+}
+
+void seevr_scene_gen_towers_stacked(seevr_scene* s, uint64_t seed, uint32_t towers,
+                                    uint32_t height, float spacing, float overlap) {
     SplitMix64 rng(seed);
     const Mats m = default_materials(s);
     s->begin();
@@ -761,7 +772,7 @@ void seevr_scene_gen_towers(seevr_scene* s, uint64_t seed, uint32_t towers, uint
         for (uint32_t k = 0; k < height; ++k) {
             float c[3];
             c[0] = tx + float(0.01 * rng.normal());
-            c[1] = 0.5f + float(k);
+            c[1] = 0.5f - overlap + float(k) * (1.0f - overlap);
             c[2] = tz + float(0.01 * rng.normal());
             s->add_box(c, half, kRed, 0.6f, 0.f, m.body);
         }

@@ -37,6 +37,7 @@ __global__ void __launch_bounds__(kSolverThreads)
     k_solver(World w, Consts k, Scratch s, uint32_t mode, float dt, uint32_t smem_bodies) {
     extern __shared__ float sm[];
     __shared__ uint32_t sh_levels;
+    if (halted(w.status)) return;  // contacts from a scan that gave up
     const uint32_t scene = blockIdx.x;  // bundle index
     const uint32_t b0 = w.bundle_off[scene], b1 = w.bundle_off[scene + 1];
     const uint32_t nbs = b1 - b0;
@@ -187,6 +188,7 @@ __global__ void __launch_bounds__(kSolverThreads)
 // k (bundle_c0[nbundles] = the contact count).  Marked in one pass instead of
 // a binary search at the start of every solver block.
 __global__ void k_bundle_ranges(World w, uint32_t* __restrict__ bundle_c0) {
+    if (halted(w.status)) return;  // contacts from a scan that gave up
     const uint32_t nc = min(w.counters[1], w.max_contacts);
     for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c <= nc; c += gridDim.x * blockDim.x) {
         const uint32_t cur = c < nc ? w.body_bundle[w.geom_body[w.c_a[c]]] : w.nbundles;
@@ -280,6 +282,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
     // bodies (a single scene above the bundle size) solves on the bound
     // velocity buffers in place
     extern __shared__ float sm[];
+    if (halted(w.status)) return;  // contacts from a scan that gave up
     const unsigned full = 0xFFFFFFFFu;
     const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
     const uint32_t bundle = blockIdx.x * kWarpsPerBlock + wid;

@@ -82,8 +82,9 @@ class Data:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
-            L.lib.seevr_scene_destroy(h)
+        lib = getattr(L, "lib", None)  # None while the interpreter shuts down
+        if h and lib is not None:
+            lib.seevr_scene_destroy(h)
             self._h = None
 
     # ---- builders (data.zig) ----
@@ -142,15 +143,27 @@ class Data:
         return d
 
     @classmethod
+    def batch_seeds(cls, seeds, min_bodies=8, max_bodies=512, segments=16) -> "Data":
+        """The scenes of Data.batch(seed_base=0) whose numbers are listed, in
+        the listed order (scene k is generated from seed k)."""
+        d = cls()
+        arr = np.ascontiguousarray(seeds, dtype=np.uint64)
+        L.lib.seevr_scene_gen_batch_seeds(d._h, arr.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                          len(arr), min_bodies, max_bodies, segments)
+        return d
+
+    @classmethod
     def rollout(cls, num_scenes=1024, bodies=64, segments=16, seed_base=0) -> "Data":
         d = cls()
         L.lib.seevr_scene_gen_rollout(d._h, num_scenes, bodies, segments, seed_base)
         return d
 
     @classmethod
-    def towers(cls, seed=0, towers=1024, height=256, spacing=2.0) -> "Data":
+    def towers(cls, seed=0, towers=1024, height=256, spacing=2.0, overlap=0.0) -> "Data":
+        """Stacks of unit boxes; each box sinks `overlap` m into the one below
+        (0: boxes that just touch)."""
         d = cls()
-        L.lib.seevr_scene_gen_towers(d._h, seed, towers, height, spacing)
+        L.lib.seevr_scene_gen_towers_stacked(d._h, seed, towers, height, spacing, overlap)
         return d
 
     # ---- views ----

@@ -89,13 +89,22 @@ class Physics:
         t = L.Tuning()
         L.check(L.lib.seevr_physics_get_tuning(self._h, C.byref(t)))
         return {"bundle_bodies": t.bundle_bodies, "narrow_blocks_per_sm": t.narrow_blocks_per_sm,
-                "broad_tile_rows": t.broad_tile_rows}
+                "broad_tile_rows": t.broad_tile_rows, "scene_groups": t.scene_groups,
+                "giant_island_contacts": t.giant_island_contacts}
 
     def set_tuning(self, bundle_bodies: int = 0, narrow_blocks_per_sm: int = 0,
-                   broad_tile_rows: int = 0) -> None:
-        """seevr_physics_set_tuning: results are unchanged, only speed (0 = default)."""
-        t = L.Tuning(bundle_bodies, narrow_blocks_per_sm, broad_tile_rows, 0)
+                   broad_tile_rows: int = 0, scene_groups: int = 0,
+                   giant_island_contacts: int = 0) -> None:
+        """seevr_physics_set_tuning (0 = default): launch shapes that change
+        speed only, and the coloured mode's grid-wide island threshold."""
+        t = L.Tuning(bundle_bodies, narrow_blocks_per_sm, broad_tile_rows, scene_groups,
+                     giant_island_contacts)
         L.check(L.lib.seevr_physics_set_tuning(self._h, C.byref(t)))
+
+    def set_wait_limit(self, polls: int) -> None:
+        """seevr_physics_set_wait_limit: polls of an unpublished tile before a
+        device-side look-back gives up (the step then reports ERR_TIMEOUT)."""
+        L.check(L.lib.seevr_physics_set_wait_limit(self._h, polls))
 
     def upload_state(self, num_bodies: int, pos=None, quat=None, vel=None, omega=None) -> None:
         ptr = lambda a: None if a is None else C.c_void_p(a.ctypes.data if isinstance(a, np.ndarray) else a.data_ptr())

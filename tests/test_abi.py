@@ -58,7 +58,7 @@ def test_create_argument_errors():
 def test_status_strings():
     for s in range(8):
         assert L.lib.seevr_status_string(s)
-    assert L.lib.seevr_abi_version() == 1
+    assert L.lib.seevr_abi_version() == 2
 
 
 def test_null_handle_calls_fail_cleanly():

@@ -93,3 +93,45 @@ def test_coloured_batch_close_to_sequential(cuda):
                   params=make_params(pgs_iterations=30, solver=SOLVER_WAVEFRONT, flags=4))
     assert np.isfinite(col["vel"]).all()
     assert np.abs(col["pos"] - seq["pos"]).max() < 0.05
+
+
+
+@pytest.mark.parametrize("n", [36])
+def test_giant_island_grid_solve_on_towers(cuda, n):
+    """The grid-wide coloured solve (giant.cu) on 36 towers of 32 boxes,
+    with the threshold lowered to 16 contacts so that every tower's island
+    takes it (flag bit 5): deterministic (two runs equal bit for bit),
+    finite, and the tower tops sink by the same mean as under the
+    sequential order after 1 s (as the warp-coloured solve does)."""
+    from seevr_b200 import _lib as L
+
+    h = 32
+    d = towers(n, h)
+    st0 = {"pos": d.arrays()["body_pos"].reshape(-1, 3)}
+    caps = Caps.for_data(d, pairs_per_body=8.0, contacts_per_body=4.0)
+    runs = []
+    for solver in (SOLVER_COLORED, SOLVER_COLORED, SOLVER_WAVEFRONT):
+        buf = d.upload(cuda, caps)
+        ph = Physics(buf, make_params(pgs_iterations=30, solver=solver, flags=4))
+        ph.set_tuning(giant_island_contacts=16)
+        flags = 0
+        for _ in range(60):
+            ph.step(buf.num_bodies, 0, buf.num_hull_verts, 10, DT, G)
+            flags |= ph.read_flags()
+        r = read_back(buf)
+        r["flags"] = flags
+        runs.append(r)
+        ph.deinit()
+    col1, col2, seq = runs
+    assert col1["flags"] & L.DEVICE_FLAG_GIANT_ISLANDS, col1["flags"]
+    assert not (col1["flags"] & L.DEVICE_FLAG_TIMEOUT), col1["flags"]
+    assert not (seq["flags"] & L.DEVICE_FLAG_GIANT_ISLANDS)
+    for k in ("pos", "quat", "vel", "omega", "lambda"):
+        assert np.array_equal(col1[k], col2[k]), k
+        assert np.isfinite(col1[k]).all(), k
+    drift_col = np.abs(_tops(col1, n, h) - _tops(st0, n, h))
+    drift_seq = np.abs(_tops(seq, n, h) - _tops(st0, n, h))
+    print("tower-top drift after 1 s: grid-coloured mean %.4f max %.4f, sequential mean %.4f "
+          "max %.4f" % (drift_col.mean(), drift_col.max(), drift_seq.mean(), drift_seq.max()))
+    assert abs(drift_col.mean() - drift_seq.mean()) < 0.02
+    assert drift_col.mean() < 0.3

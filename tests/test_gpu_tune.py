@@ -32,10 +32,57 @@ def test_tuning_leaves_results_unchanged(cuda):
     d = _batch()
     ref = _run(d, cuda)
     for t in ({"narrow_blocks_per_sm": 2}, {"broad_tile_rows": 8}, {"broad_tile_rows": 512},
-              {"bundle_bodies": 64}, {"bundle_bodies": 4096, "narrow_blocks_per_sm": 7}):
+              {"bundle_bodies": 64}, {"bundle_bodies": 4096, "narrow_blocks_per_sm": 7},
+              {"scene_groups": 2}, {"scene_groups": 3, "bundle_bodies": 64},
+              {"scene_groups": 8, "narrow_blocks_per_sm": 3}):
         got = _run(d, cuda, t)
-        for k in ("pos", "quat", "vel", "omega", "pairs", "c_a", "c_b", "lambda"):
+        assert (got["num_pairs"], got["num_contacts"]) == (ref["num_pairs"], ref["num_contacts"])
+        for k in ("pos", "quat", "vel", "omega", "aabb_min", "aabb_max", "pairs", "c_pos",
+                  "c_normal", "c_pen", "c_a", "c_b", "lambda", "verts"):
             assert np.array_equal(got[k], ref[k]), (t, k)
+
+
+@pytest.mark.parametrize("groups", [2, 4])
+def test_scene_groups_in_the_frame_graph(cuda, groups):
+    """Scene groups on their own streams inside the captured frame graph:
+    every output of the batch equals the single-group graph step's, frame
+    after frame, and the flags and counters are those of the whole batch."""
+    import torch
+
+    d = Data.batch(num_scenes=96, min_bodies=8, max_bodies=256, seed_base=41)
+    caps = Caps.for_data(d, pairs_per_body=8.0, contacts_per_body=4.0)
+    outs = []
+    for g in (1, groups):
+        buf = d.upload(cuda, caps)
+        ph = Physics(buf, make_params(pgs_iterations=10, flags=2))
+        ph.set_tuning(scene_groups=g)
+        assert ph.get_tuning()["scene_groups"] == g
+        ph.step_async(buf.num_bodies, buf.num_vertices, buf.num_hull_verts, 10, DT, G, frames=25)
+        torch.cuda.synchronize()
+        outs.append((read_back(buf), ph.read_flags(), ph.read_counters()))
+        ph.deinit()
+    (a, fa, ca), (b, fb, cb) = outs
+    assert a["num_contacts"] > 100 and ca == cb and fa == fb
+    for k in ("pos", "quat", "vel", "omega", "aabb_min", "aabb_max", "pairs", "c_pos",
+              "c_normal", "c_pen", "c_a", "c_b", "lambda", "verts"):
+        assert np.array_equal(a[k], b[k]), k
+
+
+def test_scene_groups_overflow_is_reported(cuda):
+    """The merged counters are the batch's true totals: a pair cap below them
+    raises ERR_CAPACITY as without groups."""
+    d = _batch()
+    caps = Caps.for_data(d, pairs_per_body=8.0, contacts_per_body=4.0)
+    ref = _run(d, cuda, frames=1)
+    caps.max_pairs = max(ref["num_pairs"] // 2, 1)
+    buf = d.upload(cuda, caps)
+    ph = Physics(buf, make_params(pgs_iterations=10, flags=4))
+    ph.set_tuning(scene_groups=3)
+    with pytest.raises(SeevrError) as e:
+        ph.step(buf.num_bodies, buf.num_vertices, buf.num_hull_verts, 10, DT, G)
+    assert e.value.status == 2  # ERR_CAPACITY
+    assert ph.read_counters()[0] == ref["num_pairs"]
+    ph.deinit()
 
 
 def test_tuning_limits_and_defaults(cuda):
@@ -43,14 +90,17 @@ def test_tuning_limits_and_defaults(cuda):
     buf = d.upload(cuda, Caps.for_data(d))
     ph = Physics(buf, make_params(pgs_iterations=10))
     assert ph.get_tuning() == {"bundle_bodies": 512, "narrow_blocks_per_sm": 7,
-                               "broad_tile_rows": 64}
+                               "broad_tile_rows": 64, "scene_groups": 1,
+                               "giant_island_contacts": 4096}
     for bad in ({"narrow_blocks_per_sm": 8}, {"broad_tile_rows": 4},
-                {"broad_tile_rows": 4096}, {"bundle_bodies": (1 << 24) + 1}):
+                {"broad_tile_rows": 4096}, {"bundle_bodies": (1 << 24) + 1},
+                {"scene_groups": 9}):
         with pytest.raises(SeevrError):
             ph.set_tuning(**bad)
     ph.set_tuning(bundle_bodies=256, broad_tile_rows=128)
     assert ph.get_tuning() == {"bundle_bodies": 256, "narrow_blocks_per_sm": 7,
-                               "broad_tile_rows": 128}
+                               "broad_tile_rows": 128, "scene_groups": 1,
+                               "giant_island_contacts": 4096}
     ph.deinit()
 
 

@@ -70,3 +70,53 @@ def test_noalloc_rejects_sizes_beyond_its_limits(cuda):
     st = L.lib.seevr_physics_step_noalloc(C.byref(bind), C.byref(p), 40000, 4000, d.num_bodies,
                                           0, d.num_hull_verts, 1, DT, L.fptr(G, 3), None)
     assert st == L.ERR_INVALID_ARGUMENT
+
+
+def _noalloc_frames(d, cuda, frames, pgs, solver, caps):
+    """`frames` calls of the no-allocation step on a fresh upload of d."""
+    import torch
+
+    buf = d.upload(cuda, caps)
+    bind = buf.bindings()
+    p = make_params(pgs_iterations=pgs, solver=solver, flags=4)  # no render vertices
+    for _ in range(frames):
+        L.check(L.lib.seevr_physics_step_noalloc(C.byref(bind), C.byref(p), caps.max_pairs,
+                                                 caps.max_contacts, buf.num_bodies, 0,
+                                                 buf.num_hull_verts, 10, DT, L.fptr(G, 3),
+                                                 None))
+    torch.cuda.synchronize()
+    return read_back(buf)
+
+
+@pytest.mark.parametrize("scene,frames,pgs,solver", [
+    # 36 towers of 32 boxes, 1,153 bodies: above the 1,024 bodies of the
+    # warp solver, so one block solves the scene with its bodies in shared
+    # memory (the handle's step would use its island solver instead)
+    ("towers", 3, 30, 0), ("towers", 3, 30, 1),
+    # a 2,601-body pile: above the 2,048 bodies of the shared-memory
+    # broadphase and solver, so pairs come from the global-memory
+    # all-pairs kernel and the block solver sweeps in global memory
+    ("pile", 30, 4, 1),
+])
+def test_noalloc_large_scenes_bit_exact(cuda, scene, frames, pgs, solver):
+    import pyoracle
+
+    if scene == "towers":
+        d = Data.towers(seed=1, towers=36, height=32, spacing=2.0)
+        assert 1024 < d.num_bodies <= 2048
+    else:
+        d = Data.pile(seed=11, n_boxes=1300, n_spheres=1300, lo=(-16, 0, -16), hi=(18, 3, 18))
+        assert 2048 < d.num_bodies <= 4096
+    caps = Caps.for_data(d, pairs_per_body=8.0, contacts_per_body=4.0)
+    assert caps.max_pairs <= 32768 and caps.max_contacts <= 16384
+    ref = pyoracle.run(d.arrays(), frames=frames, substeps=10, dt=DT, gravity=G,
+                       pgs_iterations=pgs, max_pairs=caps.max_pairs,
+                       max_contacts=caps.max_contacts, update_verts=False)
+    assert ref["num_contacts"] > 300
+    got = _noalloc_frames(d, cuda, frames, pgs, solver, caps)
+    assert (got["num_pairs"], got["num_contacts"]) == (ref["num_pairs"], ref["num_contacts"])
+    for k in ("pos", "quat", "vel", "omega", "aabb_min", "aabb_max", "pairs", "c_pos",
+              "c_normal", "c_pen", "lambda", "c_a", "c_b"):
+        r = np.asarray(ref[k])
+        r = r.astype(np.float32) if r.dtype == np.float64 else r
+        assert np.array_equal(got[k], r), k

@@ -74,9 +74,14 @@ def parse():
     ap.add_argument("--no-config1", action="store_true")
     ap.add_argument("--config1-bodies", type=int, default=32768)
     ap.add_argument("--config1-frames", type=int, default=60)
+    ap.add_argument("--no-raytrace", action="store_true")
+    ap.add_argument("--rt-width", type=int, default=640)
+    ap.add_argument("--rt-height", type=int, default=480)
     ap.add_argument("--prof-frames", type=int, default=3)
     ap.add_argument("--bundle-bodies", type=int, default=0,
                     help="solver bundle size in bodies (0: the library default)")
+    ap.add_argument("--scene-groups", type=int, default=0,
+                    help="scene ranges stepped on their own streams (0: the library default)")
     ap.add_argument("--autotune", action="store_true",
                     help="time launch shapes on the settled state and use the fastest")
     return ap.parse_args()
@@ -286,6 +291,8 @@ def ours(a, rank, world, local_rank):
     buf = d.upload(dev, caps)
     ph = Physics(buf, make_params(pgs_iterations=a.pgs, flags=FLAG_CUDA_GRAPH,
                                   bundle_bodies=a.bundle_bodies))
+    if a.scene_groups:
+        ph.set_tuning(**(ph.get_tuning() | {"scene_groups": a.scene_groups}))
     stream = torch.cuda.Stream(dev)
 
     def frames(n):
@@ -376,6 +383,8 @@ def ours(a, rank, world, local_rank):
             extras["config0"] = config0_leg(a, dev)
         if world == 1 and not a.no_config1:
             extras["config1"] = config1_leg(a, dev)
+        if world == 1 and not a.no_raytrace:
+            extras["raytrace"] = raytrace_leg(a, dev)
     del buf
     torch.cuda.empty_cache()
     adj = None if a.no_adjoint else adjoint_leg(a, rank, world, dev)
@@ -405,6 +414,7 @@ def ours(a, rank, world, local_rank):
             "plain": extras.get("plain"),
             "config0": extras.get("config0"),
             "config1": extras.get("config1"),
+            "raytrace": extras.get("raytrace"),
             "adjoint": adj,
             "towers": tow,
             "stage_ms_per_frame": stage_ms,
@@ -833,6 +843,63 @@ def config1_leg(a, dev):
     out["states_equal"] = all(np.array_equal(res["lbvh"][0][k], res["all_pairs"][0][k])
                               for k, _, _ in STATE)
     return out
+
+
+def raytrace_leg(a, dev):
+    """Raytrace mode on the 512-body drop-in scene after 60 settling frames:
+    the triangle LBVH build of its render mesh (BVH.build) and frames of the
+    path tracer (16 samples per pixel, up to 16 bounces, raytrace.comp),
+    CUDA events around each."""
+    import torch
+
+    from seevr_b200 import Caps, Data, Physics, make_params
+    from seevr_b200 import _lib as L
+    from seevr_b200.bvh import BVH
+    from seevr_b200.raytrace import Raytracer
+
+    d = Data.pile(seed=0)
+    buf = d.upload(dev, Caps.for_data(d))
+    ph = Physics(buf, make_params(pgs_iterations=a.pgs))
+    for _ in range(60):
+        ph.step(buf.num_bodies, buf.num_vertices, buf.num_hull_verts, a.substeps, DT, G)
+    ph.deinit()
+    arr = d.arrays()
+    ntri = len(arr["indices"])
+    verts = buf["vertices"][: buf.num_vertices * 3].clone()
+    idx = torch.tensor(arr["indices"].reshape(-1).view(np.int32), device=dev)
+    bvh = BVH(verts, idx)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    bvh.build(ntri)  # warm-up
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(5):
+        bvh.build(ntri)
+    e1.record()
+    e1.synchronize()
+    build_ms = e0.elapsed_time(e1) / 5
+    w, h = a.rt_width, a.rt_height
+    rt = Raytracer(d, bvh, w, h)
+    cam = np.array([0.0, 12.0, 24.0, 0.0, -0.35, -1.0, 1.0, 0.0, 0.0, 0.0, 1.0, -0.35], np.float32)
+    cam[3:6] /= np.linalg.norm(cam[3:6])
+    cam[9:12] /= np.linalg.norm(cam[9:12])
+    rt.render(cam[0:3], cam[3:6], cam[6:9], cam[9:12], ntri)  # warm-up
+    torch.cuda.synchronize()
+    frames = 5
+    e0.record()
+    for _ in range(frames):
+        rt.render(cam[0:3], cam[3:6], cam[6:9], cam[9:12], ntri)
+    e1.record()
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / frames
+    finite = bool(torch.isfinite(rt.image).all())
+    bvh.deinit()
+    return {"triangles": ntri, "bvh_build_ms": build_ms,
+            "bvh_triangles_per_s": ntri / (build_ms / 1e3),
+            "width": w, "height": h, "samples_per_pixel": 16, "max_bounces": 16,
+            "frame_ms": ms, "pixel_samples_per_s": w * h * 16 / (ms / 1e3),
+            "image_finite": finite,
+            "scene": "the 512-body drop-in scene after 60 frames, its render mesh "
+                     f"(fov scale {L.lib.seevr_raytrace_fov_scale():.6f})"}
 
 
 def main():

@@ -18,6 +18,7 @@ DEFAULT_CANDIDATES = {
     "narrow_blocks_per_sm": [4, 5, 6, 7],
     "broad_tile_rows": [32, 64, 128, 256],
     "bundle_bodies": [256, 512, 1024],
+    "scene_groups": [1, 2, 3, 4],
 }
 
 

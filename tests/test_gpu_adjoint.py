@@ -105,7 +105,10 @@ def test_adjoint_matches_fp64_finite_differences(cuda, seed):
     for k in fd:
         scale = np.abs(fd[k]).max() + 1e-12
         err = np.abs(ga[k] - fd[k])
-        bad = smooth[k] & (err > 2e-3 * scale + 1e-2 * np.abs(fd[k]))
+        print(f"seed {seed} {k}: largest |FD| {scale:.3e}, largest |adjoint - FD| over smooth "
+              f"components {err[smooth[k]].max() if smooth[k].any() else 0.0:.3e}")
+        # every smooth component within 2e-3 of the group's largest gradient
+        bad = smooth[k] & (err > 2e-3 * scale)
         assert not bad.any(), (k, np.argwhere(bad)[:4].tolist(), ga[k][bad][:4], fd[k][bad][:4])
     # the gradient is not trivially zero where contacts act
     assert np.abs(ga["friction"]).max() > 0.0

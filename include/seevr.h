@@ -120,6 +120,17 @@ enum seevr_solver {
                                     contact order, assessed by drift        */
 };
 
+enum seevr_narrowphase {
+    SEEVR_NARROWPHASE_MPR = 0,     /* Minkowski portal refinement, the
+                                      reference's (physics.comp:171-399)      */
+    SEEVR_NARROWPHASE_GJK_EPA = 1  /* GJK then the expanding polytope
+                                      algorithm: no counterpart in the
+                                      reference's code (its README names
+                                      GJK + EPA); same contract: normal,
+                                      depth and contact point per pair; not
+                                      available to the adjoint               */
+};
+
 enum seevr_flags {
     SEEVR_FLAG_NO_SYNC = 1u << 0,      /* do not synchronize before return  */
     SEEVR_FLAG_CUDA_GRAPH = 1u << 1,   /* capture the frame once, replay    */
@@ -144,6 +155,7 @@ typedef struct seevr_params {
                                   solved together up to this many bodies
                                   (0 = 512); any value gives the same
                                   results, only speed changes              */
+    uint32_t narrowphase;      /* enum seevr_narrowphase (ABI version 2)    */
 } seevr_params;
 
 /* Per-stage device timings in milliseconds, summed over the substeps of one

@@ -26,6 +26,7 @@ typedef struct oracle_params {
     uint32_t pgs_iterations;
     float baumgarte, slop, lin_damp, ang_damp, eps, tol;
     uint32_t mpr_iterations, discover_trials, max_pairs, max_contacts;
+    uint32_t narrowphase;  // 0: MPR, 1: GJK + EPA
 } oracle_params;
 
 // Outputs (any pointer may be NULL).  Values of the last substep.
@@ -85,6 +86,7 @@ oracle::Params to_params(const oracle_params* p) {
     P.discover_trials = p->discover_trials;
     P.max_pairs = p->max_pairs;
     P.max_contacts = p->max_contacts;
+    P.narrowphase = p->narrowphase;
     return P;
 }
 

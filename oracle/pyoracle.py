@@ -41,7 +41,7 @@ class OracleParams(C.Structure):
                 ("lin_damp", C.c_float), ("ang_damp", C.c_float), ("eps", C.c_float),
                 ("tol", C.c_float), ("mpr_iterations", C.c_uint32),
                 ("discover_trials", C.c_uint32), ("max_pairs", C.c_uint32),
-                ("max_contacts", C.c_uint32)]
+                ("max_contacts", C.c_uint32), ("narrowphase", C.c_uint32)]
 
 
 class OracleOut(C.Structure):
@@ -116,7 +116,7 @@ def _params(pgs_iterations, max_pairs, max_contacts, consts) -> OracleParams:
                         consts.get("lin_damp", 0.999), consts.get("ang_damp", 0.998),
                         consts.get("eps", 1e-6), consts.get("tol", 1e-6),
                         consts.get("mpr_iterations", 50), consts.get("discover_trials", 15),
-                        max_pairs, max_contacts)
+                        max_pairs, max_contacts, consts.get("narrowphase", 0))
 
 
 def _outputs(nb: int, nv: int, max_pairs: int, max_contacts: int):

@@ -129,6 +129,7 @@ struct Params {
     uint32_t discover_trials = 15;// physics.comp:290
     uint32_t max_pairs = 10000;   // physics.comp:70
     uint32_t max_contacts = 4000; // physics.comp:69
+    uint32_t narrowphase = 0;     // 0: MPR (physics.comp:171-399), 1: GJK + EPA
 };
 
 // Work counters for the algorithmic flop count of one run.
@@ -492,6 +493,211 @@ class Physics {
         return found;
     }
 
+
+    // ---- GJK + EPA (no counterpart in the reference, whose narrowphase is
+    // MPR only; the alternative narrowphase of seevr_params.narrowphase) ----
+    // Gilbert-Johnson-Keerthi finds a tetrahedron of Minkowski points (A-B
+    // support points) enclosing the origin; the expanding polytope algorithm
+    // then grows it toward the boundary of A-B until the face closest to the
+    // origin is within tolerance of the boundary: its normal and distance
+    // are the contact normal and depth, and the barycentric coordinates of
+    // the origin's projection on it weight the witness points into the
+    // contact point.  Same contract as mpr(): normal n (A is pushed along -n),
+    // depth, contact point.
+    struct SPt {
+        V3<R> v, sa, sb;
+    };
+    static constexpr uint32_t kGjkIters = 64, kEpaIters = 64, kEpaMaxV = 32, kEpaMaxF = 64,
+                              kEpaMaxE = 96;
+    // Reduce the simplex s[0..n) (newest last) toward the origin; returns
+    // true when a tetrahedron encloses it.  d: the next search direction.
+    bool gjk_line(SPt* s, uint32_t& n, V3<R>& d) {
+        const V3<R> a = s[n - 1].v, b = s[n - 2].v;
+        const V3<R> ab = b - a, ao = -a;
+        if (dot(ab, ao) > R(0)) {
+            s[0] = s[n - 2];
+            s[1] = s[n - 1];
+            n = 2;
+            d = cross(cross(ab, ao), ab);
+        } else {
+            s[0] = s[n - 1];
+            n = 1;
+            d = ao;
+        }
+        return false;
+    }
+    bool gjk_triangle(SPt* s, uint32_t& n, V3<R>& d) {  // s = [c, b, a]
+        const V3<R> a = s[2].v, b = s[1].v, c = s[0].v;
+        const V3<R> ab = b - a, ac = c - a, ao = -a;
+        const V3<R> abc = cross(ab, ac);
+        if (dot(cross(abc, ac), ao) > R(0)) {
+            if (dot(ac, ao) > R(0)) {
+                s[1] = s[2];  // [c, a]
+                n = 2;
+                d = cross(cross(ac, ao), ac);
+                return false;
+            }
+            s[0] = s[1];  // [b, a]
+            s[1] = s[2];
+            n = 2;
+            return gjk_line(s, n, d);
+        }
+        if (dot(cross(ab, abc), ao) > R(0)) {
+            s[0] = s[1];  // [b, a]
+            s[1] = s[2];
+            n = 2;
+            return gjk_line(s, n, d);
+        }
+        if (dot(abc, ao) > R(0)) {
+            d = abc;
+        } else {
+            const SPt t = s[0];  // [b, c, a]
+            s[0] = s[1];
+            s[1] = t;
+            d = -abc;
+        }
+        return false;
+    }
+    bool gjk_tetra(SPt* s, uint32_t& n, V3<R>& d) {  // s = [d, c, b, a]
+        const V3<R> a = s[3].v, b = s[2].v, c = s[1].v, dd = s[0].v;
+        const V3<R> ab = b - a, ac = c - a, ad = dd - a, ao = -a;
+        if (dot(cross(ab, ac), ao) > R(0)) {  // outside face abc: [c, b, a]
+            s[0] = s[1];
+            s[1] = s[2];
+            s[2] = s[3];
+            n = 3;
+            return gjk_triangle(s, n, d);
+        }
+        if (dot(cross(ac, ad), ao) > R(0)) {  // outside face acd: [d, c, a]
+            s[2] = s[3];
+            n = 3;
+            return gjk_triangle(s, n, d);
+        }
+        if (dot(cross(ad, ab), ao) > R(0)) {  // outside face adb: [b, d, a]
+            const SPt t = s[0];
+            s[0] = s[2];
+            s[1] = t;
+            s[2] = s[3];
+            n = 3;
+            return gjk_triangle(s, n, d);
+        }
+        return true;
+    }
+    bool gjk(uint32_t a, uint32_t b, SPt* s) {
+        const R e2 = eps() * eps();
+        V3<R> d = get3(pos, a) - get3(pos, b);
+        if (dot(d, d) < e2) d = v3(R(1), R(0), R(0));
+        mink(a, b, d, s[0].v, s[0].sa, s[0].sb);
+        uint32_t n = 1;
+        d = -s[0].v;
+        for (uint32_t it = 0; it < kGjkIters; ++it) {
+            if (dot(d, d) < e2) return false;  // the origin lies on the simplex: touching
+            SPt p;
+            mink(a, b, d, p.v, p.sa, p.sb);
+            if (dot(p.v, d) <= R(0)) return false;  // A-B does not reach past the origin
+            s[n++] = p;
+            const bool in = n == 2   ? gjk_line(s, n, d)
+                            : n == 3 ? gjk_triangle(s, n, d)
+                                     : gjk_tetra(s, n, d);
+            if (in) return true;
+        }
+        return false;
+    }
+    struct Face {
+        uint32_t i, j, k;
+        V3<R> n;
+        R dist;
+    };
+    Face make_face(const SPt* v, uint32_t i, uint32_t j, uint32_t k) const {
+        Face f{i, j, k, v3(R(0), R(0), R(0)), R(1e30)};
+        const V3<R> n = cross(v[j].v - v[i].v, v[k].v - v[i].v);
+        const R l = length(n);
+        if (l > R(0)) {
+            f.n = divs(n, l);
+            f.dist = dot(f.n, v[i].v);
+        }
+        return f;
+    }
+    bool gjk_epa(uint32_t a, uint32_t b, V3<R>& normal, R& depth, V3<R>& cp) {
+        SPt v[kEpaMaxV];
+        if (!gjk(a, b, v)) return false;
+        uint32_t nv = 4, nf = 0;
+        Face f[kEpaMaxF];
+        const uint32_t tri[4][4] = {{3, 2, 1, 0}, {3, 1, 0, 2}, {3, 0, 2, 1}, {2, 0, 1, 3}};
+        for (uint32_t t = 0; t < 4; ++t) {
+            Face g = make_face(v, tri[t][0], tri[t][1], tri[t][2]);
+            if (dot(g.n, v[tri[t][3]].v - v[tri[t][0]].v) > R(0)) {  // the fourth point in front
+                g = make_face(v, tri[t][0], tri[t][2], tri[t][1]);
+            }
+            f[nf++] = g;
+        }
+        Face g{};
+        for (uint32_t it = 0;; ++it) {
+            uint32_t best = 0;  // the closest face (the first of equals)
+            for (uint32_t i = 1; i < nf; ++i)
+                if (f[i].dist < f[best].dist) best = i;
+            g = f[best];
+            if (it >= kEpaIters || nv == kEpaMaxV) break;
+            SPt p;
+            mink(a, b, g.n, p.v, p.sa, p.sb);
+            const R dp = dot(p.v, g.n);
+            if (dp - g.dist < R(P.tol) + eps() * gmax(R(1), dp)) break;
+            // faces the new point sees are removed; their unshared edges
+            // (the horizon) are joined to it
+            uint32_t e[kEpaMaxE][2], ne = 0;
+            bool full = false;
+            uint32_t keep = 0;
+            for (uint32_t i = 0; i < nf; ++i) {
+                if (dot(f[i].n, p.v - v[f[i].i].v) > R(0)) {
+                    const uint32_t ed[3][2] = {{f[i].i, f[i].j}, {f[i].j, f[i].k}, {f[i].k, f[i].i}};
+                    for (uint32_t q = 0; q < 3; ++q) {
+                        uint32_t r = 0;
+                        while (r < ne && !(e[r][0] == ed[q][1] && e[r][1] == ed[q][0])) ++r;
+                        if (r < ne) {  // shared with another removed face
+                            for (uint32_t t = r; t + 1 < ne; ++t) {
+                                e[t][0] = e[t + 1][0];
+                                e[t][1] = e[t + 1][1];
+                            }
+                            --ne;
+                        } else if (ne < kEpaMaxE) {
+                            e[ne][0] = ed[q][0];
+                            e[ne][1] = ed[q][1];
+                            ++ne;
+                        } else {
+                            full = true;
+                        }
+                    }
+                } else {
+                    f[keep++] = f[i];
+                }
+            }
+            if (full || keep + ne > kEpaMaxF) break;  // out of room: the last closest face
+            nf = keep;
+            v[nv] = p;
+            for (uint32_t r = 0; r < ne; ++r) f[nf++] = make_face(v, e[r][0], e[r][1], nv);
+            ++nv;
+        }
+        if (!(g.dist < R(1e30))) return false;  // no face with a normal
+        normal = g.n;
+        depth = g.dist;
+        // barycentric coordinates of the origin's projection g.n * g.dist
+        const V3<R> A = v[g.i].v, B = v[g.j].v, C = v[g.k].v;
+        const V3<R> e0 = B - A, e1 = C - A, e2 = g.dist * g.n - A;
+        const R d00 = dot(e0, e0), d01 = dot(e0, e1), d11 = dot(e1, e1);
+        const R d20 = dot(e2, e0), d21 = dot(e2, e1);
+        const R den = d00 * d11 - d01 * d01;
+        R wb = R(1) / R(3), wc = R(1) / R(3);
+        if (std::fabs(den) > eps() * eps()) {
+            wb = (d11 * d20 - d01 * d21) / den;
+            wc = (d00 * d21 - d01 * d20) / den;
+        }
+        const R wa = R(1) - wb - wc;
+        const V3<R> pa = wa * v[g.i].sa + wb * v[g.j].sa + wc * v[g.k].sa;
+        const V3<R> pb = wa * v[g.i].sb + wb * v[g.j].sb + wc * v[g.k].sb;
+        cp = R(0.5) * (pa + pb);
+        return true;
+    }
+
     // ---- steps ----
     void step_gravity(R dt, const R g[3]) {  // physics.comp:418-428
         const R ld = R(P.lin_damp), ad = R(P.ang_damp);
@@ -564,7 +770,8 @@ class Physics {
             const uint32_t a = pairs[pi * 2], b = pairs[pi * 2 + 1];
             V3<R> n{}, cp{};
             R depth = R(0);
-            const bool found = mpr(a, b, n, depth, cp);
+            const bool found = P.narrowphase == 1 ? gjk_epa(a, b, n, depth, cp)
+                                                  : mpr(a, b, n, depth, cp);
             const bool hit = decide(found && depth > R(0));
             mix(a, (uint64_t(b - a) << 8) ^ (hit ? 0x5Aull : 0ull));
             if (hit) {

@@ -6,7 +6,8 @@ this package fails if that library is not built.
 """
 from ._lib import (SeevrError, Profile, STAGE_NAMES, SOLVER_SEQUENTIAL, SOLVER_WAVEFRONT,
                    SOLVER_COLORED, BROADPHASE_N2, BROADPHASE_LBVH, FLAG_NO_SYNC,
-                   FLAG_CUDA_GRAPH, FLAG_SKIP_RENDER_VERTS, LIB_PATH)
+                   FLAG_CUDA_GRAPH, FLAG_SKIP_RENDER_VERTS, LIB_PATH, NARROWPHASE_MPR,
+                   NARROWPHASE_GJK_EPA)
 from .data import Caps, Data, DeviceBuffers
 from .physics import Physics, make_params
 
@@ -14,4 +15,5 @@ __all__ = [
     "Caps", "Data", "DeviceBuffers", "Physics", "make_params", "SeevrError", "Profile",
     "STAGE_NAMES", "SOLVER_SEQUENTIAL", "SOLVER_WAVEFRONT", "SOLVER_COLORED", "BROADPHASE_N2",
     "BROADPHASE_LBVH", "FLAG_NO_SYNC", "FLAG_CUDA_GRAPH", "FLAG_SKIP_RENDER_VERTS", "LIB_PATH",
+    "NARROWPHASE_MPR", "NARROWPHASE_GJK_EPA",
 ]

@@ -23,6 +23,7 @@ OK, ERR_INVALID_ARGUMENT, ERR_CAPACITY, ERR_CUDA, ERR_TIMEOUT, ERR_NO_DEVICE, \
     ERR_OUT_OF_MEMORY, ERR_NOT_SUPPORTED = range(8)
 
 BROADPHASE_N2, BROADPHASE_LBVH = 0, 1
+NARROWPHASE_MPR, NARROWPHASE_GJK_EPA = 0, 1
 SOLVER_SEQUENTIAL, SOLVER_WAVEFRONT, SOLVER_COLORED = 0, 1, 2
 FLAG_NO_SYNC, FLAG_CUDA_GRAPH, FLAG_SKIP_RENDER_VERTS = 1, 2, 4
 # bits of seevr_physics_read_flags
@@ -56,7 +57,7 @@ class Params(C.Structure):
                 ("mpr_eps", C.c_float), ("mpr_tolerance", C.c_float),
                 ("mpr_iterations", C.c_uint32), ("mpr_discover_trials", C.c_uint32),
                 ("broadphase", C.c_uint32), ("solver", C.c_uint32), ("flags", C.c_uint32),
-                ("bundle_bodies", C.c_uint32)]
+                ("bundle_bodies", C.c_uint32), ("narrowphase", C.c_uint32)]
 
 
 BVH_NUM_BINDINGS = 18

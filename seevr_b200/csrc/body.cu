@@ -37,23 +37,6 @@ int launch_hull_range_from_geom_data(const float* geom_data, uint32_t* out, uint
     return 1;
 }
 
-// p + R v of two vertices at once: the products and sums of add(p, mul(R, v))
-// in the same order, on packed FP32 pairs (sm_100's FMUL2 / FADD2), each
-// component rounded as the scalar operation rounds it.
-__device__ __forceinline__ void xform2(const m3& R, f3 p, f3 a, f3 b, f3& wa, f3& wb) {
-    const float2 X = make_float2(a.x, b.x), Y = make_float2(a.y, b.y), Z = make_float2(a.z, b.z);
-    auto row = [&](float r0, float r1, float r2, float pp) {
-        float2 t = __fadd2_rn(__fmul2_rn(make_float2(r0, r0), X), __fmul2_rn(make_float2(r1, r1), Y));
-        t = __fadd2_rn(t, __fmul2_rn(make_float2(r2, r2), Z));
-        return __fadd2_rn(make_float2(pp, pp), t);
-    };
-    const float2 x = row(R.c0.x, R.c1.x, R.c2.x, p.x);
-    const float2 y = row(R.c0.y, R.c1.y, R.c2.y, p.y);
-    const float2 z = row(R.c0.z, R.c1.z, R.c2.z, p.z);
-    wa = mk(x.x, y.x, z.x);
-    wb = mk(x.y, y.y, z.y);
-}
-
 constexpr uint32_t kBodyThreads = 256;
 // Hulls up to this many vertices are transformed by the body's own thread;
 // larger ones by a warp in the block's second phase.
@@ -150,15 +133,8 @@ __global__ void __launch_bounds__(kBodyThreads) k_body_stage(World w, Consts k, 
         const bool big = hc > kSmallVerts;
         if ((flags & kAabb) && hc <= kSmallVerts) {
             f3 mn = mk(inf, inf, inf), mx = mk(-inf, -inf, -inf);
-            uint32_t i = 0;
-#pragma unroll 4
-            for (; i + 1 < hc; i += 2) {  // vertex order kept: a, then b
-                f3 wa, wb;
-                xform2(R, p, ld3(w.hull, hs + i), ld3(w.hull, hs + i + 1), wa, wb);
-                mn = vmin(vmin(mn, wa), wb);
-                mx = vmax(vmax(mx, wa), wb);
-            }
-            if (i < hc) {
+#pragma unroll 8
+            for (uint32_t i = 0; i < hc; ++i) {
                 const f3 wv = add(p, mul(R, ld3(w.hull, hs + i)));
                 mn = vmin(mn, wv);
                 mx = vmax(mx, wv);
@@ -202,23 +178,17 @@ __global__ void __launch_bounds__(kBodyThreads) k_body_stage(World w, Consts k, 
 #pragma unroll
                     for (uint32_t j = 0; j < kLaneVerts; ++j) {
                         const uint32_t i = c0 + lane + 32u * j;
-                        v[j] = mk(0.f, 0.f, 0.f);  // past the hull: transformed, not reduced
                         if (i < hc) {
                             const float* q = w.hull + size_t(hs + i) * 3;
                             v[j] = mk(__ldg(q), __ldg(q + 1), __ldg(q + 2));
                         }
                     }
 #pragma unroll
-                    for (uint32_t j = 0; j < kLaneVerts; j += 2) {
-                        f3 wa, wb;
-                        xform2(R, p, v[j], v[j + 1], wa, wb);
+                    for (uint32_t j = 0; j < kLaneVerts; ++j) {
                         if (c0 + lane + 32u * j < hc) {
-                            mn = vmin(mn, wa);
-                            mx = vmax(mx, wa);
-                        }
-                        if (c0 + lane + 32u * (j + 1) < hc) {
-                            mn = vmin(mn, wb);
-                            mx = vmax(mx, wb);
+                            const f3 wv = add(p, mul(R, v[j]));
+                            mn = vmin(mn, wv);
+                            mx = vmax(mx, wv);
                         }
                     }
                 }
@@ -264,15 +234,12 @@ __global__ void __launch_bounds__(kRenderThreads) k_render_verts(World w) {
 #pragma unroll
             for (uint32_t j = 0; j < kRenderBatch; ++j) {
                 const uint32_t i = c0 + lane + 32u * j;
-                v[j] = i < ve ? ld3(w.orig, i) : mk(0.f, 0.f, 0.f);
+                if (i < ve) v[j] = ld3(w.orig, i);
             }
 #pragma unroll
-            for (uint32_t j = 0; j < kRenderBatch; j += 2) {
-                f3 wa, wb;
-                xform2(R, p, v[j], v[j + 1], wa, wb);
+            for (uint32_t j = 0; j < kRenderBatch; ++j) {
                 const uint32_t i = c0 + lane + 32u * j;
-                if (i < ve) st3(w.verts, i, wa);
-                if (i + 32u < ve) st3(w.verts, i + 32u, wb);
+                if (i < ve) st3(w.verts, i, add(p, mul(R, v[j])));
             }
         }
     }

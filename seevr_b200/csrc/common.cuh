@@ -86,6 +86,7 @@ struct World {
 struct Consts {
     float baumgarte, slop, lin_damp, ang_damp, eps, tol;
     uint32_t pgs_iterations, mpr_iterations, discover_trials;
+    uint32_t narrowphase;  // 0: MPR, 1: GJK + EPA (seevr_params.narrowphase)
 };
 
 // Grid-wide coloured solve of giant islands (giant.cu); list == NULL: not

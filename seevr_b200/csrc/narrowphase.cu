@@ -64,9 +64,8 @@ __device__ __forceinline__ Shape load_shape(const World& w, uint32_t b, const Po
 // hull vertices when lk == 0 (brute force), else for each of the 3 axes the
 // two lookup bins around the direction's angle.  One loop over candidates
 // serves both, so lanes of a warp holding boxes and spheres share it.
-__device__ __forceinline__ f3 support(const World& w, const Shape& s, const Pose& P, uint32_t i,
-                                      f3 d, uint32_t& chosen) {
-    const m3 R = P.R(i);
+__device__ __forceinline__ f3 support_rp(const World& w, const Shape& s, const m3& R, f3 pos,
+                                         f3 d, uint32_t& chosen) {
     const f3 ld = mulT(R, d);
     const bool lut = s.lk != 0;
     float a0 = 0.f, a1 = 0.f, a2 = 0.f;
@@ -100,7 +99,12 @@ __device__ __forceinline__ f3 support(const World& w, const Shape& s, const Pose
             chosen = idx;
         }
     }
-    return add(P.p(i), mul(R, bv));
+    return add(pos, mul(R, bv));
+}
+
+__device__ __forceinline__ f3 support(const World& w, const Shape& s, const Pose& P, uint32_t i,
+                                      f3 d, uint32_t& chosen) {
+    return support_rp(w, s, P.R(i), P.p(i), d, chosen);
 }
 
 // A Minkowski support point (mink_support_pts, physics.comp:165-169): its
@@ -423,6 +427,243 @@ __global__ void __launch_bounds__(kNarrowThreads, kMinBlocks)
     }
 }
 
+// ---- GJK + EPA -----------------------------------------------------------------
+// The alternative narrowphase (seevr_params.narrowphase = GJK_EPA; no
+// counterpart in the reference, whose shader has MPR only).  Gilbert-Johnson-
+// Keerthi finds a tetrahedron of Minkowski points enclosing the origin; the
+// expanding polytope algorithm grows it toward the boundary of A-B until the
+// face nearest the origin is within tolerance: its normal and distance are the
+// contact normal and depth, and the barycentric coordinates of the origin's
+// projection weight the witness points into the contact point.  One thread
+// per pair, the polytope in local memory (32 points, 64 faces); the
+// arithmetic and the order of every test are those of the oracle's gjk_epa,
+// so results are equal bit for bit.
+struct SPt {
+    f3 v, sa, sb;
+};
+constexpr uint32_t kGjkIters = 64, kEpaIters = 64, kEpaMaxV = 32, kEpaMaxF = 64, kEpaMaxE = 96;
+
+struct PairShapes {
+    Shape A, B;
+    m3 Ra, Rb;
+    f3 pa, pb;
+};
+
+__device__ __forceinline__ SPt mink_pt(const World& w, const PairShapes& q, f3 d) {
+    uint32_t ia, ib;
+    SPt p;
+    p.sa = support_rp(w, q.A, q.Ra, q.pa, d, ia);
+    p.sb = support_rp(w, q.B, q.Rb, q.pb, neg(d), ib);
+    p.v = sub(p.sa, p.sb);
+    return p;
+}
+
+__device__ __forceinline__ bool gjk_line(SPt* s, uint32_t& n, f3& d) {
+    const f3 a = s[n - 1].v, b = s[n - 2].v;
+    const f3 ab = sub(b, a), ao = neg(a);
+    if (dot(ab, ao) > 0.0f) {
+        s[0] = s[n - 2];
+        s[1] = s[n - 1];
+        n = 2;
+        d = cross(cross(ab, ao), ab);
+    } else {
+        s[0] = s[n - 1];
+        n = 1;
+        d = ao;
+    }
+    return false;
+}
+
+__device__ __forceinline__ bool gjk_triangle(SPt* s, uint32_t& n, f3& d) {  // s = [c, b, a]
+    const f3 a = s[2].v, b = s[1].v, c = s[0].v;
+    const f3 ab = sub(b, a), ac = sub(c, a), ao = neg(a);
+    const f3 abc = cross(ab, ac);
+    if (dot(cross(abc, ac), ao) > 0.0f) {
+        if (dot(ac, ao) > 0.0f) {
+            s[1] = s[2];
+            n = 2;
+            d = cross(cross(ac, ao), ac);
+            return false;
+        }
+        s[0] = s[1];
+        s[1] = s[2];
+        n = 2;
+        return gjk_line(s, n, d);
+    }
+    if (dot(cross(ab, abc), ao) > 0.0f) {
+        s[0] = s[1];
+        s[1] = s[2];
+        n = 2;
+        return gjk_line(s, n, d);
+    }
+    if (dot(abc, ao) > 0.0f) {
+        d = abc;
+    } else {
+        const SPt t = s[0];
+        s[0] = s[1];
+        s[1] = t;
+        d = neg(abc);
+    }
+    return false;
+}
+
+__device__ __forceinline__ bool gjk_tetra(SPt* s, uint32_t& n, f3& d) {  // s = [d, c, b, a]
+    const f3 a = s[3].v, b = s[2].v, c = s[1].v, dd = s[0].v;
+    const f3 ab = sub(b, a), ac = sub(c, a), ad = sub(dd, a), ao = neg(a);
+    if (dot(cross(ab, ac), ao) > 0.0f) {
+        s[0] = s[1];
+        s[1] = s[2];
+        s[2] = s[3];
+        n = 3;
+        return gjk_triangle(s, n, d);
+    }
+    if (dot(cross(ac, ad), ao) > 0.0f) {
+        s[2] = s[3];
+        n = 3;
+        return gjk_triangle(s, n, d);
+    }
+    if (dot(cross(ad, ab), ao) > 0.0f) {
+        const SPt t = s[0];
+        s[0] = s[2];
+        s[1] = t;
+        s[2] = s[3];
+        n = 3;
+        return gjk_triangle(s, n, d);
+    }
+    return true;
+}
+
+struct Face {
+    uint32_t i, j, k;
+    f3 n;
+    float dist;
+};
+
+__device__ __forceinline__ Face make_face(const SPt* v, uint32_t i, uint32_t j, uint32_t k) {
+    Face f{i, j, k, mk(0.f, 0.f, 0.f), 1e30f};
+    const f3 n = cross(sub(v[j].v, v[i].v), sub(v[k].v, v[i].v));
+    const float l = length(n);
+    if (l > 0.0f) {
+        f.n = divs(n, l);
+        f.dist = dot(f.n, v[i].v);
+    }
+    return f;
+}
+
+// GJK + EPA for one pair; false: no contact.
+__device__ bool gjk_epa(const World& w, const Consts& k, const PairShapes& q, f3& normal,
+                        float& depth, f3& cp) {
+    SPt v[kEpaMaxV];
+    const float e2 = k.eps * k.eps;
+    // ---- GJK ----
+    f3 d = sub(q.pa, q.pb);
+    if (dot(d, d) < e2) d = mk(1.f, 0.f, 0.f);
+    v[0] = mink_pt(w, q, d);
+    uint32_t n = 1;
+    d = neg(v[0].v);
+    bool in = false;
+    for (uint32_t it = 0; it < kGjkIters && !in; ++it) {
+        if (dot(d, d) < e2) return false;  // the origin lies on the simplex: touching
+        const SPt p = mink_pt(w, q, d);
+        if (dot(p.v, d) <= 0.0f) return false;  // A-B does not reach past the origin
+        v[n++] = p;
+        in = n == 2 ? gjk_line(v, n, d) : n == 3 ? gjk_triangle(v, n, d) : gjk_tetra(v, n, d);
+    }
+    if (!in) return false;
+    // ---- EPA ----
+    Face f[kEpaMaxF];
+    uint32_t nv = 4, nf = 0;
+    const uint32_t tri[4][4] = {{3, 2, 1, 0}, {3, 1, 0, 2}, {3, 0, 2, 1}, {2, 0, 1, 3}};
+    for (uint32_t t = 0; t < 4; ++t) {
+        Face g = make_face(v, tri[t][0], tri[t][1], tri[t][2]);
+        if (dot(g.n, sub(v[tri[t][3]].v, v[tri[t][0]].v)) > 0.0f)
+            g = make_face(v, tri[t][0], tri[t][2], tri[t][1]);
+        f[nf++] = g;
+    }
+    Face g{};
+    for (uint32_t it = 0;; ++it) {
+        uint32_t best = 0;
+        for (uint32_t i = 1; i < nf; ++i)
+            if (f[i].dist < f[best].dist) best = i;
+        g = f[best];
+        if (it >= kEpaIters || nv == kEpaMaxV) break;
+        const SPt p = mink_pt(w, q, g.n);
+        const float dp = dot(p.v, g.n);
+        if (dp - g.dist < k.tol + k.eps * gmax(1.0f, dp)) break;
+        uint32_t e[kEpaMaxE][2], ne = 0, keep = 0;
+        bool full = false;
+        for (uint32_t i = 0; i < nf; ++i) {
+            if (dot(f[i].n, sub(p.v, v[f[i].i].v)) > 0.0f) {
+                const uint32_t ed[3][2] = {{f[i].i, f[i].j}, {f[i].j, f[i].k}, {f[i].k, f[i].i}};
+                for (uint32_t t = 0; t < 3; ++t) {
+                    uint32_t r = 0;
+                    while (r < ne && !(e[r][0] == ed[t][1] && e[r][1] == ed[t][0])) ++r;
+                    if (r < ne) {
+                        for (uint32_t u = r; u + 1 < ne; ++u) {
+                            e[u][0] = e[u + 1][0];
+                            e[u][1] = e[u + 1][1];
+                        }
+                        --ne;
+                    } else if (ne < kEpaMaxE) {
+                        e[ne][0] = ed[t][0];
+                        e[ne][1] = ed[t][1];
+                        ++ne;
+                    } else {
+                        full = true;
+                    }
+                }
+            } else {
+                f[keep++] = f[i];
+            }
+        }
+        if (full || keep + ne > kEpaMaxF) break;
+        nf = keep;
+        v[nv] = p;
+        for (uint32_t r = 0; r < ne; ++r) f[nf++] = make_face(v, e[r][0], e[r][1], nv);
+        ++nv;
+    }
+    if (!(g.dist < 1e30f)) return false;
+    normal = g.n;
+    depth = g.dist;
+    const f3 A = v[g.i].v, B = v[g.j].v, C = v[g.k].v;
+    const f3 e0 = sub(B, A), e1 = sub(C, A), e2v = sub(scale(g.dist, g.n), A);
+    const float d00 = dot(e0, e0), d01 = dot(e0, e1), d11 = dot(e1, e1);
+    const float d20 = dot(e2v, e0), d21 = dot(e2v, e1);
+    const float den = d00 * d11 - d01 * d01;
+    float wb = 1.0f / 3.0f, wc = 1.0f / 3.0f;
+    if (fabsf(den) > e2) {
+        wb = (d11 * d20 - d01 * d21) / den;
+        wc = (d00 * d21 - d01 * d20) / den;
+    }
+    const float wa = 1.0f - wb - wc;
+    const f3 pa = add(add(scale(wa, v[g.i].sa), scale(wb, v[g.j].sa)), scale(wc, v[g.k].sa));
+    const f3 pb = add(add(scale(wa, v[g.i].sb), scale(wb, v[g.j].sb)), scale(wc, v[g.k].sb));
+    cp = scale(0.5f, add(pa, pb));
+    return true;
+}
+
+__global__ void __launch_bounds__(128)
+    k_gjk_epa(World w, Consts k, float4* __restrict__ res0, float4* __restrict__ res1,
+              uint32_t* __restrict__ flag, const uint32_t* __restrict__ order) {
+    if (halted(w.status)) return;
+    const uint32_t np = min(w.counters[0], w.max_pairs);
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < np; t += gridDim.x * blockDim.x) {
+        const uint32_t p = order ? order[t] : t;
+        const uint32_t a = w.pairs[size_t(p) * 2], b = w.pairs[size_t(p) * 2 + 1];
+        PairShapes q;
+        q.A = Shape{w.hull_range[size_t(a) * 2], w.hull_range[size_t(a) * 2 + 1], w.sup_off[a]};
+        q.B = Shape{w.hull_range[size_t(b) * 2], w.hull_range[size_t(b) * 2 + 1], w.sup_off[b]};
+        q.Ra = quat_to_mat(w.quat, a);
+        q.Rb = quat_to_mat(w.quat, b);
+        q.pa = ld3(w.pos, a);
+        q.pb = ld3(w.pos, b);
+        f3 n = mk(0.f, 0.f, 0.f), cp = n;
+        float depth = 0.0f;
+        const bool found = gjk_epa(w, k, q, n, depth, cp);
+        finish(res0, res1, flag, p, found, cp, n, depth);
+    }
+}
+
 // ---- pair order by support path ---------------------------------------------
 // A warp's lanes run their pairs' support calls together; a shape with a
 // support lookup (lk != 0) takes three arctangents and six candidates, one
@@ -519,7 +760,10 @@ int launch_narrowphase_taped(const World& w, const Consts& k, const Scratch& s, 
         order = s.pair_coff;
         n += 2;
     }
-    if (pair_tape) {
+    if (k.narrowphase == 1u && !pair_tape) {  // GJK + EPA (the adjoint tapes MPR only)
+        k_gjk_epa<<<grid_for(w.max_pairs, 128, uint32_t(148 * 16)), 128, 0, st>>>(
+            w, k, s.pair_res0, s.pair_res1, s.pair_flag, order);
+    } else if (pair_tape) {
         if (seven)
             k_narrow<true, 7><<<blocks, kNarrowThreads, 0, st>>>(
                 w, k, s.pair_res0, s.pair_res1, s.pair_flag, &s.status[1], pair_tape, order);

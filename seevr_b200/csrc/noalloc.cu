@@ -265,6 +265,7 @@ extern "C" seevr_status seevr_physics_step_noalloc(
     k.pgs_iterations = p.pgs_iterations;
     k.mpr_iterations = p.mpr_iterations;
     k.discover_trials = p.mpr_discover_trials;
+    k.narrowphase = p.narrowphase <= SEEVR_NARROWPHASE_GJK_EPA ? p.narrowphase : 0u;
 
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     // state the kernels expect to start from: a clear status word, the one

@@ -62,13 +62,14 @@ enum Stage {
     kStClearCounters = 8
 };
 
+// The arguments a captured frame graph was built for (the graph itself can
+// be launched on any stream).
 struct GraphKey {
     uint32_t nb, nv, nhv, substeps;
     float dt, g[3];
-    cudaStream_t stream;
     bool operator==(const GraphKey& o) const {
         return nb == o.nb && nv == o.nv && nhv == o.nhv && substeps == o.substeps && dt == o.dt &&
-               g[0] == o.g[0] && g[1] == o.g[1] && g[2] == o.g[2] && stream == o.stream;
+               g[0] == o.g[0] && g[1] == o.g[1] && g[2] == o.g[2];
     }
 };
 
@@ -253,6 +254,7 @@ void setup_world(seevr_physics* h) {
     h->k.pgs_iterations = p.pgs_iterations;
     h->k.mpr_iterations = p.mpr_iterations;
     h->k.discover_trials = p.mpr_discover_trials;
+    h->k.narrowphase = p.narrowphase;
 }
 
 __global__ void k_single_scene(uint32_t* body_scene, uint32_t* body_bundle, uint32_t* scene_off,
@@ -742,6 +744,7 @@ void seevr_params_default(seevr_params* p) {
     p->solver = SEEVR_SOLVER_WAVEFRONT;
     p->flags = 0;
     p->bundle_bodies = 0;
+    p->narrowphase = SEEVR_NARROWPHASE_MPR;
 }
 
 seevr_status seevr_physics_create(const seevr_bindings* b, const seevr_caps* caps,
@@ -770,8 +773,9 @@ seevr_status seevr_physics_create(const seevr_bindings* b, const seevr_caps* cap
     seevr_params p;
     seevr_params_default(&p);
     if (params) p = *params;
-    if (p.broadphase > SEEVR_BROADPHASE_LBVH || p.solver > SEEVR_SOLVER_COLORED)
-        return fail(SEEVR_ERR_INVALID_ARGUMENT, "unknown broadphase or solver");
+    if (p.broadphase > SEEVR_BROADPHASE_LBVH || p.solver > SEEVR_SOLVER_COLORED ||
+        p.narrowphase > SEEVR_NARROWPHASE_GJK_EPA)
+        return fail(SEEVR_ERR_INVALID_ARGUMENT, "unknown broadphase, solver or narrowphase");
 
     auto* h = new seevr_physics();
     cudaGetDevice(&h->device);
@@ -1006,20 +1010,23 @@ seevr_status seevr_physics_step_async(seevr_physics* h, uint32_t num_bodies, uin
         return SEEVR_OK;
     }
     const GraphKey key{num_bodies, num_vertices, num_hull_verts, substeps, dt,
-                       {gravity[0], gravity[1], gravity[2]}, s};
+                       {gravity[0], gravity[1], gravity[2]}};
     if (!h->graph_exec || !(h->graph_key == key)) {
         if (h->graph_exec) {
             cudaGraphExecDestroy(h->graph_exec);
             h->graph_exec = nullptr;
         }
+        // captured on the handle's own stream (the legacy default stream
+        // cannot be captured), launched on the caller's
+        const cudaStream_t cap = h->stream;
         cudaGraph_t g = nullptr;
-        SEEVR_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        SEEVR_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
         const uint64_t n = h->groups.empty()
                                ? issue_frame(h, num_bodies, num_vertices, num_hull_verts, substeps,
-                                             dt, gravity, s, nullptr)
+                                             dt, gravity, cap, nullptr)
                                : issue_frame_groups(h, num_vertices, num_hull_verts, substeps, dt,
-                                                    gravity, s, nullptr);
-        cudaError_t e = cudaStreamEndCapture(s, &g);
+                                                    gravity, cap, nullptr);
+        cudaError_t e = cudaStreamEndCapture(cap, &g);
         if (e != cudaSuccess) return fail(SEEVR_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
         e = cudaGraphInstantiate(&h->graph_exec, g, 0);
         cudaGraphDestroy(g);
@@ -1170,6 +1177,8 @@ seevr_status seevr_physics_adjoint_substep(seevr_physics* h, uint32_t num_bodies
     if (!grads->pos || !grads->quat || !grads->vel || !grads->omega || !grads->friction)
         return fail(SEEVR_ERR_INVALID_ARGUMENT, "a gradient buffer is NULL");
     if (num_bodies == 0) return SEEVR_OK;
+    if (h->params.narrowphase != SEEVR_NARROWPHASE_MPR)
+        return fail(SEEVR_ERR_NOT_SUPPORTED, "the adjoint differentiates the MPR narrowphase only");
     seevr_status st = check_step_args(h, num_bodies, 0, num_hull_verts);
     if (st != SEEVR_OK) return st;
     SEEVR_CUDA(cudaSetDevice(h->device));

@@ -21,54 +21,48 @@ __device__ __forceinline__ bool is_fixed(const BodyView& B, uint32_t i) {
 
 // One normal + friction update of contact c (physics.comp:525-580), given
 // the two bodies' constant data; v, w: velocities and angular velocities,
-// indexed by la / lb; a fixed body's velocities are not written.  The
-// vector arithmetic runs on packed FP32 pairs (the p3 forms of vmath.cuh),
-// equal to the scalar expressions bit for bit: a warp's update issues fewer
-// instructions, which the warps sharing an SM sub-partition compete for.
+// indexed by la / lb; a fixed body's velocities are not written.
 __device__ __forceinline__ void solve_core(float* V, float* W, uint32_t la, uint32_t lb, bool fixed_a,
-                                           bool fixed_b, float ima, float imb, const m3& Ra_,
-                                           const m3& Rb_, f3 Ia_, f3 Ib_, f3 n_, f3 ra_, f3 rb_,
+                                           bool fixed_b, float ima, float imb, const m3& Ra,
+                                           const m3& Rb, f3 Ia, f3 Ib, f3 n, f3 ra, f3 rb,
                                            float bias, float kn, float mu, float* lam) {
-    const pm3 Ra = pkm(Ra_), Rb = pkm(Rb_);
-    const p3 Ia = pk(Ia_), Ib = pk(Ib_), n = pk(n_), ra = pk(ra_), rb = pk(rb_);
-    p3 va = pk(ld3(V, la)), wa = pk(ld3(W, la)), vb = pk(ld3(V, lb)), wb = pk(ld3(W, lb));
-    p3 ua = padd(va, pcross(wa, ra)), ub = padd(vb, pcross(wb, rb));
-    const float vn = pdot(psub(ub, ua), n);
+    f3 va = ld3(V, la), wa = ld3(W, la), vb = ld3(V, lb), wb = ld3(W, lb);
+    f3 ua = add(va, cross(wa, ra)), ub = add(vb, cross(wb, rb));
+    const float vn = dot(sub(ub, ua), n);
     float d_ln = (-vn + bias) / kn;
     const float old_ln = *lam;
     const float new_ln = gmax(old_ln + d_ln, 0.0f);
     d_ln = new_ln - old_ln;
     *lam = new_ln;
-    const p3 imp = pscale(d_ln, n);
-    va = psub(va, pscale(ima, imp));
-    vb = padd(vb, pscale(imb, imp));
-    wa = psub(wa, papply_inv_I(Ra, Ia, pcross(ra, imp)));
-    wb = padd(wb, papply_inv_I(Rb, Ib, pcross(rb, imp)));
+    const f3 imp = scale(d_ln, n);
+    va = sub(va, scale(ima, imp));
+    vb = add(vb, scale(imb, imp));
+    wa = sub(wa, apply_inv_I(Ra, Ia, cross(ra, imp)));
+    wb = add(wb, apply_inv_I(Rb, Ib, cross(rb, imp)));
     // Coulomb friction along the current slip direction
-    ua = padd(va, pcross(wa, ra));
-    ub = padd(vb, pcross(wb, rb));
-    const p3 dv = psub(ub, ua);
-    const p3 vt = psub(dv, pscale(pdot(dv, n), n));
-    const float vt_len = sqrtf(pdot(vt, vt));
+    ua = add(va, cross(wa, ra));
+    ub = add(vb, cross(wb, rb));
+    const f3 dv = sub(ub, ua);
+    const f3 vt = sub(dv, scale(dot(dv, n), n));
+    const float vt_len = length(vt);
     if (vt_len > 1e-6f) {
-        const p3 td = p3{make_float2(vt.xy.x / vt_len, vt.xy.y / vt_len), vt.z / vt_len};
-        const p3 rat = pcross(ra, td), rbt = pcross(rb, td);
-        const float kt = ima + imb + pdot(rat, papply_inv_I(Ra, Ia, rat)) +
-                         pdot(rbt, papply_inv_I(Rb, Ib, rbt));
+        const f3 td = divs(vt, vt_len);
+        const f3 rat = cross(ra, td), rbt = cross(rb, td);
+        const float kt = ima + imb + dot(rat, apply_inv_I(Ra, Ia, rat)) + dot(rbt, apply_inv_I(Rb, Ib, rbt));
         const float d_lt = gmin(vt_len / kt, mu * new_ln);
-        const p3 it = pscale(d_lt, td);
-        va = padd(va, pscale(ima, it));
-        vb = psub(vb, pscale(imb, it));
-        wa = padd(wa, papply_inv_I(Ra, Ia, pcross(ra, it)));
-        wb = psub(wb, papply_inv_I(Rb, Ib, pcross(rb, it)));
+        const f3 it = scale(d_lt, td);
+        va = add(va, scale(ima, it));
+        vb = sub(vb, scale(imb, it));
+        wa = add(wa, apply_inv_I(Ra, Ia, cross(ra, it)));
+        wb = sub(wb, apply_inv_I(Rb, Ib, cross(rb, it)));
     }
     if (!fixed_a) {
-        st3(V, la, up(va));
-        st3(W, la, up(wa));
+        st3(V, la, va);
+        st3(W, la, wa);
     }
     if (!fixed_b) {
-        st3(V, lb, up(vb));
-        st3(W, lb, up(wb));
+        st3(V, lb, vb);
+        st3(W, lb, wb);
     }
 }
 

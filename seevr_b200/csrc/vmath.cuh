@@ -86,69 +86,6 @@ __device__ __forceinline__ m3 ld_m3(const float* p, uint32_t i) {
     return m;
 }
 
-// ---- packed forms (sm_100 FMUL2 / FADD2) -----------------------------------
-// The same expressions with the x and y components of a vector in one
-// register pair: each packed operation rounds every component exactly as the
-// scalar operation (__fadd2_rn / __fmul2_rn), and a - b is a + (-b), which
-// IEEE addition makes identical to the subtraction.  So every result below
-// equals its scalar counterpart above bit for bit, in fewer instructions.
-struct p3 {
-    float2 xy;
-    float z;
-};
-__device__ __forceinline__ p3 pk(f3 a) { return p3{make_float2(a.x, a.y), a.z}; }
-__device__ __forceinline__ f3 up(p3 a) { return f3{a.xy.x, a.xy.y, a.z}; }
-__device__ __forceinline__ float2 bc(float s) { return make_float2(s, s); }
-__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
-__device__ __forceinline__ p3 padd(p3 a, p3 b) { return p3{__fadd2_rn(a.xy, b.xy), a.z + b.z}; }
-__device__ __forceinline__ p3 psub(p3 a, p3 b) { return p3{__fadd2_rn(a.xy, neg2(b.xy)), a.z - b.z}; }
-__device__ __forceinline__ p3 pscale(float s, p3 a) { return p3{__fmul2_rn(bc(s), a.xy), s * a.z}; }
-__device__ __forceinline__ float pdot(p3 a, p3 b) {
-    const float2 m = __fmul2_rn(a.xy, b.xy);
-    return m.x + m.y + a.z * b.z;
-}
-__device__ __forceinline__ p3 pcross(p3 a, p3 b) {
-    return p3{make_float2(a.xy.y * b.z - a.z * b.xy.y, a.z * b.xy.x - a.xy.x * b.z),
-              a.xy.x * b.xy.y - a.xy.y * b.xy.x};
-}
-// A rotation for apply_inv_I: columns with x,y paired (for R v), and rows
-// 0 and 1 paired per column (for the first two dot products of R^T v).
-struct pm3 {
-    float2 c0, c1, c2;  // (c_k.x, c_k.y)
-    float z0, z1, z2;   // c_k.z
-    float2 rx, ry, rz;  // (c0.x, c1.x), (c0.y, c1.y), (c0.z, c1.z)
-};
-__device__ __forceinline__ pm3 pkm(const m3& R) {
-    pm3 m;
-    m.c0 = make_float2(R.c0.x, R.c0.y);
-    m.c1 = make_float2(R.c1.x, R.c1.y);
-    m.c2 = make_float2(R.c2.x, R.c2.y);
-    m.z0 = R.c0.z;
-    m.z1 = R.c1.z;
-    m.z2 = R.c2.z;
-    m.rx = make_float2(R.c0.x, R.c1.x);
-    m.ry = make_float2(R.c0.y, R.c1.y);
-    m.rz = make_float2(R.c0.z, R.c1.z);
-    return m;
-}
-// R v = (c0 v.x + c1 v.y) + c2 v.z
-__device__ __forceinline__ p3 pmul(const pm3& R, p3 v) {
-    const float2 t = __fadd2_rn(__fadd2_rn(__fmul2_rn(R.c0, bc(v.xy.x)), __fmul2_rn(R.c1, bc(v.xy.y))),
-                                __fmul2_rn(R.c2, bc(v.z)));
-    return p3{t, R.z0 * v.xy.x + R.z1 * v.xy.y + R.z2 * v.z};
-}
-// R^T v = (dot(c0, v), dot(c1, v), dot(c2, v))
-__device__ __forceinline__ p3 pmulT(const pm3& R, p3 v) {
-    const float2 t = __fadd2_rn(__fadd2_rn(__fmul2_rn(R.rx, bc(v.xy.x)), __fmul2_rn(R.ry, bc(v.xy.y))),
-                                __fmul2_rn(R.rz, bc(v.z)));
-    const float2 m = __fmul2_rn(R.c2, v.xy);
-    return p3{t, m.x + m.y + R.z2 * v.z};
-}
-__device__ __forceinline__ p3 papply_inv_I(const pm3& R, p3 inv_i, p3 v) {
-    const p3 l = pmulT(R, v);
-    return pmul(R, p3{__fmul2_rn(inv_i.xy, l.xy), inv_i.z * l.z});
-}
-
 // Arctangent of y/x in (-pi, pi], replacing GLSL atan(y,x)
 // (physics.comp:136-140).  After folding to t = min/max in [0,1], values
 // above tan(pi/8) use atan(t) = pi/4 + atan((t-1)/(t+1)), leaving

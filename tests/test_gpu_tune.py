@@ -57,12 +57,12 @@ def test_scene_groups_in_the_frame_graph(cuda, groups):
         ph = Physics(buf, make_params(pgs_iterations=10, flags=2))
         ph.set_tuning(scene_groups=g)
         assert ph.get_tuning()["scene_groups"] == g
-        ph.step_async(buf.num_bodies, buf.num_vertices, buf.num_hull_verts, 10, DT, G, frames=25)
+        ph.step_async(buf.num_bodies, buf.num_vertices, buf.num_hull_verts, 10, DT, G, frames=70)
         torch.cuda.synchronize()
         outs.append((read_back(buf), ph.read_flags(), ph.read_counters()))
         ph.deinit()
     (a, fa, ca), (b, fb, cb) = outs
-    assert a["num_contacts"] > 100 and ca == cb and fa == fb
+    assert a["num_contacts"] > 50 and ca == cb and fa == fb
     for k in ("pos", "quat", "vel", "omega", "aabb_min", "aabb_max", "pairs", "c_pos",
               "c_normal", "c_pen", "c_a", "c_b", "lambda", "verts"):
         assert np.array_equal(a[k], b[k]), k

@@ -214,3 +214,61 @@ def test_karras_hierarchy_structure():
             stack.append(int(right[x]))
             stack.append(int(left[x]))
     assert order == list(range(n))
+
+
+def _two(shape_a, shape_b, offset):
+    from seevr_b200 import Data
+
+    d = Data()
+    m = d.add_material((0.5, 0.5, 0.5), 0.5, 0.0, (0, 0, 0), 0.0, 1000.0)
+
+    def add(s, c):
+        if s[0] == "box":
+            return d.add_box(c, s[1], (1, 1, 1), 0.5, 0.2, m)
+        return d.add_sphere(c, s[1], (1, 1, 1), 16, 0.5, 0.2, m)
+
+    add(shape_a, (0.0, 5.0, 0.0))
+    add(shape_b, (offset[0], 5.0 + offset[1], offset[2]))
+    return d
+
+
+@pytest.mark.parametrize("case", [
+    # shapes, offset of B from A, exact depth and normal (None: not analytic)
+    (("box", (0.5, 0.5, 0.5)), ("box", (0.5, 0.5, 0.5)), (0.0, 0.9, 0.0), 0.1, (0, 1, 0)),
+    (("box", (0.5, 0.5, 0.5)), ("box", (0.5, 0.5, 0.5)), (0.95, 0.1, 0.2), 0.05, (1, 0, 0)),
+    (("sphere", 0.5), ("box", (0.5, 0.5, 0.5)), (0.0, 0.95, 0.0), None, None),
+    (("sphere", 0.5), ("sphere", 0.4), (0.3, 0.7, 0.1), None, None),
+])
+def test_gjk_epa_known_answers_and_mpr_agreement(case):
+    """The GJK + EPA narrowphase (narrowphase=1) on single pairs: the depth and
+    normal of two overlapping axis-aligned boxes are the overlap along the
+    separating axis; on every case depth and normal agree with MPR's (the
+    reference's narrowphase) to float rounding."""
+    from seevr_b200 import Caps
+
+    sa, sb, off, depth, normal = case
+    d = _two(sa, sb, off)
+    caps = Caps.for_data(d)
+    got = {}
+    for nph in (0, 1):
+        r = pyoracle.run(d.arrays(), frames=1, substeps=1, pgs_iterations=4,
+                         max_pairs=caps.max_pairs, max_contacts=caps.max_contacts,
+                         narrowphase=nph)
+        assert r["num_contacts"] == 1
+        got[nph] = r
+    epa, mpr = got[1], got[0]
+    if depth is not None:
+        assert epa["c_pen"][0] == pytest.approx(depth, abs=2e-6)
+        np.testing.assert_allclose(epa["c_normal"][0], normal, atol=1e-6)
+    assert epa["c_pen"][0] == pytest.approx(mpr["c_pen"][0], rel=1e-5, abs=1e-6)
+    np.testing.assert_allclose(epa["c_normal"][0], mpr["c_normal"][0], atol=1e-5)
+
+
+def test_gjk_epa_separated_pair_has_no_contact():
+    from seevr_b200 import Caps
+
+    d = _two(("box", (0.5, 0.5, 0.5)), ("box", (0.5, 0.5, 0.5)), (0.0, 1.2, 0.0))
+    caps = Caps.for_data(d)
+    r = pyoracle.run(d.arrays(), frames=1, substeps=1, max_pairs=caps.max_pairs,
+                     max_contacts=caps.max_contacts, narrowphase=1)
+    assert r["num_contacts"] == 0

@@ -66,7 +66,7 @@ def parse():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--towers", type=int, default=1024)
     ap.add_argument("--tower-height", type=int, default=256)
-    ap.add_argument("--tower-frames", type=int, default=20)
+    ap.add_argument("--tower-frames", type=int, default=300)
     ap.add_argument("--tower-overlap", type=float, default=0.002)
     ap.add_argument("--no-towers", action="store_true")
     ap.add_argument("--no-config0", action="store_true")
@@ -82,8 +82,9 @@ def parse():
                     help="solver bundle size in bodies (0: the library default)")
     ap.add_argument("--scene-groups", type=int, default=0,
                     help="scene ranges stepped on their own streams (0: the library default)")
-    ap.add_argument("--autotune", action="store_true",
-                    help="time launch shapes on the settled state and use the fastest")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="keep the library's launch shapes instead of timing candidates on "
+                         "the settled state before the timed region")
     return ap.parse_args()
 
 

@@ -32,10 +32,10 @@ def test_gjk_epa_pile_bit_exact(cuda):
 def test_gjk_epa_batch_graph_bit_exact(cuda):
     d = Data.batch(num_scenes=32, min_bodies=8, max_bodies=128, seed_base=7)
     caps = Caps.for_data(d, pairs_per_body=8.0, contacts_per_body=4.0)
-    ref = _oracle(d, caps, 40, 10)
+    ref = _oracle(d, caps, 70, 10)
     assert ref["num_contacts"] > 50
     p = make_params(pgs_iterations=10, flags=2, narrowphase=NARROWPHASE_GJK_EPA)
-    got = gpu_run(d, cuda, frames=40, pgs=10, caps=caps, graph=True, params=p)
+    got = gpu_run(d, cuda, frames=70, pgs=10, caps=caps, graph=True, params=p)
     assert_bit_exact(got, ref)
 
 

@@ -361,8 +361,11 @@ def ours(a, rank, world, local_rank):
     e2e_same = all(np.array_equal(host[k].numpy(), end_state[k]) for k in host)
 
     # ---- per-stage device times of one frame (profiling mode, separate
-    # handle; the state continues from the end of the e2e frames)
+    # handle with the timed handle's launch shapes and scene groups, whose
+    # stages then run one group after another; the state continues from the
+    # end of the e2e frames)
     ph_prof = Physics(buf, make_params(pgs_iterations=a.pgs, bundle_bodies=a.bundle_bodies))
+    ph_prof.set_tuning(**ph.get_tuning())
     prof = Profile()
     for _ in range(a.prof_frames):
         ph_prof.step(nb, nv, nhv, a.substeps, DT, G, prof)
@@ -420,6 +423,9 @@ def ours(a, rank, world, local_rank):
             "adjoint": adj,
             "towers": tow,
             "stage_ms_per_frame": stage_ms,
+            "stage_ms_how": ("CUDA events around each stage of one frame on a handle with the "
+                             "timed handle's launch shapes, the scene groups one after another "
+                             "(the timed frames overlap them, so the sum exceeds ms_per_step)"),
             "last_substep": {"pairs": pairs, "contacts": contacts},
         }
         print(json.dumps(line))
@@ -635,11 +641,55 @@ def plain_dropin(a, d, state, dev):
 
 
 # Figures of single-kernel ncu captures (not measured by this run): per
-# main kernel of each stage, DRAM bytes per launch and issue/warp
-# utilisation, captured on a 1,024-scene batch (same distributions, 0.25x the
-# bodies) and scaled to this workload by bodies (body stage, broadphase,
-# solver) or pairs (narrowphase).  The command is given with each entry.
-NCU_CAPTURE = {}
+# main kernel of each stage, DRAM bytes (read + write) per launch and issue
+# and warp utilisation, captured on a 1,024-scene batch of the same
+# distributions (123,288 bodies, 118,511 pairs and 28,215 contacts at the
+# captured substep) and scaled to a run by its bodies (body stage,
+# broadphase, solver, render vertices) or pairs (narrowphase).  Captured as
+#   ncu --metrics <NCU_METRICS> --clock-control none -k regex:<kernel>
+#       -s <pre-roll and warm-up launches> -c 2 --csv <NCU_SMALL>
+# after the same command exited 0 without ncu; each figure is the mean of
+# the two captured launches.
+NCU_SMALL = ("python bench.py --scenes 1024 --steps 2 --warmup 1 --preroll 90 --no-cpu-baseline "
+             "--no-adjoint --no-towers --no-config0 --no-config1 --no-raytrace --plain-scenes 0 "
+             "--no-autotune --prof-frames 1")
+NCU_METRICS = ("gpu__time_duration.sum,dram__bytes_read.sum,dram__bytes_write.sum,"
+               "sm__inst_executed.sum,sm__issue_active.avg.pct_of_peak_sustained_elapsed,"
+               "sm__warps_active.avg.pct_of_peak_sustained_active,"
+               "smsp__thread_inst_executed_per_inst_executed.ratio,lts__t_sector_hit_rate.pct,"
+               "l1tex__t_sector_hit_rate.pct,launch__registers_per_thread,"
+               "gpu__dram_throughput.avg.pct_of_peak_sustained_elapsed")
+NCU_CAPTURED = {"bodies": 123288, "pairs": 118511, "contacts": 28215}
+NCU_CAPTURE = {
+    "phys/aabb": {"kernel": "k_body_stage", "skip": 1001, "scale": "bodies",
+                  "dram_bytes_per_launch": 247369472, "duration_us": 71.1,
+                  "issue_active_pct": 46.3, "warps_active_pct": 35.7, "lanes_per_inst": 29.2,
+                  "registers": 63},
+    "phys/broad_phase": {"kernel": "k_broad_tile<0> + k_broad_tile<1>", "skip": 1820,
+                         "scale": "bodies", "dram_bytes_per_launch": 9496832,
+                         "duration_us": 57.3, "issue_active_pct": 48.8,
+                         "warps_active_pct": 44.1, "lanes_per_inst": 30.9, "registers": 63},
+    "phys/narrow_phase": {"kernel": "k_narrow<0, 7>", "skip": 910, "scale": "pairs",
+                          "dram_bytes_per_launch": 99364480, "duration_us": 134.6,
+                          "issue_active_pct": 25.1, "warps_active_pct": 28.7,
+                          "lanes_per_inst": 12.7, "registers": 72},
+    "phys/pgs_solve": {"kernel": "k_solver_warp", "skip": 910, "scale": "bodies",
+                       "dram_bytes_per_launch": 10574720, "duration_us": 320.8,
+                       "issue_active_pct": 8.4, "warps_active_pct": 4.9, "lanes_per_inst": 16.0,
+                       "registers": 127},
+    "phys/render_verts": {"kernel": "k_render_verts", "skip": 91, "scale": "bodies",
+                          "dram_bytes_per_launch": 393891200, "duration_us": 97.6,
+                          "issue_active_pct": 36.3, "warps_active_pct": 39.7,
+                          "lanes_per_inst": 30.0, "registers": 62},
+}
+
+
+def ncu_scaled(stage, nb, pairs):
+    """The captured DRAM bytes per launch of a stage's main kernel, scaled
+    from the captured batch to this run by bodies or pairs."""
+    c = NCU_CAPTURE[stage]
+    f = (pairs / NCU_CAPTURED["pairs"]) if c["scale"] == "pairs" else (nb / NCU_CAPTURED["bodies"])
+    return c["dram_bytes_per_launch"] * f
 
 
 def roofline(stage_ms, ms_per_step, nb, nhv, nv, pairs, contacts, substeps, peak, peak_kind, a):
@@ -677,26 +727,28 @@ def roofline(stage_ms, ms_per_step, nb, nhv, nv, pairs, contacts, substeps, peak
         e = {"stage": k, "kernel": kern, "bound": bound, "share": ms / total_stage,
              "launch_ms": launch_ms, "algorithmic_bytes_per_launch": algo,
              "achieved_gbs": gbs, "hbm_frac": gbs / peak}
-        if k in NCU_CAPTURE and default_workload(a):
-            e["ncu"] = NCU_CAPTURE[k]
+        if k in NCU_CAPTURE:
+            e["ncu"] = dict(NCU_CAPTURE[k])
+            e["ncu"]["dram_bytes_per_launch_scaled"] = ncu_scaled(k, nb, pairs)
         stages.append(e)
-    traffic = None
-    if default_workload(a) and all(k in NCU_CAPTURE for k in per_substep if k != "phys/clear_impulse"):
-        traffic = sum(substeps * NCU_CAPTURE[k]["dram_bytes_per_launch"]
-                      for k in per_substep if k != "phys/clear_impulse")
+    # per frame: the stage kernels' captured DRAM bytes per launch, scaled to
+    # this run, times their launches per frame (the impulse clear is a
+    # memset of 4 bytes per contact, counted at its algorithmic size)
+    traffic = sum(substeps * ncu_scaled(k, nb, pairs) for k in per_substep
+                  if k in NCU_CAPTURE) + substeps * 4 * contacts + \
+        ncu_scaled("phys/render_verts", nb, pairs)
     return {"bound": "hbm", "kernel": f"whole frame ({substeps} substeps + render vertices)",
             "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "peak_source": peak_kind, "traffic": traffic,
-            "traffic_source": ("sum over the stage kernels of their ncu-captured DRAM bytes "
-                               "per launch (stages[].ncu)") if traffic else None,
+            "traffic_source": ("per frame: the stage kernels' ncu-captured DRAM bytes per launch "
+                               "(stages[].ncu, a 1,024-scene capture scaled by bodies or pairs) "
+                               "times their launches"),
+            "traffic_over_algorithmic": traffic / frame_bytes,
+            "ncu_command": f"ncu --metrics {NCU_METRICS} --clock-control none "
+                           f"-k regex:<kernel> -s <skip> -c 2 --csv {NCU_SMALL}",
             "algorithmic_bytes_per_frame": frame_bytes,
             "dominant_stage": stages[0]["stage"] if stages else None,
             "stages": stages}
-
-
-def default_workload(a):
-    return (a.scenes, a.min_bodies, a.max_bodies, a.segments, a.substeps, a.pgs, a.preroll) == \
-        (4096, 8, 512, 16, 10, 30, 90)
 
 
 def cpu_baseline(a, full_off, state, dev, rank):

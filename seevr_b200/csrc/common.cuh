@@ -70,6 +70,9 @@ struct World {
     uint32_t* pairs;
     const uint32_t* sup_off;
     const uint32_t* sup_lut;
+    // per body, the offset of a lookup table equal in content to its own
+    // (launch_lut_alias; NULL: sup_off)
+    const uint32_t* lut_off;
     const uint32_t* hull_range;  // (start,count) per geom: binding 30 or derived
     const uint32_t* body_scene;  // body -> scene
     const uint32_t* scene_off;   // scene -> first body, [num_scenes+1]
@@ -137,8 +140,10 @@ struct Scratch {
     uint32_t* pair_flag;    // [max_pairs] 1 if the pair makes a contact
     uint32_t* pair_coff;    // [max_pairs] exclusive scan of pair_flag (before it:
                             // the narrowphase's pair order)
-    uint32_t* pair_class;   // [8] pairs per support-path class and cursors
+    uint32_t* pair_class;   // [2*kPairClasses] pairs per class and cursors
                             // (NULL: pairs taken in index order)
+    uint32_t* lut_rep;      // [kLutHullMax] first body with a lookup per hull size
+    uint32_t* lut_off;      // [max_bodies] lookup offset read by the narrowphase
     // solver, per contact
     float* s_ra;            // [max_contacts*3]
     float* s_rb;            // [max_contacts*3]
@@ -226,6 +231,16 @@ constexpr uint32_t kTileRows = 64;
 // cap; measured best of 4 to 8)
 constexpr uint32_t kNarrowBlocksPerSm = 7;
 int launch_narrowphase(const World& w, const Consts& k, const Scratch& s, cudaStream_t st);
+// The support lookups of bodies whose table equals, entry for entry, the
+// table of the first body with the same hull size are read through that one
+// table (s.lut_off): the same values, from a copy that stays in cache.
+constexpr uint32_t kLutHullMax = 4096;
+// narrowphase pair order: 4 classes by the two shapes' support paths
+constexpr uint32_t kPairClasses = 4;
+int launch_lut_alias(const World& w, const Scratch& s, cudaStream_t st);
+__device__ __forceinline__ uint32_t lut_of(const World& w, uint32_t b) {
+    return w.lut_off ? w.lut_off[b] : w.sup_off[b];
+}
 // Narrowphase that also tapes the supporting hull vertices of each contact's
 // final portal (2 uint4 per pair / contact) for the adjoint.
 int launch_narrowphase_taped(const World& w, const Consts& k, const Scratch& s, uint4* pair_tape,

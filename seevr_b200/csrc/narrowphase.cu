@@ -56,14 +56,16 @@ struct Pose {
 
 __device__ __forceinline__ Shape load_shape(const World& w, uint32_t b, const Pose& P, uint32_t i) {
     P.put(i, quat_to_mat(w.quat, b), ld3(w.pos, b));
-    return Shape{w.hull_range[size_t(b) * 2], w.hull_range[size_t(b) * 2 + 1], w.sup_off[b]};
+    return Shape{w.hull_range[size_t(b) * 2], w.hull_range[size_t(b) * 2 + 1], lut_of(w, b)};
 }
 
 // support (physics.comp:107-162).  Both paths of the reference visit a list
 // of candidate vertices in order and keep the first strict maximum: all
 // hull vertices when lk == 0 (brute force), else for each of the 3 axes the
-// two lookup bins around the direction's angle.  One loop over candidates
-// serves both, so lanes of a warp holding boxes and spheres share it.
+// two lookup bins around the direction's angle.  The lookup path issues its
+// six entry loads, then its six vertex loads, each level at once (two
+// dependent memory latencies per call instead of twelve); pairs are ordered
+// by path (k_pair_classes), so a warp's lanes mostly take the same one.
 __device__ __forceinline__ f3 support_rp(const World& w, const Shape& s, const m3& R, f3 pos,
                                          f3 d, uint32_t& chosen) {
     const f3 ld = mulT(R, d);
@@ -77,26 +79,40 @@ __device__ __forceinline__ f3 support_rp(const World& w, const Shape& s, const m
     float best = -1e10f;
     f3 bv = mk(0.f, 0.f, 0.f);
     chosen = kNone;  // no vertex beat -1e10: the support point is the body position
-    const uint32_t n = lut ? 6u : s.vc;
-    uint32_t b0 = 0;
-    for (uint32_t k = 0; k < n; ++k) {
-        uint32_t idx = k;
-        if (lut) {
-            const uint32_t ax = k >> 1;
-            if ((k & 1u) == 0u) {
-                float a = ax == 0 ? a0 : (ax == 1 ? a1 : a2);
-                if (a < 0.0f) a += 6.2831853f;
-                const float bin_f = a / 6.2831853f * 64.0f;
-                b0 = uint32_t(bin_f) % 64u;
-            }
-            idx = w.sup_lut[s.lk + ax * 64u + ((k & 1u) ? (b0 + 1u) % 64u : b0)];
+    if (lut) {
+        // the six lookup entries, then the six candidate vertices, all loads
+        // of a level in flight together; compared in the reference's order
+        uint32_t idx[6];
+#pragma unroll
+        for (uint32_t ax = 0; ax < 3; ++ax) {
+            float a = ax == 0 ? a0 : (ax == 1 ? a1 : a2);
+            if (a < 0.0f) a += 6.2831853f;
+            const float bin_f = a / 6.2831853f * 64.0f;
+            const uint32_t b0 = uint32_t(bin_f) % 64u;
+            idx[2 * ax] = w.sup_lut[s.lk + ax * 64u + b0];
+            idx[2 * ax + 1] = w.sup_lut[s.lk + ax * 64u + (b0 + 1u) % 64u];
         }
-        const f3 v = ld3(w.hull, s.vs + idx);
+        f3 v[6];
+#pragma unroll
+        for (uint32_t k = 0; k < 6; ++k) v[k] = ld3(w.hull, s.vs + idx[k]);
+#pragma unroll
+        for (uint32_t k = 0; k < 6; ++k) {
+            const float dd = dot(v[k], ld);
+            if (dd > best) {
+                best = dd;
+                bv = v[k];
+                chosen = idx[k];
+            }
+        }
+        return add(pos, mul(R, bv));
+    }
+    for (uint32_t k = 0; k < s.vc; ++k) {
+        const f3 v = ld3(w.hull, s.vs + k);
         const float dd = dot(v, ld);
         if (dd > best) {
             best = dd;
             bv = v;
-            chosen = idx;
+            chosen = k;
         }
     }
     return add(pos, mul(R, bv));
@@ -651,8 +667,8 @@ __global__ void __launch_bounds__(128)
         const uint32_t p = order ? order[t] : t;
         const uint32_t a = w.pairs[size_t(p) * 2], b = w.pairs[size_t(p) * 2 + 1];
         PairShapes q;
-        q.A = Shape{w.hull_range[size_t(a) * 2], w.hull_range[size_t(a) * 2 + 1], w.sup_off[a]};
-        q.B = Shape{w.hull_range[size_t(b) * 2], w.hull_range[size_t(b) * 2 + 1], w.sup_off[b]};
+        q.A = Shape{w.hull_range[size_t(a) * 2], w.hull_range[size_t(a) * 2 + 1], lut_of(w, a)};
+        q.B = Shape{w.hull_range[size_t(b) * 2], w.hull_range[size_t(b) * 2 + 1], lut_of(w, b)};
         q.Ra = quat_to_mat(w.quat, a);
         q.Rb = quat_to_mat(w.quat, b);
         q.pa = ld3(w.pos, a);
@@ -668,8 +684,12 @@ __global__ void __launch_bounds__(128)
 // A warp's lanes run their pairs' support calls together; a shape with a
 // support lookup (lk != 0) takes three arctangents and six candidates, one
 // without walks all its hull vertices.  Taking the pairs grouped by the two
-// shapes' paths (4 classes) keeps a warp's lanes on one path.  Each pair's
-// result is staged at its own index, so the order changes no result.
+// shapes' paths (4 classes) keeps a warp's lanes on one path, and within a
+// class the broadphase's order, in which neighbouring pairs share a body
+// (and its hull in cache).  Each pair's result is staged at its own index,
+// so the order changes no result.  (Putting pairs whose bounding spheres
+// overlap first, as longer MPR runs, measured 11% slower: it breaks up
+// those shared bodies.)
 __device__ __forceinline__ uint32_t pair_class(const World& w, uint32_t p) {
     const uint32_t a = w.pairs[size_t(p) * 2], b = w.pairs[size_t(p) * 2 + 1];
     return (w.sup_off[a] != 0u ? 2u : 0u) | (w.sup_off[b] != 0u ? 1u : 0u);
@@ -681,29 +701,81 @@ __global__ void k_pair_classes(World w, uint32_t* __restrict__ cls, uint32_t* __
     if (halted(w.status)) return;
     const uint32_t np = min(w.counters[0], w.max_pairs);
     const uint32_t lane = threadIdx.x & 31u;
-    uint32_t pre[4] = {0, 0, 0, 0};
-    if (kScatter) {
-        pre[1] = cls[0];
-        pre[2] = pre[1] + cls[1];
-        pre[3] = pre[2] + cls[2];
-    }
+    uint32_t pre[kPairClasses];
+    pre[0] = 0;
+#pragma unroll
+    for (uint32_t k = 1; k < kPairClasses; ++k) pre[k] = kScatter ? pre[k - 1] + cls[k - 1] : 0u;
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t p0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); p0 < np; p0 += stride) {
         const uint32_t p = p0 + lane;
-        const uint32_t c = p < np ? pair_class(w, p) : 4u;
+        const uint32_t c = p < np ? pair_class(w, p) : kPairClasses;
 #pragma unroll
-        for (uint32_t k = 0; k < 4; ++k) {
+        for (uint32_t k = 0; k < kPairClasses; ++k) {
             const unsigned m = __ballot_sync(0xFFFFFFFFu, c == k);
             if (!m) continue;
             const uint32_t leader = __ffs(m) - 1;
             uint32_t base = 0;
-            if (lane == leader) base = atomicAdd(&cls[kScatter ? 4 + k : k], uint32_t(__popc(m)));
+            if (lane == leader)
+                base = atomicAdd(&cls[kScatter ? kPairClasses + k : k], uint32_t(__popc(m)));
             if (kScatter) {
                 base = __shfl_sync(0xFFFFFFFFu, base, leader);
                 if (c == k) order[pre[k] + base + __popc(m & ((1u << lane) - 1u))] = p;
             }
         }
     }
+}
+
+static uint32_t grid_for(uint32_t cap, uint32_t threads, uint32_t max_blocks) {
+    uint32_t g = (cap + threads - 1) / threads;
+    if (g > max_blocks) g = max_blocks;
+    return g ? g : 1;
+}
+
+// ---- shared lookup tables ------------------------------------------------------
+// Scene builders give every geom with a lookup its own table (data.zig:299-353),
+// though all UV spheres of one segment count have identical ones: the bench
+// batch holds about 250,000 copies of one 768-byte table, which the support
+// calls would read from 190 MB.  Per frame, the first body with a lookup of
+// each hull size is found, and a body whose table equals that body's entry
+// for entry reads it instead: the same indices, one copy in cache.
+__global__ void k_lut_reps(World w, uint32_t* __restrict__ rep) {
+    if (check_failed(w.status)) return;
+    for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < w.nb; b += gridDim.x * blockDim.x) {
+        if (w.sup_off[b] == 0u) continue;
+        const uint32_t hc = w.hull_range[size_t(b) * 2 + 1];
+        if (hc < kLutHullMax) atomicMin(&rep[hc], b);
+    }
+}
+
+__global__ void k_lut_alias(World w, const uint32_t* __restrict__ rep, uint32_t* __restrict__ out) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    if (check_failed(w.status)) return;
+    for (uint32_t b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < w.nb; b += nwarps) {
+        const uint32_t lk = w.sup_off[b];
+        uint32_t res = lk;
+        if (lk != 0u) {
+            const uint32_t hc = w.hull_range[size_t(b) * 2 + 1];
+            const uint32_t r = hc < kLutHullMax ? rep[hc] : kNone;
+            if (r != kNone && r != b) {
+                const uint32_t lr = w.sup_off[r];
+                bool same = true;
+                for (uint32_t k = lane; k < 192u; k += 32u) same &= w.sup_lut[lk + k] == w.sup_lut[lr + k];
+                if (__all_sync(0xFFFFFFFFu, same)) res = lr;
+            }
+        }
+        if (lane == 0) out[b] = res;
+    }
+}
+
+int launch_lut_alias(const World& w, const Scratch& s, cudaStream_t st) {
+    if (!s.lut_off || w.nb == 0) return 0;
+    cudaMemsetAsync(s.lut_rep, 0xFF, sizeof(uint32_t) * kLutHullMax, st);
+    const uint32_t blocks = grid_for(w.nb, 256, 148 * 8);
+    k_lut_reps<<<blocks, 256, 0, st>>>(w, s.lut_rep);
+    // a warp per body, 8 per block
+    k_lut_alias<<<grid_for(w.nb, 8, 148 * 16), 256, 0, st>>>(w, s.lut_rep, s.lut_off);
+    return 2;
 }
 
 // add_contact (physics.comp:403-412) at the scanned slot.
@@ -732,12 +804,6 @@ __global__ void k_contact_scatter(World w, const float4* __restrict__ res0,
     }
 }
 
-static uint32_t grid_for(uint32_t cap, uint32_t threads, uint32_t max_blocks) {
-    uint32_t g = (cap + threads - 1) / threads;
-    if (g > max_blocks) g = max_blocks;
-    return g ? g : 1;
-}
-
 int launch_narrowphase_taped(const World& w, const Consts& k, const Scratch& s, uint4* pair_tape,
                              uint4* contact_tape, cudaStream_t st) {
     if (w.max_pairs == 0) return 0;
@@ -753,7 +819,7 @@ int launch_narrowphase_taped(const World& w, const Consts& k, const Scratch& s, 
     const uint32_t* order = nullptr;
     int n = 3;
     if (s.pair_class) {
-        cudaMemsetAsync(s.pair_class, 0, 8 * sizeof(uint32_t), st);
+        cudaMemsetAsync(s.pair_class, 0, 2 * kPairClasses * sizeof(uint32_t), st);
         const uint32_t cb = grid_for(w.max_pairs, 256, 148 * 8);
         k_pair_classes<false><<<cb, 256, 0, st>>>(w, s.pair_class, nullptr);
         k_pair_classes<true><<<cb, 256, 0, st>>>(w, s.pair_class, s.pair_coff);

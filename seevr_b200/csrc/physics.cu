@@ -236,6 +236,7 @@ void setup_world(seevr_physics* h) {
     w.pairs = static_cast<uint32_t*>(P(SEEVR_B_COLLISION_PAIRS));
     w.sup_off = static_cast<const uint32_t*>(P(SEEVR_B_SUPPORT_OFFSET));
     w.sup_lut = static_cast<const uint32_t*>(P(SEEVR_B_SUPPORT_LOOKUP));
+    w.lut_off = h->s.lut_off;
     w.hull_range = P(SEEVR_B_HULL_RANGE) ? static_cast<const uint32_t*>(P(SEEVR_B_HULL_RANGE))
                                          : h->s.derived_hull_range;
     w.body_scene = h->body_scene;
@@ -335,6 +336,10 @@ uint64_t issue_frame(seevr_physics* h, uint32_t nb, uint32_t nv, uint32_t nhv, u
         World wc = w;
         wc.nv = render ? nv : 0u;
         n += launch_check_inputs(wc, uint32_t(h->b.bytes[SEEVR_B_SUPPORT_LOOKUP] / 4), st);
+    }
+    {
+        const Range r("phys/lut_alias");
+        n += launch_lut_alias(w, h->s, st);
     }
     for (uint32_t s = 0; s < substeps; ++s) {
         T.begin();
@@ -800,7 +805,9 @@ seevr_status seevr_physics_create(const seevr_bindings* b, const seevr_caps* cap
     ALLOC(h->s.pair_res1, c.max_pairs);
     ALLOC(h->s.pair_flag, c.max_pairs);
     ALLOC(h->s.pair_coff, c.max_pairs);
-    ALLOC(h->s.pair_class, 8);
+    ALLOC(h->s.pair_class, 2 * kPairClasses);
+    ALLOC(h->s.lut_rep, kLutHullMax);
+    ALLOC(h->s.lut_off, c.max_bodies);
     ALLOC(h->s.s_ra, size_t(c.max_contacts) * 3);
     ALLOC(h->s.s_rb, size_t(c.max_contacts) * 3);
     ALLOC(h->s.s_bias, c.max_contacts);
@@ -1224,6 +1231,7 @@ seevr_status seevr_physics_adjoint_substep(seevr_physics* h, uint32_t num_bodies
     n += launch_body_stage(w, h->k, kGravity | kAabb, dt, gravity[0], gravity[1], gravity[2], s);
     n += h->params.broadphase == SEEVR_BROADPHASE_LBVH ? launch_broadphase_lbvh(w, h->s, h->lb, s)
                                                        : launch_broadphase_n2(w, h->s, h->max_scene_bodies, s);
+    n += launch_lut_alias(w, h->s, s);
     n += launch_narrowphase_taped(w, h->k, h->s, a.ptape, a.ctape, s);
     n += launch_bundle_ranges(w, h->s, s);
     const Grads g{grads->pos, grads->quat, grads->vel, grads->omega, grads->friction};

@@ -670,9 +670,9 @@ NCU_CAPTURE = {
                          "duration_us": 57.3, "issue_active_pct": 48.8,
                          "warps_active_pct": 44.1, "lanes_per_inst": 30.9, "registers": 63},
     "phys/narrow_phase": {"kernel": "k_narrow<0, 7>", "skip": 910, "scale": "pairs",
-                          "dram_bytes_per_launch": 99364480, "duration_us": 134.6,
-                          "issue_active_pct": 25.1, "warps_active_pct": 28.7,
-                          "lanes_per_inst": 12.7, "registers": 72},
+                          "dram_bytes_per_launch": 97745024, "duration_us": 122.6,
+                          "issue_active_pct": 24.3, "warps_active_pct": 31.1,
+                          "lanes_per_inst": 12.6, "registers": 72},
     "phys/pgs_solve": {"kernel": "k_solver_warp", "skip": 910, "scale": "bodies",
                        "dram_bytes_per_launch": 10574720, "duration_us": 320.8,
                        "issue_active_pct": 8.4, "warps_active_pct": 4.9, "lanes_per_inst": 16.0,

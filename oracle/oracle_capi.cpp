@@ -313,8 +313,7 @@ void oracle_karras(const uint32_t* sorted, uint32_t n, uint32_t* left, uint32_t*
     std::copy(p.begin(), p.end(), parent);
 }
 
-float oracle_atan2f(float y, float x) { return oracle::seevr_atan2<float>(y, x); }
-double oracle_atan2d(double y, double x) { return oracle::seevr_atan2<double>(y, x); }
+uint32_t oracle_angle_bin64f(float y, float x) { return oracle::angle_bin64<float>(y, x); }
 
 int oracle_num_threads(void) {
 #ifdef _OPENMP

@@ -76,10 +76,8 @@ def _load():
     lib.oracle_morton.argtypes = [_f, C.c_uint32, _u, _f]
     lib.oracle_radix_sort.argtypes = [_u, C.c_uint32, _u, _u]
     lib.oracle_karras.argtypes = [_u, C.c_uint32, _u, _u, _u]
-    lib.oracle_atan2f.restype = C.c_float
-    lib.oracle_atan2f.argtypes = [C.c_float, C.c_float]
-    lib.oracle_atan2d.restype = C.c_double
-    lib.oracle_atan2d.argtypes = [C.c_double, C.c_double]
+    lib.oracle_angle_bin64f.restype = C.c_uint32
+    lib.oracle_angle_bin64f.argtypes = [C.c_float, C.c_float]
     lib.oracle_num_threads.restype = C.c_int
     return lib
 
@@ -258,9 +256,7 @@ def karras(sorted_codes: np.ndarray):
     return left, right, parent
 
 
-def atan2f(y: float, x: float) -> float:
-    return float(lib.oracle_atan2f(y, x))
-
-
-def atan2d(y: float, x: float) -> float:
-    return float(lib.oracle_atan2d(y, x))
+def angle_bin64(y: float, x: float) -> int:
+    """The support lookup's angle bin (0-63) of atan2(y, x) in [0, 2 pi),
+    FP32 (seevr_oracle.hpp angle_bin64)."""
+    return int(lib.oracle_angle_bin64f(y, x))

@@ -16,9 +16,13 @@
 //     order and contacts in pair order (the reference appends both with
 //     atomicAdd, physics.comp:465 and 404, so its own order varies run to
 //     run);
-//  2. GLSL atan(y,x) (physics.comp:136-140), whose precision the GLSL spec
-//     leaves to the implementation, is replaced by seevr_atan2 below, a
-//     Maclaurin-series arctangent with the pi/4 addition identity.
+//  2. the support lookup's bin of each axis angle, uint(atan(y,x) (+2 pi if
+//     negative) / 2 pi * 64) % 64 (physics.comp:136-147), is found without
+//     the angle: by quadrant and by comparing against the tangents of the
+//     bin boundaries (angle_bin64 below).  It is the same bin except for
+//     directions within rounding of a bin boundary, where the reference's
+//     own choice depends on its GLSL atan and division, both of
+//     implementation-defined precision.
 // FP32 instantiation compiled with -ffp-contract=off (no FMA), so every
 // expression rounds exactly as written; FP64 instantiation = error reference.
 #pragma once
@@ -70,39 +74,40 @@ template <class R> inline V3<R> mulT(const M3<R>& m, V3<R> v) {
     return {dot(m.c0, v), dot(m.c1, v), dot(m.c2, v)};
 }
 
-// Arctangent of y/x in (-pi, pi] (replaces GLSL atan(y,x)).  |t| <= 1 after
-// octant folding; for t > tan(pi/8) the identity atan(t) = pi/4 +
-// atan((t-1)/(t+1)) brings |u| <= tan(pi/8) ~ 0.4142, where the Maclaurin
-// series atan(u) = sum (-1)^k u^(2k+1)/(2k+1), truncated after u^19, is
-// accurate to below 1e-9.  atan2(0,0) = 0.
+// tan(j*pi/32), j = 0..15, rounded to float: the boundaries of the 16 bins
+// of one quadrant.  The CUDA kernel holds the same float values.
+constexpr float kTanBin[16] = {0.0f,       0.0984914f, 0.19891237f, 0.3033467f,
+                               0.41421357f, 0.53451115f, 0.6681786f,  0.8206788f,
+                               1.0f,        1.2185035f,  1.4966058f,  1.8708684f,
+                               2.4142137f,  3.2965581f,  5.0273395f,  10.153171f};
+
+// Bin k of 64 equal bins of the angle atan2(y, x) taken in [0, 2 pi) (bin k
+// covers [k pi/32, (k+1) pi/32)), found without the angle.  The quadrant
+// comes from the signs; (u, v), the direction rotated into the first
+// quadrant (u > 0, v >= 0), has angle phi = atan(v/u) in [0, pi/2), and
+// phi >= j pi/32 exactly when v >= u tan(j pi/32), so a binary search over
+// the 15 tangents gives the bin within the quadrant.  (0,0) -> bin 0, as
+// the reference's atan(0,0) = 0.
 template <class R>
-inline R seevr_atan2(R y, R x) {
-    const R ax = std::fabs(x), ay = std::fabs(y);
-    const R mx = ax < ay ? ay : ax;
-    const R mn = ax < ay ? ax : ay;
-    if (mx == R(0)) return R(0);
-    R t = mn / mx;
-    R base = R(0);
-    if (t > R(0.41421356237309503)) {
-        t = (t - R(1)) / (t + R(1));
-        base = R(0.78539816339744831);
+inline uint32_t angle_bin64(R y, R x) {
+    R u, v;
+    uint32_t q;
+    if (x > R(0) && y >= R(0)) {
+        q = 0, u = x, v = y;
+    } else if (x <= R(0) && y > R(0)) {
+        q = 16, u = y, v = -x;
+    } else if (x < R(0) && y <= R(0)) {
+        q = 32, u = -x, v = -y;
+    } else if (x >= R(0) && y < R(0)) {
+        q = 48, u = -y, v = x;
+    } else {
+        return 0;
     }
-    const R u2 = t * t;
-    R p = R(1) / R(19);
-    p = R(1) / R(17) - u2 * p;
-    p = R(1) / R(15) - u2 * p;
-    p = R(1) / R(13) - u2 * p;
-    p = R(1) / R(11) - u2 * p;
-    p = R(1) / R(9) - u2 * p;
-    p = R(1) / R(7) - u2 * p;
-    p = R(1) / R(5) - u2 * p;
-    p = R(1) / R(3) - u2 * p;
-    p = R(1) - u2 * p;
-    R r = base + t * p;
-    if (ay > ax) r = R(1.5707963267948966) - r;
-    if (x < R(0)) r = R(3.1415926535897931) - r;
-    if (y < R(0)) r = -r;
-    return r;
+    uint32_t j = v >= u * R(kTanBin[8]) ? 8u : 0u;
+    if (v >= u * R(kTanBin[j + 4])) j += 4;
+    if (v >= u * R(kTanBin[j + 2])) j += 2;
+    if (v >= u * R(kTanBin[j + 1])) j += 1;
+    return q + j;
 }
 
 // Input arrays, indexed like the physics.comp bindings (physics.comp:16-57).
@@ -308,16 +313,14 @@ class Physics {
             return p + mul(Rm, bv);
         }
         ops.support_lookup++;
-        const R angles[3] = {seevr_atan2(ld.z, ld.y), seevr_atan2(ld.z, ld.x), seevr_atan2(ld.y, ld.x)};
-        const R two_pi = R(6.2831853);
+        // the bins of atan(z,y), atan(z,x), atan(y,x) (X, Y, Z axes)
+        const uint32_t bins[3] = {angle_bin64(ld.z, ld.y), angle_bin64(ld.z, ld.x),
+                                  angle_bin64(ld.y, ld.x)};
         R best = R(-1e10);
         V3<R> bv = {R(0), R(0), R(0)};
         uint32_t chosen = 0xFFFFFFFFu;
         for (uint32_t ax = 0; ax < 3; ++ax) {
-            R a = angles[ax];
-            if (a < R(0)) a += two_pi;
-            const R bin_f = a / two_pi * R(64);
-            const uint32_t b0 = uint32_t(bin_f) % 64u;
+            const uint32_t b0 = bins[ax];
             const uint32_t b1 = (b0 + 1) % 64u;
             const V3<R> v0 = get3(hull, vs + sup_lut[lk + ax * 64 + b0]);
             const R d0 = dot(v0, ld);

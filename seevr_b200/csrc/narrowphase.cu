@@ -69,26 +69,20 @@ __device__ __forceinline__ Shape load_shape(const World& w, uint32_t b, const Po
 __device__ __forceinline__ f3 support_rp(const World& w, const Shape& s, const m3& R, f3 pos,
                                          f3 d, uint32_t& chosen) {
     const f3 ld = mulT(R, d);
-    const bool lut = s.lk != 0;
-    float a0 = 0.f, a1 = 0.f, a2 = 0.f;
-    if (lut) {
-        a0 = seevr_atan2f(ld.z, ld.y);  // X axis
-        a1 = seevr_atan2f(ld.z, ld.x);  // Y axis
-        a2 = seevr_atan2f(ld.y, ld.x);  // Z axis
-    }
     float best = -1e10f;
     f3 bv = mk(0.f, 0.f, 0.f);
     chosen = kNone;  // no vertex beat -1e10: the support point is the body position
-    if (lut) {
-        // the six lookup entries, then the six candidate vertices, all loads
-        // of a level in flight together; compared in the reference's order
+    if (s.lk != 0) {
+        // the angle bins of the X, Y, Z axes (atan(z,y), atan(z,x),
+        // atan(y,x)); then the six lookup entries, then the six candidate
+        // vertices, all loads of a level in flight together; compared in
+        // the reference's order
+        const uint32_t bins[3] = {angle_bin64(ld.z, ld.y), angle_bin64(ld.z, ld.x),
+                                  angle_bin64(ld.y, ld.x)};
         uint32_t idx[6];
 #pragma unroll
         for (uint32_t ax = 0; ax < 3; ++ax) {
-            float a = ax == 0 ? a0 : (ax == 1 ? a1 : a2);
-            if (a < 0.0f) a += 6.2831853f;
-            const float bin_f = a / 6.2831853f * 64.0f;
-            const uint32_t b0 = uint32_t(bin_f) % 64u;
+            const uint32_t b0 = bins[ax];
             idx[2 * ax] = w.sup_lut[s.lk + ax * 64u + b0];
             idx[2 * ax + 1] = w.sup_lut[s.lk + ax * 64u + (b0 + 1u) % 64u];
         }
@@ -682,7 +676,7 @@ __global__ void __launch_bounds__(128)
 
 // ---- pair order by support path ---------------------------------------------
 // A warp's lanes run their pairs' support calls together; a shape with a
-// support lookup (lk != 0) takes three arctangents and six candidates, one
+// support lookup (lk != 0) takes three angle bins and six candidates, one
 // without walks all its hull vertices.  Taking the pairs grouped by the two
 // shapes' paths (4 classes) keeps a warp's lanes on one path, and within a
 // class the broadphase's order, in which neighbouring pairs share a body

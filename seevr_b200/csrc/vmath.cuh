@@ -86,38 +86,50 @@ __device__ __forceinline__ m3 ld_m3(const float* p, uint32_t i) {
     return m;
 }
 
-// Arctangent of y/x in (-pi, pi], replacing GLSL atan(y,x)
-// (physics.comp:136-140).  After folding to t = min/max in [0,1], values
-// above tan(pi/8) use atan(t) = pi/4 + atan((t-1)/(t+1)), leaving
-// |u| <= 0.4142 for the Maclaurin series sum (-1)^k u^(2k+1)/(2k+1)
-// truncated after u^19 (truncation error < 1e-9).  atan2(0,0) = 0.
-__device__ __forceinline__ float seevr_atan2f(float y, float x) {
-    const float ax = fabsf(x), ay = fabsf(y);
-    const float mx = ax < ay ? ay : ax;
-    const float mn = ax < ay ? ax : ay;
-    if (mx == 0.0f) return 0.0f;
-    float t = mn / mx;
-    float base = 0.0f;
-    if (t > 0.41421356237309503f) {
-        t = (t - 1.0f) / (t + 1.0f);
-        base = 0.78539816339744831f;
+// The support lookup's bin of an axis angle (physics.comp:136-147: atan(y,x),
+// plus 2 pi when negative, / 2 pi * 64, truncated, mod 64), found without
+// the angle.  The quadrant comes from the signs; (u, v), the direction
+// rotated into the first quadrant (u > 0, v >= 0), has angle atan(v/u) in
+// [0, pi/2), which is at least j pi/32 exactly when v >= u tan(j pi/32), so
+// a binary search over the tangents of the 15 inner boundaries gives the
+// bin within the quadrant.  The same bin as the angle's except within
+// rounding of a boundary (where the reference's own GLSL atan and division
+// are of implementation-defined precision); (0,0) -> bin 0, as atan(0,0)
+// = 0.  Four multiplies and compares instead of an arctangent and two
+// divisions.  The thresholds are tan(j pi/32) rounded to float.
+__device__ __forceinline__ uint32_t angle_bin64(float y, float x) {
+    float u, v;
+    uint32_t q;
+    if (x > 0.0f && y >= 0.0f) {
+        q = 0, u = x, v = y;
+    } else if (x <= 0.0f && y > 0.0f) {
+        q = 16, u = y, v = -x;
+    } else if (x < 0.0f && y <= 0.0f) {
+        q = 32, u = -x, v = -y;
+    } else if (x >= 0.0f && y < 0.0f) {
+        q = 48, u = -y, v = x;
+    } else {
+        return 0;
     }
-    const float u2 = t * t;
-    float p = 1.0f / 19.0f;
-    p = 1.0f / 17.0f - u2 * p;
-    p = 1.0f / 15.0f - u2 * p;
-    p = 1.0f / 13.0f - u2 * p;
-    p = 1.0f / 11.0f - u2 * p;
-    p = 1.0f / 9.0f - u2 * p;
-    p = 1.0f / 7.0f - u2 * p;
-    p = 1.0f / 5.0f - u2 * p;
-    p = 1.0f / 3.0f - u2 * p;
-    p = 1.0f - u2 * p;
-    float r = base + t * p;
-    if (ay > ax) r = 1.5707963267948966f - r;
-    if (x < 0.0f) r = 3.1415926535897931f - r;
-    if (y < 0.0f) r = -r;
-    return r;
+    // tan(j pi/32) for j = 4, 8, 12; then j + 2 in {2, 6, 10, 14}; then the odd j
+    const bool h8 = v >= u * 1.0f;
+    const bool h4 = v >= u * (h8 ? 2.4142137f : 0.41421357f);
+    const uint32_t j4 = (h8 ? 8u : 0u) + (h4 ? 4u : 0u);
+    const float t2 = h8 ? (h4 ? 5.0273395f : 1.4966058f) : (h4 ? 0.6681786f : 0.19891237f);
+    const bool h2 = v >= u * t2;
+    const uint32_t j2 = j4 + (h2 ? 2u : 0u);
+    float t1;
+    switch (j2) {  // tan((j2 + 1) pi/32)
+        case 0: t1 = 0.0984914f; break;
+        case 2: t1 = 0.3033467f; break;
+        case 4: t1 = 0.53451115f; break;
+        case 6: t1 = 0.8206788f; break;
+        case 8: t1 = 1.2185035f; break;
+        case 10: t1 = 1.8708684f; break;
+        case 12: t1 = 3.2965581f; break;
+        default: t1 = 10.153171f; break;
+    }
+    return q + j2 + (v >= u * t1 ? 1u : 0u);
 }
 
 }  // namespace seevr

@@ -130,17 +130,34 @@ def test_static_static_contact_skipped():  # KAT 7
     assert out["ops"]["pgs_contact_iters"] == 0
 
 
-def test_atan2_accuracy():
+def test_angle_bins_match_the_angle():
+    """The support lookup's bin (physics.comp:136-147: atan(y,x), +2 pi when
+    negative, / 2 pi * 64, truncated, mod 64) found by quadrant and tangent
+    comparisons equals the bin of the exact angle, except within float
+    rounding of a bin boundary."""
     rng = np.random.default_rng(1)
     pts = rng.normal(size=(20000, 2)) * rng.choice([1e-3, 1, 1e3], size=(20000, 1))
-    for y, x in pts[:2000]:
-        ref = math.atan2(y, x)
-        assert abs(pyoracle.atan2d(y, x) - ref) < 1e-12 + 1e-9 * abs(ref)
-        assert abs(pyoracle.atan2f(np.float32(y), np.float32(x)) -
-                   math.atan2(np.float32(y), np.float32(x))) < 6e-7
-    assert pyoracle.atan2f(0.0, 0.0) == 0.0
-    assert abs(pyoracle.atan2f(0.0, -1.0) - math.pi) < 1e-6
-    assert abs(pyoracle.atan2f(-1.0, 0.0) + math.pi / 2) < 1e-6
+    near = 0
+    for y, x in pts.astype(np.float32):
+        a = math.atan2(float(y), float(x))
+        if a < 0:
+            a += 2 * math.pi
+        f = a / (2 * math.pi) * 64
+        want = int(f) % 64
+        got = pyoracle.angle_bin64(y, x)
+        if got != want:
+            # only at a boundary: the exact angle is within 1e-6 of a bin edge
+            assert abs(f - round(f)) < 64e-6 / (2 * math.pi), (y, x, got, want)
+            assert got in ((want + 1) % 64, (want - 1) % 64)
+            near += 1
+    assert near < 20
+    # axis directions and the origin, as the reference's atan(0,0) = 0
+    assert [pyoracle.angle_bin64(y, x) for y, x in
+            ((0, 1), (1, 0), (0, -1), (-1, 0), (0, 0), (1, 1), (-1, -1))] == [0, 16, 32, 48, 0, 8, 40]
+    # every bin is reached, in order around the circle
+    th = (np.arange(64) + 0.5) * (2 * math.pi / 64)
+    assert [pyoracle.angle_bin64(np.float32(math.sin(t)), np.float32(math.cos(t))) for t in th] == \
+        list(range(64))
 
 
 def test_fp32_vs_fp64_one_step():

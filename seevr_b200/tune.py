@@ -14,11 +14,13 @@ from __future__ import annotations
 
 from typing import Callable
 
+# scene groups first: the shapes of the other stages' kernels are best
+# chosen at the group size they will run at
 DEFAULT_CANDIDATES = {
+    "scene_groups": [1, 2, 4, 6, 8],
     "narrow_blocks_per_sm": [4, 5, 6, 7],
     "broad_tile_rows": [32, 64, 128, 256],
     "bundle_bodies": [256, 512, 1024],
-    "scene_groups": [1, 2, 3, 4],
 }
 
 

@@ -13,7 +13,12 @@
 //
 // The reference reduces AABBs with a thread-0 serial loop per 256-vertex
 // workgroup and a multi-launch cascade; min/max are exact in any order, so
-// the reductions here give the same values in one pass.  Hull vertex
+// the reductions here give the same values in one pass.  They reduce R v
+// and add the position once: rounding is monotone, so the least (greatest)
+// of p + R v_i, each rounded, is p + the least (greatest) R v_i, rounded.
+// fminf/fmaxf (one instruction) stand for GLSL min/max (y < x ? y : x);
+// with no NaN among finite vertices the two differ only in which zero they
+// return for min(-0, +0), and every later test treats the two zeros alike.  Hull vertex
 // ownership: body b owns [hull_start, hull_start+hull_count), which is what
 // the reference's binary search (physics.comp:695-703) yields for
 // contiguous hull ranges.
@@ -43,6 +48,9 @@ constexpr uint32_t kBodyThreads = 256;
 constexpr uint32_t kSmallVerts = 32;
 // Vertices per lane per round of loads in the warp phase.
 constexpr uint32_t kLaneVerts = 10;
+
+__device__ __forceinline__ f3 fmin3(f3 a, f3 b) { return f3{fminf(a.x, b.x), fminf(a.y, b.y), fminf(a.z, b.z)}; }
+__device__ __forceinline__ f3 fmax3(f3 a, f3 b) { return f3{fmaxf(a.x, b.x), fmaxf(a.y, b.y), fmaxf(a.z, b.z)}; }
 
 // Integrate (physics.comp:586-604) and gravity (418-428) of body b, in the
 // reference's arithmetic; returns the (possibly updated) pose.
@@ -135,13 +143,13 @@ __global__ void __launch_bounds__(kBodyThreads) k_body_stage(World w, Consts k, 
             f3 mn = mk(inf, inf, inf), mx = mk(-inf, -inf, -inf);
 #pragma unroll 8
             for (uint32_t i = 0; i < hc; ++i) {
-                const f3 wv = add(p, mul(R, ld3(w.hull, hs + i)));
-                mn = vmin(mn, wv);
-                mx = vmax(mx, wv);
+                const f3 rv = mul(R, ld3(w.hull, hs + i));
+                mn = fmin3(mn, rv);
+                mx = fmax3(mx, rv);
             }
             if (hc > 0) {
-                st3(w.aabb_min, b, mn);
-                st3(w.aabb_max, b, mx);
+                st3(w.aabb_min, b, add(p, mn));
+                st3(w.aabb_max, b, add(p, mx));
             }
         }
 
@@ -186,24 +194,24 @@ __global__ void __launch_bounds__(kBodyThreads) k_body_stage(World w, Consts k, 
 #pragma unroll
                     for (uint32_t j = 0; j < kLaneVerts; ++j) {
                         if (c0 + lane + 32u * j < hc) {
-                            const f3 wv = add(p, mul(R, v[j]));
-                            mn = vmin(mn, wv);
-                            mx = vmax(mx, wv);
+                            const f3 rv = mul(R, v[j]);
+                            mn = fmin3(mn, rv);
+                            mx = fmax3(mx, rv);
                         }
                     }
                 }
 #pragma unroll
                 for (int off = 16; off > 0; off >>= 1) {
-                    mn.x = gmin(mn.x, __shfl_xor_sync(full, mn.x, off));
-                    mn.y = gmin(mn.y, __shfl_xor_sync(full, mn.y, off));
-                    mn.z = gmin(mn.z, __shfl_xor_sync(full, mn.z, off));
-                    mx.x = gmax(mx.x, __shfl_xor_sync(full, mx.x, off));
-                    mx.y = gmax(mx.y, __shfl_xor_sync(full, mx.y, off));
-                    mx.z = gmax(mx.z, __shfl_xor_sync(full, mx.z, off));
+                    mn.x = fminf(mn.x, __shfl_xor_sync(full, mn.x, off));
+                    mn.y = fminf(mn.y, __shfl_xor_sync(full, mn.y, off));
+                    mn.z = fminf(mn.z, __shfl_xor_sync(full, mn.z, off));
+                    mx.x = fmaxf(mx.x, __shfl_xor_sync(full, mx.x, off));
+                    mx.y = fmaxf(mx.y, __shfl_xor_sync(full, mx.y, off));
+                    mx.z = fmaxf(mx.z, __shfl_xor_sync(full, mx.z, off));
                 }
                 if (lane == 0) {
-                    st3(w.aabb_min, bb, mn);
-                    st3(w.aabb_max, bb, mx);
+                    st3(w.aabb_min, bb, add(p, mn));
+                    st3(w.aabb_max, bb, add(p, mx));
                 }
             }
         }

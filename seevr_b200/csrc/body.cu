@@ -16,9 +16,12 @@
 // the reductions here give the same values in one pass.  They reduce R v
 // and add the position once: rounding is monotone, so the least (greatest)
 // of p + R v_i, each rounded, is p + the least (greatest) R v_i, rounded.
-// fminf/fmaxf (one instruction) stand for GLSL min/max (y < x ? y : x);
-// with no NaN among finite vertices the two differ only in which zero they
-// return for min(-0, +0), and every later test treats the two zeros alike.  Hull vertex
+// fminf/fmaxf (one instruction) stand for GLSL min/max (y < x ? y : x):
+// on numbers the two differ only in which zero they return for
+// min(-0, +0), and every later test treats the two zeros alike; a NaN pose
+// gives NaN bounds as the reference's reduction does (aabb_bound).  (A NaN
+// among a hull's own vertices is skipped here, where the reference keeps
+// it when it is the first vertex of its pass.)  Hull vertex
 // ownership: body b owns [hull_start, hull_start+hull_count), which is what
 // the reference's binary search (physics.comp:695-703) yields for
 // contiguous hull ranges.
@@ -49,6 +52,17 @@ constexpr uint32_t kSmallVerts = 32;
 // Vertices per lane per round of loads in the warp phase.
 constexpr uint32_t kLaneVerts = 10;
 
+// p + the reduced bound of one axis; NaN when the position or the
+// rotation's row on that axis has a NaN.  Then every p + R v of the axis is
+// NaN, and the reference's reduction, which starts from the first vertex's
+// value and keeps it against NaN (min(x, y) = y < x ? y : x), ends at NaN.
+__device__ __forceinline__ float aabb_axis(float p, float r0, float r1, float r2, float m) {
+    return (p != p || r0 != r0 || r1 != r1 || r2 != r2) ? __int_as_float(0x7fffffff) : p + m;
+}
+__device__ __forceinline__ f3 aabb_bound(f3 p, const m3& R, f3 m) {
+    return f3{aabb_axis(p.x, R.c0.x, R.c1.x, R.c2.x, m.x), aabb_axis(p.y, R.c0.y, R.c1.y, R.c2.y, m.y),
+              aabb_axis(p.z, R.c0.z, R.c1.z, R.c2.z, m.z)};
+}
 __device__ __forceinline__ f3 fmin3(f3 a, f3 b) { return f3{fminf(a.x, b.x), fminf(a.y, b.y), fminf(a.z, b.z)}; }
 __device__ __forceinline__ f3 fmax3(f3 a, f3 b) { return f3{fmaxf(a.x, b.x), fmaxf(a.y, b.y), fmaxf(a.z, b.z)}; }
 
@@ -148,8 +162,8 @@ __global__ void __launch_bounds__(kBodyThreads) k_body_stage(World w, Consts k, 
                 mx = fmax3(mx, rv);
             }
             if (hc > 0) {
-                st3(w.aabb_min, b, add(p, mn));
-                st3(w.aabb_max, b, add(p, mx));
+                st3(w.aabb_min, b, aabb_bound(p, R, mn));
+                st3(w.aabb_max, b, aabb_bound(p, R, mx));
             }
         }
 
@@ -210,8 +224,8 @@ __global__ void __launch_bounds__(kBodyThreads) k_body_stage(World w, Consts k, 
                     mx.z = fmaxf(mx.z, __shfl_xor_sync(full, mx.z, off));
                 }
                 if (lane == 0) {
-                    st3(w.aabb_min, bb, add(p, mn));
-                    st3(w.aabb_max, bb, add(p, mx));
+                    st3(w.aabb_min, bb, aabb_bound(p, R, mn));
+                    st3(w.aabb_max, bb, aabb_bound(p, R, mx));
                 }
             }
         }

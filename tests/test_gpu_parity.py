@@ -9,8 +9,9 @@ import numpy as np
 import pytest
 
 import pyoracle
-from helpers import DT, G, assert_bit_exact, gpu_run, max_rel_err
-from seevr_b200 import Caps, Data, SeevrError, SOLVER_SEQUENTIAL, SOLVER_WAVEFRONT, make_params
+from helpers import DT, G, assert_bit_exact, gpu_run, max_rel_err, read_back
+from seevr_b200 import (Caps, Data, Physics, SeevrError, SOLVER_SEQUENTIAL, SOLVER_WAVEFRONT,
+                        make_params)
 
 pytestmark = pytest.mark.gpu
 
@@ -242,3 +243,37 @@ def test_profile_mode_and_launch_count(cuda):
     assert prof.ms[1] > 0 and prof.ms[2] > 0 and prof.ms[5] > 0
     assert ph.kernel_launches >= 10 * 8
     ph.deinit()
+
+
+def test_batch_with_a_nan_body_matches_oracle(cuda):
+    """A body whose quaternion is NaN gets NaN bounds, as the reference's
+    reduction (seeded with the first vertex's NaN) does, and the reference's
+    predicate then counts it as overlapping every body of its scene.  Every
+    output, NaNs included, equals the oracle's."""
+    import torch
+
+    d = Data.batch(num_scenes=16, min_bodies=8, max_bodies=64, seed_base=77)
+    off = d.scene_body_offset()
+    k = int(off[3]) + 1
+    a = d.arrays()
+    a["body_quat"][k] = np.nan
+    ref = pyoracle.run(a, frames=2, substeps=10, dt=DT, gravity=G, pgs_iterations=4,
+                       max_pairs=Caps.for_data(d).max_pairs,
+                       max_contacts=Caps.for_data(d).max_contacts)
+    buf = d.upload(cuda)
+    buf.tensors["body_quat"][4 * k: 4 * k + 4] = float("nan")
+    ph = Physics(buf, make_params(pgs_iterations=4))
+    for _ in range(2):
+        ph.step(buf.num_bodies, buf.num_vertices, buf.num_hull_verts, 10, DT, G)
+    torch.cuda.synchronize()
+    got = read_back(buf)
+    ph.deinit()
+    assert np.isnan(got["quat"][k]).all() and np.isnan(got["aabb_min"][k]).all()
+    assert ref["num_pairs"] > 0
+    assert (got["num_pairs"], got["num_contacts"]) == (ref["num_pairs"], ref["num_contacts"])
+    for key in ("pos", "quat", "vel", "omega", "aabb_min", "aabb_max", "pairs", "c_pos",
+                "c_normal", "c_pen", "lambda", "verts"):
+        g = np.asarray(got[key])
+        r = np.asarray(ref[key]).astype(g.dtype)
+        assert g.shape == r.shape, key
+        assert np.array_equal(g, r, equal_nan=g.dtype.kind == "f"), key

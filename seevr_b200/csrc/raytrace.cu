@@ -32,6 +32,7 @@
 //     double and rounded to float.
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <string>
 
 #include "../../include/seevr.h"
@@ -367,6 +368,32 @@ __global__ void k_rt_resolve(RtArgs g, const float* __restrict__ samples) {
     }
 }
 
+// The work arrays come from a memory pool of the library's own per device,
+// which keeps freed memory for the next frame (the device's default pool
+// returns it to the system at every synchronisation, and mapping it again
+// costs milliseconds per frame).
+cudaMemPool_t work_pool(int dev) {
+    static std::mutex mu;
+    static cudaMemPool_t pools[64] = {};
+    if (dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!pools[dev]) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t p = nullptr;
+        if (cudaMemPoolCreate(&p, &props) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        uint64_t keep = ~uint64_t(0);
+        cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+        pools[dev] = p;
+    }
+    return pools[dev];
+}
+
 }  // namespace
 }  // namespace seevr
 
@@ -438,7 +465,9 @@ seevr_status seevr_raytrace(const seevr_rt_bindings* b, const seevr_rt_params* p
     const size_t node_bytes = size_t(nnodes) * sizeof(NodeP), tri_bytes = size_t(p->num_triangles) * sizeof(TriP);
     const size_t sample_bytes = size_t(nitems) * 3 * sizeof(float);
     void* work = nullptr;
-    cudaError_t e = cudaMallocAsync(&work, node_bytes + tri_bytes + sample_bytes + 16, st);
+    const cudaMemPool_t pool = work_pool(dev);
+    cudaError_t e = pool ? cudaMallocFromPoolAsync(&work, node_bytes + tri_bytes + sample_bytes + 16, pool, st)
+                         : cudaMallocAsync(&work, node_bytes + tri_bytes + sample_bytes + 16, st);
     if (e != cudaSuccess) {
         cudaGetLastError();
         set_last_error(std::string("raytrace work arrays: ") + cudaGetErrorString(e));

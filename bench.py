@@ -643,7 +643,7 @@ def plain_dropin(a, d, state, dev):
 # Figures of single-kernel ncu captures (not measured by this run): per
 # main kernel of each stage, DRAM bytes (read + write) per launch and issue
 # and warp utilisation, captured on a 1,024-scene batch of the same
-# distributions (123,288 bodies, 118,511 pairs and 28,215 contacts at the
+# distributions (123,288 bodies, 118,480 pairs and 28,231 contacts at the
 # captured substep) and scaled to a run by its bodies (body stage,
 # broadphase, solver, render vertices) or pairs (narrowphase).  Captured as
 #   ncu --metrics <NCU_METRICS> --clock-control none -k regex:<kernel>
@@ -659,27 +659,27 @@ NCU_METRICS = ("gpu__time_duration.sum,dram__bytes_read.sum,dram__bytes_write.su
                "smsp__thread_inst_executed_per_inst_executed.ratio,lts__t_sector_hit_rate.pct,"
                "l1tex__t_sector_hit_rate.pct,launch__registers_per_thread,"
                "gpu__dram_throughput.avg.pct_of_peak_sustained_elapsed")
-NCU_CAPTURED = {"bodies": 123288, "pairs": 118511, "contacts": 28215}
+NCU_CAPTURED = {"bodies": 123288, "pairs": 118480, "contacts": 28231}
 NCU_CAPTURE = {
     "phys/aabb": {"kernel": "k_body_stage", "skip": 1001, "scale": "bodies",
-                  "dram_bytes_per_launch": 247369472, "duration_us": 71.1,
-                  "issue_active_pct": 46.3, "warps_active_pct": 35.7, "lanes_per_inst": 29.2,
-                  "registers": 63},
+                  "dram_bytes_per_launch": 247077504, "duration_us": 60.7,
+                  "issue_active_pct": 45.5, "warps_active_pct": 37.9, "lanes_per_inst": 27.9,
+                  "registers": 64},
     "phys/broad_phase": {"kernel": "k_broad_tile<0> + k_broad_tile<1>", "skip": 1820,
-                         "scale": "bodies", "dram_bytes_per_launch": 9496832,
-                         "duration_us": 57.3, "issue_active_pct": 48.8,
-                         "warps_active_pct": 44.1, "lanes_per_inst": 30.9, "registers": 63},
+                         "scale": "bodies", "dram_bytes_per_launch": 10462720,
+                         "duration_us": 57.4, "issue_active_pct": 40.5,
+                         "warps_active_pct": 56.6, "lanes_per_inst": 29.5, "registers": 63},
     "phys/narrow_phase": {"kernel": "k_narrow<0, 7>", "skip": 910, "scale": "pairs",
-                          "dram_bytes_per_launch": 97745024, "duration_us": 122.6,
-                          "issue_active_pct": 24.3, "warps_active_pct": 31.1,
-                          "lanes_per_inst": 12.6, "registers": 72},
+                          "dram_bytes_per_launch": 97402880, "duration_us": 120.2,
+                          "issue_active_pct": 24.0, "warps_active_pct": 32.2,
+                          "lanes_per_inst": 12.1, "registers": 72},
     "phys/pgs_solve": {"kernel": "k_solver_warp", "skip": 910, "scale": "bodies",
-                       "dram_bytes_per_launch": 10574720, "duration_us": 320.8,
-                       "issue_active_pct": 8.4, "warps_active_pct": 4.9, "lanes_per_inst": 16.0,
-                       "registers": 127},
+                       "dram_bytes_per_launch": 10579712, "duration_us": 316.9,
+                       "issue_active_pct": 8.8, "warps_active_pct": 2.8, "lanes_per_inst": 15.9,
+                       "registers": 124},
     "phys/render_verts": {"kernel": "k_render_verts", "skip": 91, "scale": "bodies",
-                          "dram_bytes_per_launch": 393891200, "duration_us": 97.6,
-                          "issue_active_pct": 36.3, "warps_active_pct": 39.7,
+                          "dram_bytes_per_launch": 393440640, "duration_us": 97.5,
+                          "issue_active_pct": 36.4, "warps_active_pct": 39.8,
                           "lanes_per_inst": 30.0, "registers": 62},
 }
 

@@ -737,7 +737,10 @@ __global__ void k_lut_reps(World w, uint32_t* __restrict__ rep) {
     for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < w.nb; b += gridDim.x * blockDim.x) {
         if (w.sup_off[b] == 0u) continue;
         const uint32_t hc = w.hull_range[size_t(b) * 2 + 1];
-        if (hc < kLutHullMax) atomicMin(&rep[hc], b);
+        // most bodies find a smaller one already there: a plain read first
+        // keeps them off the contended word
+        if (hc < kLutHullMax && b < *reinterpret_cast<volatile uint32_t*>(&rep[hc]))
+            atomicMin(&rep[hc], b);
     }
 }
 

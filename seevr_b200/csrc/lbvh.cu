@@ -412,19 +412,38 @@ __device__ __forceinline__ void traverse(const World& w, const LbvhView& t, uint
 
 // Rows of dynamic bodies, one thread each; static bodies' rows (a ground
 // box overlapping thousands of bodies) are left to k_lbvh_static_rows and
-// listed here.
+// listed here.  A row of at most kRowCache partners is kept, sorted, in
+// row_cache, so the write pass copies it instead of traversing again.
+// Threads take bodies in Morton order (the tree's leaf order), so a warp's
+// bodies are neighbours whose traversals visit the same nodes.
 __global__ void k_lbvh_count(World w, LbvhView t, uint32_t* __restrict__ row_count, uint32_t* err,
-                             uint32_t* static_list, uint32_t* static_count) {
+                             uint32_t* static_list, uint32_t* static_count,
+                             uint32_t* __restrict__ row_cache) {
     if (halted(err)) return;  // the tree was not built
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= w.nb) return;
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= w.nb) return;
+    const uint32_t i = w.nb >= 2 ? t.vals[q] : q;
     if (w.inv_mass[i] <= 0.0f) {
         static_list[atomicAdd(static_count, 1u)] = i;
         return;
     }
     uint32_t c = 0;
-    if (w.nb >= 2) traverse(w, t, i, i, err, [&](uint32_t) { ++c; });
+    uint32_t buf[kRowCache];
+    if (w.nb >= 2)
+        traverse(w, t, i, i, err, [&](uint32_t j) {
+            if (c < kRowCache) {  // insertion into the ascending buffer
+                uint32_t pos = c;
+                while (pos > 0 && buf[pos - 1] > j) {
+                    buf[pos] = buf[pos - 1];
+                    --pos;
+                }
+                buf[pos] = j;
+            }
+            ++c;
+        });
     row_count[i] = c;
+    if (c <= kRowCache)
+        for (uint32_t k = 0; k < c; ++k) row_cache[size_t(i) * kRowCache + k] = buf[k];
 }
 
 // Rows of static bodies, one block each: a breadth-first traversal whose
@@ -499,15 +518,26 @@ __global__ void __launch_bounds__(256)
     }
 }
 
-// Writes row i's pairs at row_off[i] in ascending j: rows are emitted in
-// chunks of up to kRowBuf smallest remaining j, one traversal per chunk.
+// Writes row i's pairs at row_off[i] in ascending j: a row the count pass
+// kept is copied; longer rows are emitted in chunks of up to kRowBuf
+// smallest remaining j, one traversal per chunk.
 __global__ void k_lbvh_write(World w, LbvhView t, const uint32_t* __restrict__ row_count,
-                             const uint32_t* __restrict__ row_off, uint32_t* err) {
+                             const uint32_t* __restrict__ row_off, uint32_t* err,
+                             const uint32_t* __restrict__ row_cache) {
     if (halted(err)) return;  // the tree or the row offsets are not valid
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= w.nb || w.inv_mass[i] <= 0.0f) return;  // static rows: k_lbvh_static_rows
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;  // Morton order, as the count
+    if (q >= w.nb) return;
+    const uint32_t i = w.nb >= 2 ? t.vals[q] : q;
+    if (w.inv_mass[i] <= 0.0f) return;  // static rows: k_lbvh_static_rows
     uint32_t remaining = row_count[i];
     uint32_t slot = row_off[i];
+    if (remaining <= kRowCache) {
+        for (uint32_t k = 0; k < remaining && slot < w.max_pairs; ++k, ++slot) {
+            w.pairs[size_t(slot) * 2] = i;
+            w.pairs[size_t(slot) * 2 + 1] = row_cache[size_t(i) * kRowCache + k];
+        }
+        return;
+    }
     uint32_t lo = i;
     while (remaining > 0 && slot < w.max_pairs) {
         uint32_t buf[kRowBuf];
@@ -593,12 +623,13 @@ int launch_broadphase_lbvh(const World& w, const Scratch& sc, const LbvhScratch&
     LbvhView t{s.node_min, s.node_max, s.left, s.right, s.vals_sorted};
     cudaMemsetAsync(s.static_count, 0, sizeof(uint32_t), st);
     k_lbvh_count<<<blocks_for(n, 128), 128, 0, st>>>(w, t, sc.row_count, &sc.status[0],
-                                                     s.static_list, s.static_count);
+                                                     s.static_list, s.static_count, s.row_cache);
     k_lbvh_static_rows<false><<<kStaticBlocks, 256, 0, st>>>(w, t, sc.row_count, nullptr,
                                                             s.static_list, s.static_count, s.bfs);
     launch_exclusive_scan(sc.row_count, sc.row_off, nullptr, n, &w.counters[0], w.max_pairs,
                           kFlagPairOverflow, sc, st);
-    k_lbvh_write<<<blocks_for(n, 128), 128, 0, st>>>(w, t, sc.row_count, sc.row_off, &sc.status[0]);
+    k_lbvh_write<<<blocks_for(n, 128), 128, 0, st>>>(w, t, sc.row_count, sc.row_off, &sc.status[0],
+                                                     s.row_cache);
     k_lbvh_static_rows<true><<<kStaticBlocks, 256, 0, st>>>(w, t, nullptr, sc.row_off,
                                                            s.static_list, s.static_count, s.bfs);
     return k + 5;

@@ -29,12 +29,17 @@ struct LbvhScratch {
     uint32_t* static_list;   // [cap]
     uint32_t* static_count;  // [1]
     uint32_t* bfs;
+    // partners of each dynamic body's row found by the count traversal, in
+    // ascending order, for rows of at most kRowCache partners
+    uint32_t* row_cache;  // [cap * kRowCache]
     // polls of an unpublished sort tile before a look-back gives up
     uint32_t wait_limit = kSpinLimit;
 };
 
 // Blocks that traverse static bodies' rows.
 constexpr uint32_t kStaticBlocks = 8;
+// Partners per row the count traversal keeps for the write pass.
+constexpr uint32_t kRowCache = 8;
 
 struct LbvhView {
     const float* node_min;

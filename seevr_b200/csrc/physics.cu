@@ -930,6 +930,7 @@ seevr_status seevr_physics_create(const seevr_bindings* b, const seevr_caps* cap
         ALLOC(lb.static_list, n);
         ALLOC(lb.static_count, 1);
         ALLOC(lb.bfs, size_t(kStaticBlocks) * 3 * 2 * n);
+        ALLOC(lb.row_cache, size_t(kRowCache) * n);
     }
 #undef ALLOC
     if (st == SEEVR_OK && cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)

@@ -142,6 +142,8 @@ struct Scratch {
                             // the narrowphase's pair order)
     uint32_t* pair_class;   // [2*kPairClasses] pairs per class and cursors
                             // (NULL: pairs taken in index order)
+    uint32_t order_pairs;   // 1: pairs taken grouped by class (scene groups'
+                            // handles), 0: in index order
     uint32_t* lut_rep;      // [kLutHullMax] first body with a lookup per hull size
     uint32_t* lut_off;      // [max_bodies] lookup offset read by the narrowphase
     // solver, per contact

@@ -681,9 +681,14 @@ __global__ void __launch_bounds__(128)
 // shapes' paths (4 classes) keeps a warp's lanes on one path, and within a
 // class the broadphase's order, in which neighbouring pairs share a body
 // (and its hull in cache).  Each pair's result is staged at its own index,
-// so the order changes no result.  (Putting pairs whose bounding spheres
-// overlap first, as longer MPR runs, measured 11% slower: it breaks up
-// those shared bodies.)
+// so the order changes no result.  Scene groups' handles take it (their
+// partial-size launches run beside other groups' kernels: 12.15 against
+// 12.52 ms per frame with 8 groups); a single handle takes the pairs in the
+// broadphase's order, which keeps every pair beside the neighbours that
+// share its bodies (12.62 against 13.52 ms per frame).  (Reordering only
+// within chunks of 256 pairs fell between the two in both settings;
+// putting pairs whose bounding spheres overlap first, as longer MPR runs,
+// measured 11% slower.)
 __device__ __forceinline__ uint32_t pair_class(const World& w, uint32_t p) {
     const uint32_t a = w.pairs[size_t(p) * 2], b = w.pairs[size_t(p) * 2 + 1];
     return (w.sup_off[a] != 0u ? 2u : 0u) | (w.sup_off[b] != 0u ? 1u : 0u);
@@ -815,7 +820,7 @@ int launch_narrowphase_taped(const World& w, const Consts& k, const Scratch& s, 
     // pair order by support path, in pair_coff (free until the scan below)
     const uint32_t* order = nullptr;
     int n = 3;
-    if (s.pair_class) {
+    if (s.pair_class && s.order_pairs) {
         cudaMemsetAsync(s.pair_class, 0, 2 * kPairClasses * sizeof(uint32_t), st);
         const uint32_t cb = grid_for(w.max_pairs, 256, 148 * 8);
         k_pair_classes<false><<<cb, 256, 0, st>>>(w, s.pair_class, nullptr);

@@ -647,6 +647,7 @@ seevr_status build_groups(seevr_physics* h) {
         g.h->s.bp_tile_rows = h->s.bp_tile_rows;
         g.h->s.wait_limit = h->s.wait_limit;
         g.h->s.giant_min = h->s.giant_min;
+        g.h->s.order_pairs = 1;  // pairs by support path (narrowphase.cu)
         st = seevr_physics_set_scenes(g.h, lo.data(), s1 - s0);
         if (st != SEEVR_OK) break;
         if (cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking) != cudaSuccess ||

@@ -102,8 +102,9 @@ struct GiantScratch {
     uint64_t* prio;    // [max_bodies] highest priority of an uncoloured contact
     uint32_t* hist;    // [kGiantMaxColours] contacts per colour, then cursors
     uint32_t* first;   // [kGiantMaxColours + 1] first slot of each colour
-    uint32_t* ctr;     // [8] barrier, counts
+    uint32_t* ctr;     // [kGiantCtrWords] barrier (words 0 and 32), counts (2-4)
 };
+constexpr uint32_t kGiantCtrWords = 64;
 constexpr uint32_t kGiantMaxColours = 64 + 1024;
 // Islands of more contacts than this are solved grid-wide in the coloured
 // mode (launch_solver_giant).

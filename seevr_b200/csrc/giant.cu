@@ -40,25 +40,28 @@ __device__ __forceinline__ f3 ld3cg(const float* p, uint32_t i) {
     return mk(__ldcg(p + size_t(i) * 3), __ldcg(p + size_t(i) * 3 + 1), __ldcg(p + size_t(i) * 3 + 2));
 }
 
-// Grid barrier of a cooperative launch: arrival count and a generation word
-// (bar[0], bar[1]).  Returns false, after raising kFlagTimeout, when the
-// wait exceeds `limit` polls or another block has given up.
+// Grid barrier of a cooperative launch: arrival count bar[0] and a
+// generation word bar[kGenWord], a cache line apart so that the polls of
+// the waiting blocks do not contend with the arrivals.  Returns false, after
+// raising kFlagTimeout, when the wait exceeds `limit` polls or another
+// block has given up (checked every 64 polls).
+constexpr uint32_t kGenWord = 32;
 __device__ bool grid_sync(uint32_t* bar, uint32_t* status, uint32_t limit) {
     __shared__ uint32_t sh_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
         uint32_t ok = 1u;
-        volatile uint32_t* gen = bar + 1;
+        volatile uint32_t* gen = bar + kGenWord;
         const uint32_t g = *gen;
         __threadfence();
         if (atomicAdd(&bar[0], 1u) == gridDim.x - 1u) {
             bar[0] = 0u;
             __threadfence();
-            atomicAdd(&bar[1], 1u);
+            atomicAdd(&bar[kGenWord], 1u);
         } else {
             uint32_t spins = 0;
             while (*gen == g) {
-                if (++spins > limit || halted(status)) {
+                if (++spins > limit || ((spins & 63u) == 0u && halted(status))) {
                     atomicOr(status, kFlagTimeout);
                     ok = 0u;
                     break;
@@ -116,7 +119,7 @@ __global__ void __launch_bounds__(kGiantThreads)
     k_solver_giant(World w, Consts k, Scratch s, float dt, uint32_t threshold) {
     if (halted(w.status)) return;
     GiantScratch& g = s.isl.giant;
-    uint32_t* bar = g.ctr;        // [0..1] barrier
+    uint32_t* bar = g.ctr;        // [0] and [kGenWord]: barrier
     uint32_t* n_giant = g.ctr + 2;
     uint32_t* n_coloured = g.ctr + 3;
     uint32_t* n_colours = g.ctr + 4;
@@ -269,7 +272,7 @@ int launch_solver_giant(const World& w, const Consts& k, const Scratch& s, float
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaMemsetAsync(g.ctr, 0, 8 * sizeof(uint32_t), st);
+    cudaMemsetAsync(g.ctr, 0, kGiantCtrWords * sizeof(uint32_t), st);
     cudaMemsetAsync(g.hist, 0, sizeof(uint32_t) * kMaxColours, st);
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(uint32_t(sms) * uint32_t(per_sm));

@@ -905,7 +905,7 @@ seevr_status seevr_physics_create(const seevr_bindings* b, const seevr_caps* cap
         ALLOC(gs.prio, c.max_bodies);
         ALLOC(gs.hist, kGiantMaxColours);
         ALLOC(gs.first, kGiantMaxColours + 1);
-        ALLOC(gs.ctr, 8);
+        ALLOC(gs.ctr, kGiantCtrWords);
     }
     if (p.broadphase == SEEVR_BROADPHASE_LBVH) {
         LbvhScratch& lb = h->lb;

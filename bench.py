@@ -662,24 +662,24 @@ NCU_METRICS = ("gpu__time_duration.sum,dram__bytes_read.sum,dram__bytes_write.su
 NCU_CAPTURED = {"bodies": 123288, "pairs": 118480, "contacts": 28231}
 NCU_CAPTURE = {
     "phys/aabb": {"kernel": "k_body_stage", "skip": 1001, "scale": "bodies",
-                  "dram_bytes_per_launch": 247077504, "duration_us": 60.7,
-                  "issue_active_pct": 45.5, "warps_active_pct": 37.9, "lanes_per_inst": 27.9,
+                  "dram_bytes_per_launch": 247286528, "duration_us": 60.2,
+                  "issue_active_pct": 44.7, "warps_active_pct": 38.1, "lanes_per_inst": 27.9,
                   "registers": 64},
     "phys/broad_phase": {"kernel": "k_broad_tile<0> + k_broad_tile<1>", "skip": 1820,
-                         "scale": "bodies", "dram_bytes_per_launch": 10462720,
-                         "duration_us": 57.4, "issue_active_pct": 40.5,
-                         "warps_active_pct": 56.6, "lanes_per_inst": 29.5, "registers": 63},
+                         "scale": "bodies", "dram_bytes_per_launch": 10507520,
+                         "duration_us": 56.8, "issue_active_pct": 40.5,
+                         "warps_active_pct": 56.3, "lanes_per_inst": 29.5, "registers": 63},
     "phys/narrow_phase": {"kernel": "k_narrow<0, 7>", "skip": 910, "scale": "pairs",
-                          "dram_bytes_per_launch": 97402880, "duration_us": 120.2,
-                          "issue_active_pct": 24.0, "warps_active_pct": 32.2,
-                          "lanes_per_inst": 12.1, "registers": 72},
+                          "dram_bytes_per_launch": 96512384, "duration_us": 128.1,
+                          "issue_active_pct": 33.5, "warps_active_pct": 32.8,
+                          "lanes_per_inst": 8.1, "registers": 72},
     "phys/pgs_solve": {"kernel": "k_solver_warp", "skip": 910, "scale": "bodies",
-                       "dram_bytes_per_launch": 10579712, "duration_us": 316.9,
+                       "dram_bytes_per_launch": 10580096, "duration_us": 316.6,
                        "issue_active_pct": 8.8, "warps_active_pct": 2.8, "lanes_per_inst": 15.9,
                        "registers": 124},
     "phys/render_verts": {"kernel": "k_render_verts", "skip": 91, "scale": "bodies",
-                          "dram_bytes_per_launch": 393440640, "duration_us": 97.5,
-                          "issue_active_pct": 36.4, "warps_active_pct": 39.8,
+                          "dram_bytes_per_launch": 394073344, "duration_us": 98.7,
+                          "issue_active_pct": 35.3, "warps_active_pct": 39.8,
                           "lanes_per_inst": 30.0, "registers": 62},
 }
 

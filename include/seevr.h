@@ -167,7 +167,12 @@ typedef struct seevr_profile {
 } seevr_profile;
 /* Stage order inside seevr_profile.ms: gravity, aabb, broad_phase,
  * narrow_phase, clear_impulse, pgs_solve, integrate, render_verts,
- * clear_counters — the order of physics.zig:22-32. */
+ * clear_counters — the order of physics.zig:22-32.  Stages fused into
+ * another report 0: gravity and integrate run in the aabb stage's kernel,
+ * the impulse clear in the narrowphase's contact write (it zeroes the
+ * impulse of each contact of the substep; entries past the contact count
+ * are left as they were, where the reference zeroes all MAX_CONTACTS), and
+ * the counters are written by the scans. */
 
 typedef struct seevr_physics seevr_physics;
 

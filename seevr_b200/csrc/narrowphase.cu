@@ -799,6 +799,7 @@ __global__ void k_contact_scatter(World w, const float4* __restrict__ res0,
         w.c_pen[c] = r0.w;
         w.c_a[c] = w.pairs[size_t(p) * 2];
         w.c_b[c] = w.pairs[size_t(p) * 2 + 1];
+        w.lambda[c] = 0.0f;  // step 4 (physics.comp:494-497) for the contacts of this substep
         if (contact_tape) {
             contact_tape[size_t(c) * 2] = pair_tape[size_t(p) * 2];
             contact_tape[size_t(c) * 2 + 1] = pair_tape[size_t(p) * 2 + 1];

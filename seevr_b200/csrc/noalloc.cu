@@ -281,8 +281,7 @@ extern "C" seevr_status seevr_physics_step_noalloc(
         launch_body_stage(w, k, (sub > 0 ? kIntegrate : 0u) | kGravity | kAabb, sub_dt, gravity[0],
                           gravity[1], gravity[2], st);
         launch_broadphase_n2(w, s, num_bodies, st);
-        launch_narrowphase(w, k, s, st);
-        cudaMemsetAsync(w.lambda, 0, sizeof(float) * max_contacts, st);
+        launch_narrowphase(w, k, s, st);  // zeroes the contacts' impulses (step 4)
         launch_solver(w, k, s, mode, sub_dt, num_bodies, num_bodies, st);
     }
     launch_body_stage(w, k, kIntegrate | (render ? kRenderVerts : 0u), sub_dt, gravity[0],

@@ -383,12 +383,8 @@ struct FrameIssue {
             if (h->check) n += launch_check_contacts(w, st);
         }
         T.end(kStNarrow);
-        T.begin();
-        {
-            const Range r("phys/clear_impulse");
-            cudaMemsetAsync(w.lambda, 0, sizeof(float) * w.max_contacts, st);  // step 4
-        }
-        T.end(kStClear);
+        // step 4 (clear impulses) is done by the contact scatter, which
+        // zeroes the impulse of every contact it writes
     }
 
     void solve(uint32_t) {

@@ -833,37 +833,42 @@ def config0_leg(a, dev):
     oracle over the same frames; the final states are compared."""
     import torch
 
-    from seevr_b200 import Caps, Data, Physics, make_params
+    from seevr_b200 import FLAG_CUDA_GRAPH, Caps, Data, Physics, make_params
 
     out = {"scene": "256 boxes + 256 spheres (16 segments), seed 0, ground box",
-           "frames": a.config0_frames, "how": "synchronous Physics.step per frame (the drop-in)"}
+           "frames": a.config0_frames,
+           "how": "synchronous Physics.step per frame (the drop-in), replaying the frame's CUDA "
+                  "graph (gpu) and launching each kernel (gpu_eager)"}
     d = Data.pile(seed=0)
     caps = Caps.for_data(d)
     for pgs in (4, 30):
-        buf = d.upload(dev, caps)
-        nb, nv, nhv = buf.num_bodies, buf.num_vertices, buf.num_hull_verts
-        ph = Physics(buf, make_params(pgs_iterations=pgs))
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for _ in range(a.config0_frames):
-            ph.step(nb, nv, nhv, a.substeps, DT, G)
-        e1.record()
-        e1.synchronize()
-        ms = e0.elapsed_time(e1)
-        pairs, contacts = ph.read_counters()
-        gpu_state = read_state(buf, nb)
-        ph.deinit()
         b = dict(a.__dict__)
         b["pgs"] = pgs
         work, secs, ref = oracle_frames(d.arrays(), None, a.config0_frames,
                                         argparse.Namespace(**b), 1)
-        exact = all(np.array_equal(gpu_state[k], ref[k].astype(np.float32)) for k, _, _ in STATE)
-        out[f"pgs{pgs}"] = {"gpu": work / (ms / 1e3), "gpu_ms_per_frame": ms / a.config0_frames,
-                            "cpu_oracle_1_thread": work / secs, "unit": UNIT,
-                            "pairs_last_substep": pairs, "contacts_last_substep": contacts,
-                            "final_state_bit_exact": bool(exact)}
-        del buf
+        res = {"cpu_oracle_1_thread": work / secs, "unit": UNIT}
+        for key, flags in (("gpu", FLAG_CUDA_GRAPH), ("gpu_eager", 0)):
+            buf = d.upload(dev, caps)
+            nb, nv, nhv = buf.num_bodies, buf.num_vertices, buf.num_hull_verts
+            ph = Physics(buf, make_params(pgs_iterations=pgs, flags=flags))
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(a.config0_frames):
+                ph.step(nb, nv, nhv, a.substeps, DT, G)
+            e1.record()
+            e1.synchronize()
+            ms = e0.elapsed_time(e1)
+            pairs, contacts = ph.read_counters()
+            gpu_state = read_state(buf, nb)
+            ph.deinit()
+            exact = all(np.array_equal(gpu_state[k], ref[k].astype(np.float32)) for k, _, _ in STATE)
+            res[key] = work / (ms / 1e3)
+            res[f"{key}_ms_per_frame"] = ms / a.config0_frames
+            res[f"{key}_final_state_bit_exact"] = bool(exact)
+            res["pairs_last_substep"], res["contacts_last_substep"] = pairs, contacts
+            del buf
+        out[f"pgs{pgs}"] = res
     return out
 
 

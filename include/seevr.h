@@ -202,7 +202,10 @@ seevr_status seevr_physics_set_scenes(seevr_physics* h,
  * narrowphase, impulse clear, PGS and integration, then one render-vertex
  * update.  Synchronous unless SEEVR_FLAG_NO_SYNC; `prof` may be NULL (fast
  * mode, physics.zig:118-164) or receive per-stage device timings
- * (profiling mode, physics.zig:97-117). */
+ * (profiling mode, physics.zig:97-117).  With SEEVR_FLAG_CUDA_GRAPH and no
+ * `prof`, the frame is replayed from its captured graph (as
+ * seevr_physics_step_async does) before the wait: the same results, one
+ * launch per frame. */
 seevr_status seevr_physics_step(seevr_physics* h,
                                 uint32_t num_bodies,
                                 uint32_t num_vertices,

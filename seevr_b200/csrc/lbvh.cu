@@ -382,12 +382,28 @@ __device__ __forceinline__ bool overlap_box(f3 mna, f3 mxa, f3 mnb, f3 mxb) {
              mxb.z < mna.z);
 }
 
+// The body tree as one 32-byte record per node, written after the refit:
+// lo = (min, left child or, for a leaf, its body), hi = (max, right child
+// or kLeafBit).  A traversal step reads one sector instead of five arrays.
+constexpr uint32_t kLeafBit = 0x80000000u;
+__global__ void k_pack_nodes(uint32_t n, const float* __restrict__ node_min,
+                             const float* __restrict__ node_max, const uint32_t* __restrict__ left,
+                             const uint32_t* __restrict__ right, const uint32_t* __restrict__ vals,
+                             float4* __restrict__ packed, uint32_t* err) {
+    if (halted(err)) return;  // the tree was not built
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < 2 * n - 1; k += gridDim.x * blockDim.x) {
+        const bool leaf = k >= n - 1;
+        const f3 mn = ld3(node_min, k), mx = ld3(node_max, k);
+        packed[2 * size_t(k)] = make_float4(mn.x, mn.y, mn.z, __uint_as_float(leaf ? vals[k - (n - 1)] : left[k]));
+        packed[2 * size_t(k) + 1] = make_float4(mx.x, mx.y, mx.z, __uint_as_float(leaf ? kLeafBit : right[k]));
+    }
+}
+
 // Visit every leaf j (original index) with j > lo_j whose box overlaps
 // body i's box, excluding static-static; `emit(j)` is called for each.
 template <class F>
 __device__ __forceinline__ void traverse(const World& w, const LbvhView& t, uint32_t i,
                                          uint32_t lo_j, uint32_t* err, F emit) {
-    const uint32_t n = w.nb;
     const f3 mna = ld3(w.aabb_min, i), mxa = ld3(w.aabb_max, i);
     const bool static_i = w.inv_mass[i] <= 0.0f;
     uint32_t stack[kStack];
@@ -395,17 +411,19 @@ __device__ __forceinline__ void traverse(const World& w, const LbvhView& t, uint
     stack[sp++] = 0;  // root (n >= 2)
     while (sp > 0) {
         const uint32_t node = stack[--sp];
-        if (!overlap_box(mna, mxa, ld3(t.node_min, node), ld3(t.node_max, node))) continue;
-        if (node >= n - 1) {
-            const uint32_t j = t.vals[node - (n - 1)];
+        const float4 lo = __ldg(&t.packed[2 * size_t(node)]), hi = __ldg(&t.packed[2 * size_t(node) + 1]);
+        if (!overlap_box(mna, mxa, mk(lo.x, lo.y, lo.z), mk(hi.x, hi.y, hi.z))) continue;
+        const uint32_t a = __float_as_uint(lo.w), b = __float_as_uint(hi.w);
+        if (b == kLeafBit) {
+            const uint32_t j = a;
             if (j > lo_j && !(static_i && w.inv_mass[j] <= 0.0f)) emit(j);
         } else {
             if (sp + 2 > kStack) {
                 atomicOr(err, kFlagTimeout);
                 return;
             }
-            stack[sp++] = t.right[node];
-            stack[sp++] = t.left[node];
+            stack[sp++] = b;
+            stack[sp++] = a;
         }
     }
 }
@@ -480,15 +498,18 @@ __global__ void __launch_bounds__(256)
             __syncthreads();
             for (uint32_t k = threadIdx.x; k < cur; k += blockDim.x) {
                 const uint32_t node = in[k];
-                if (!overlap_box(mna, mxa, ld3(t.node_min, node), ld3(t.node_max, node))) continue;
-                if (node >= n - 1) {
-                    const uint32_t j = t.vals[node - (n - 1)];
+                const float4 lo = __ldg(&t.packed[2 * size_t(node)]);
+                const float4 hi = __ldg(&t.packed[2 * size_t(node) + 1]);
+                if (!overlap_box(mna, mxa, mk(lo.x, lo.y, lo.z), mk(hi.x, hi.y, hi.z))) continue;
+                const uint32_t a = __float_as_uint(lo.w), b = __float_as_uint(hi.w);
+                if (b == kLeafBit) {
+                    const uint32_t j = a;
                     // the row owner is static: only dynamic partners count
                     if (j > i && w.inv_mass[j] > 0.0f) found[atomicAdd(&sh_found, 1u)] = j;
                 } else {
                     const uint32_t o = atomicAdd(&sh_next, 2u);
-                    out[o] = t.left[node];
-                    out[o + 1] = t.right[node];
+                    out[o] = a;
+                    out[o + 1] = b;
                 }
             }
             __syncthreads();
@@ -620,7 +641,13 @@ int launch_broadphase_lbvh(const World& w, const Scratch& sc, const LbvhScratch&
     const uint32_t n = w.nb;
     if (n == 0) return 0;
     int k = lbvh_build_bodies(w, s, &sc.status[0], st);
-    LbvhView t{s.node_min, s.node_max, s.left, s.right, s.vals_sorted};
+    LbvhView t{s.node_min, s.node_max, s.left, s.right, s.vals_sorted, s.packed};
+    if (n >= 2) {
+        k_pack_nodes<<<blocks_for(2 * n - 1, 256) < 148u * 8u ? blocks_for(2 * n - 1, 256) : 148u * 8u,
+                       256, 0, st>>>(n, s.node_min, s.node_max, s.left, s.right, s.vals_sorted,
+                                     s.packed, &sc.status[0]);
+        ++k;
+    }
     cudaMemsetAsync(s.static_count, 0, sizeof(uint32_t), st);
     k_lbvh_count<<<blocks_for(n, 128), 128, 0, st>>>(w, t, sc.row_count, &sc.status[0],
                                                      s.static_list, s.static_count, s.row_cache);

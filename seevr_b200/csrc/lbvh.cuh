@@ -32,6 +32,8 @@ struct LbvhScratch {
     // partners of each dynamic body's row found by the count traversal, in
     // ascending order, for rows of at most kRowCache partners
     uint32_t* row_cache;  // [cap * kRowCache]
+    // the body tree packed for the traversals: node k at [2k, 2k+1]
+    float4* packed;  // [2 * 2*cap]
     // polls of an unpublished sort tile before a look-back gives up
     uint32_t wait_limit = kSpinLimit;
 };
@@ -47,6 +49,8 @@ struct LbvhView {
     const uint32_t* left;
     const uint32_t* right;
     const uint32_t* vals;
+    // the same tree as one 32-byte record per node (lbvh.cu k_pack_nodes)
+    const float4* packed;
 };
 
 // Output buffers of the triangle BVH, laid out as bvh.comp's bindings.

@@ -928,6 +928,7 @@ seevr_status seevr_physics_create(const seevr_bindings* b, const seevr_caps* cap
         ALLOC(lb.static_count, 1);
         ALLOC(lb.bfs, size_t(kStaticBlocks) * 3 * 2 * n);
         ALLOC(lb.row_cache, size_t(kRowCache) * n);
+        ALLOC(lb.packed, size_t(4) * n);
     }
 #undef ALLOC
     if (st == SEEVR_OK && cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
@@ -1029,11 +1030,19 @@ seevr_status seevr_physics_step(seevr_physics* h, uint32_t num_bodies, uint32_t 
     if (prof) {
         prof->calls += 1;
     }
-    h->launches += h->groups.empty()
-                       ? issue_frame(h, num_bodies, num_vertices, num_hull_verts, substeps, dt,
-                                     gravity, h->stream, prof)
-                       : issue_frame_groups(h, num_vertices, num_hull_verts, substeps, dt, gravity,
-                                            h->stream, prof);
+    if (!prof && (h->params.flags & SEEVR_FLAG_CUDA_GRAPH)) {
+        // the frame replayed from its captured graph on the handle's stream
+        // (one launch instead of one per kernel), then the same wait
+        st = seevr_physics_step_async(h, num_bodies, num_vertices, num_hull_verts, substeps, dt,
+                                      gravity, 1, h->stream);
+        if (st != SEEVR_OK) return st;
+    } else {
+        h->launches += h->groups.empty()
+                           ? issue_frame(h, num_bodies, num_vertices, num_hull_verts, substeps, dt,
+                                         gravity, h->stream, prof)
+                           : issue_frame_groups(h, num_vertices, num_hull_verts, substeps, dt,
+                                                gravity, h->stream, prof);
+    }
     SEEVR_CUDA(cudaGetLastError());
     if (h->params.flags & SEEVR_FLAG_NO_SYNC) return SEEVR_OK;
     bool overflow = false;

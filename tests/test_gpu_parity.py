@@ -277,3 +277,16 @@ def test_batch_with_a_nan_body_matches_oracle(cuda):
         r = np.asarray(ref[key]).astype(g.dtype)
         assert g.shape == r.shape, key
         assert np.array_equal(g, r, equal_nan=g.dtype.kind == "f"), key
+
+
+def test_synchronous_step_replaying_the_graph_equals_eager(cuda):
+    """seevr_physics_step with SEEVR_FLAG_CUDA_GRAPH replays the captured
+    frame before its wait; every output equals the kernel-by-kernel step's,
+    frame after frame, and the oracle's."""
+    d = low_pile(9, 40)
+    eager = gpu_run(d, cuda, frames=12, pgs=10)
+    graph = gpu_run(d, cuda, frames=12, pgs=10, params=make_params(pgs_iterations=10, flags=2))
+    for k in ("pos", "quat", "vel", "omega", "aabb_min", "aabb_max", "pairs", "c_pos", "c_normal",
+              "c_pen", "lambda", "verts"):
+        assert np.array_equal(eager[k], graph[k]), k
+    assert_bit_exact(graph, oracle(d, frames=12, pgs=10))

@@ -354,6 +354,10 @@ seevr_status seevr_physics_step_noalloc(const seevr_bindings* bindings,
                                         uint32_t num_bodies, uint32_t num_vertices,
                                         uint32_t num_hull_verts, uint32_t substeps,
                                         float dt, const float gravity[3], void* stream);
+/* The device status bits the calling thread's last synchronous
+ * seevr_physics_step_noalloc read back (the bits of seevr_physics_read_flags;
+ * bit 3: a bundle too large for shared memory was swept in global memory). */
+uint32_t seevr_physics_noalloc_flags(void);
 
 /* Number of kernels the library launched on this handle since creation. */
 uint64_t seevr_physics_kernel_launches(const seevr_physics* h);

@@ -135,6 +135,7 @@ def _load():
         "seevr_raytrace_fov_scale": (F, []),
         "seevr_physics_step_noalloc": (I, [C.POINTER(Bindings), C.POINTER(Params), U32, U32,
                                            U32, U32, U32, U32, F, FP, P]),
+        "seevr_physics_noalloc_flags": (U32, []),
         "seevr_bvh_create": (I, [C.POINTER(BvhBindings), U32, C.POINTER(P)]),
         "seevr_bvh_build": (I, [P, U32]),
         "seevr_bvh_destroy": (None, [P]),

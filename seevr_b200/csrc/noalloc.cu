@@ -74,6 +74,8 @@ std::once_flag g_once[kMaxDevices];
 unsigned char* g_dev_ptr[kMaxDevices] = {};
 cudaError_t g_setup_err[kMaxDevices] = {};
 uint32_t g_narrow_blocks[kMaxDevices] = {};
+// the status bits the calling thread's last synchronous call read back
+thread_local uint32_t t_last_flags = 0;
 
 // Once per device, with that device current: the device address of the
 // scratch array, the solver's shared-memory opt-in and the persistent
@@ -293,8 +295,14 @@ extern "C" seevr_status seevr_physics_step_noalloc(
     e = cudaMemcpyAsync(&flags, s.status, sizeof flags, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return na_fail(SEEVR_ERR_CUDA, cudaGetErrorString(e));
+    t_last_flags = flags;
     if (flags & kFlagTimeout) return na_fail(SEEVR_ERR_TIMEOUT, "a device-side wait gave up");
     if (flags & (kFlagPairOverflow | kFlagContactOverflow))
         return na_fail(SEEVR_ERR_CAPACITY, "pairs or contacts exceeded max_pairs/max_contacts");
     return SEEVR_OK;
 }
+
+// The status bits of the calling thread's last synchronous no-allocation
+// step (bit 3: the solver swept in global memory; the others as
+// seevr_physics_read_flags).
+extern "C" uint32_t seevr_physics_noalloc_flags(void) { return t_last_flags; }

@@ -443,7 +443,7 @@ def adjoint_leg(a, rank, world, dev):
     import torch
     import torch.distributed as dist
 
-    from seevr_b200 import Caps, Data, Physics, make_params
+    from seevr_b200 import FLAG_CUDA_GRAPH, FLAG_SKIP_RENDER_VERTS, Caps, Data, Physics, make_params
     from seevr_b200.grad import rollout
 
     d = Data.rollout(num_scenes=a.adjoint_scenes, bodies=a.adjoint_bodies, segments=a.segments,
@@ -451,7 +451,8 @@ def adjoint_leg(a, rank, world, dev):
     nb = d.num_bodies
     caps = Caps.for_data(d, pairs_per_body=8.0, contacts_per_body=4.0)
     buf = d.upload(dev, caps)
-    ph = Physics(buf, make_params(pgs_iterations=a.pgs, flags=4,
+    # the forward's substeps replay a captured one-substep graph
+    ph = Physics(buf, make_params(pgs_iterations=a.pgs, flags=FLAG_SKIP_RENDER_VERTS | FLAG_CUDA_GRAPH,
                                   bundle_bodies=a.adjoint_bodies + 1))
     off = d.scene_body_offset()
     first = torch.tensor(off[:-1].astype(np.int64) + 1, device=dev)  # body 0 is the ground

@@ -37,11 +37,11 @@ def settled(seed, n, frames):
     return d, a, caps, st
 
 
-def gpu_grads(d, caps, st, w, cuda, substeps, frames=1):
+def gpu_grads(d, caps, st, w, cuda, substeps, frames=1, flags=4):
     import torch
 
     buf = d.upload(cuda, caps)
-    ph = Physics(buf, make_params(pgs_iterations=PGS, flags=4))
+    ph = Physics(buf, make_params(pgs_iterations=PGS, flags=flags))
     ins = {k: torch.tensor(st[k], device=cuda, requires_grad=True) for k in
            ("pos", "quat", "vel", "omega", "friction")}
     out = rollout(ph, ins["pos"], ins["quat"], ins["vel"], ins["omega"], ins["friction"],
@@ -122,8 +122,13 @@ def test_rollout_forward_equals_step_and_backward_is_deterministic(cuda):
     w = weights(nb, 5)
     g1, fwd, _ = gpu_grads(d, caps, st, w, cuda, substeps=10, frames=2)
     g2, _, _ = gpu_grads(d, caps, st, w, cuda, substeps=10, frames=2)
+    # the forward's substeps replayed from a captured graph: the same gradients
+    g3, fwd3, _ = gpu_grads(d, caps, st, w, cuda, substeps=10, frames=2, flags=4 | 2)
     for k in g1:
         assert np.array_equal(g1[k], g2[k]), k
+        assert np.array_equal(g1[k], g3[k]), k
+    for k in fwd:
+        assert np.array_equal(fwd[k], fwd3[k]), k
     # the substep-by-substep forward is the regular 10-substep frame, bit for bit
     buf = d.upload(cuda, caps)
     for k, c in KEYS:

@@ -347,7 +347,7 @@ void seevr_physics_destroy(seevr_physics* h);
 #define SEEVR_NOALLOC_MAX_BODIES 4096u
 #define SEEVR_NOALLOC_MAX_PAIRS 32768u
 #define SEEVR_NOALLOC_MAX_CONTACTS 16384u
-#define SEEVR_NOALLOC_SCRATCH_BYTES 4965632u
+#define SEEVR_NOALLOC_SCRATCH_BYTES 5489920u
 seevr_status seevr_physics_step_noalloc(const seevr_bindings* bindings,
                                         const seevr_params* params,
                                         uint32_t max_pairs, uint32_t max_contacts,

@@ -268,7 +268,7 @@ int launch_solver_giant(const World& w, const Consts& k, const Scratch& s, float
                         cudaStream_t st);
 // Scenes above this many bodies are solved by islands (when allocated).
 constexpr uint32_t kWarpMaxBodies = 1024;
-constexpr uint32_t kRecWords = 8;  // float4 words of a warp-solver contact record
+constexpr uint32_t kRecWords = 10;  // float4 words of a warp-solver contact record
 
 // One scene group's outputs, merged into the bound buffers at frame end
 // (physics.cu): its counters and status word, its pair and contact lists in

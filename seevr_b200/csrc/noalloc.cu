@@ -10,7 +10,7 @@
 // entry point runs the same kernels on scratch carved from one file-scope
 // device array, so the caller provides only the bound buffers and a stream.
 //
-// The array holds SEEVR_NOALLOC_SCRATCH_BYTES (4,965,632 bytes, about 5.0 MB)
+// The array holds SEEVR_NOALLOC_SCRATCH_BYTES (5,489,920 bytes, about 5.5 MB)
 // on every device that loads the library, until the process exits.  All calls share it: calls whose GPU
 // work overlaps (different streams, or different host threads on one
 // device) race on it and must be serialised by the caller.  Each call

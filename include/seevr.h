@@ -315,6 +315,46 @@ seevr_status seevr_physics_download_state(seevr_physics* h, uint32_t num_bodies,
                                           float* pos, float* quat,
                                           float* vel, float* omega);
 
+/* Host arrays of one frame's state for seevr_physics_step_io: `*_in` are
+ * copied into the bound device buffers before the frame, the bound buffers
+ * into `*_out` after it (pos, vel, omega: 3 floats per body; quat: 4).  Any
+ * pointer may be NULL to skip that copy; an input and an output may be the
+ * same array. */
+typedef struct seevr_host_state {
+    const float* pos_in;
+    const float* quat_in;
+    const float* vel_in;
+    const float* omega_in;
+    float* pos_out;
+    float* quat_out;
+    float* vel_out;
+    float* omega_out;
+} seevr_host_state;
+
+/* One frame (seevr_physics_step_async with frames = 1) with its state copied
+ * in from and out to host arrays: Data.upload, Physics.step and
+ * Vulkan.readBuffer of the state (data.zig:599-611, physics.zig:80,
+ * vulkan.zig:317-328) in one call.  When every non-NULL array is page-locked
+ * (cudaHostAlloc / cudaHostRegister), the copies are ordered on `stream`
+ * without waiting (the outputs are valid once the stream has reached this
+ * point), and with scene groups each group's bodies are copied on the
+ * group's stream, just before and just after that group's frame, so that
+ * one group's copies overlap the other groups' kernels; with
+ * SEEVR_FLAG_CUDA_GRAPH the copies are part of the captured frame graph
+ * (re-captured when an array pointer changes).  With a pageable array the
+ * call copies in, steps and copies out one after another and returns after
+ * the last copy.  Results equal seevr_physics_upload_state, the step and
+ * seevr_physics_download_state.  No counterpart in the reference. */
+seevr_status seevr_physics_step_io(seevr_physics* h,
+                                   uint32_t num_bodies,
+                                   uint32_t num_vertices,
+                                   uint32_t num_hull_verts,
+                                   uint32_t substeps,
+                                   float dt,
+                                   const float gravity[3],
+                                   const seevr_host_state* io,
+                                   void* stream);
+
 /* Replaces Physics.deinit (physics.zig:219-221). */
 void seevr_physics_destroy(seevr_physics* h);
 

@@ -100,6 +100,12 @@ class RtParams(C.Structure):
                 ("num_triangles", C.c_uint32)]
 
 
+class HostState(C.Structure):
+    """seevr_host_state: host arrays copied in before and out after a frame."""
+    _fields_ = [(n, C.c_void_p) for n in ("pos_in", "quat_in", "vel_in", "omega_in",
+                                          "pos_out", "quat_out", "vel_out", "omega_out")]
+
+
 class SeevrError(RuntimeError):
     def __init__(self, status: int, message: str):
         super().__init__(f"seevr status {status}: {message}")
@@ -127,6 +133,7 @@ def _load():
         "seevr_physics_set_wait_limit": (I, [P, U32]),
         "seevr_physics_upload_state": (I, [P, U32, P, P, P, P]),
         "seevr_physics_download_state": (I, [P, U32, P, P, P, P]),
+        "seevr_physics_step_io": (I, [P, U32, U32, U32, U32, F, FP, C.POINTER(HostState), P]),
         "seevr_physics_destroy": (None, [P]),
         "seevr_physics_kernel_launches": (U64, [P]),
         "seevr_physics_read_lbvh": (I, [P, U32, UP, UP, FP]),

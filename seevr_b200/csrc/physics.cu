@@ -67,7 +67,12 @@ enum Stage {
 struct GraphKey {
     uint32_t nb, nv, nhv, substeps;
     float dt, g[3];
+    // host arrays whose copies the frame holds (seevr_physics_step_io), or
+    // none
+    const void* io[8];
     bool operator==(const GraphKey& o) const {
+        for (int i = 0; i < 8; ++i)
+            if (io[i] != o.io[i]) return false;
         return nb == o.nb && nv == o.nv && nhv == o.nhv && substeps == o.substeps && dt == o.dt &&
                g[0] == o.g[0] && g[1] == o.g[1] && g[2] == o.g[2];
     }
@@ -475,8 +480,34 @@ __global__ void k_merge_groups(World w, GroupTable t) {
 
 // One frame of every group: forked from `st` onto the groups' streams (or,
 // with per-stage profiling, group after group on `st`), joined back, merged.
+// The state rows [b0, b0 + n) between the host arrays of `io` and the bound
+// buffers (pos, vel, omega: 12 bytes a body; quat: 16), ordered on st.
+void copy_state_in(const seevr_physics* h, uint32_t b0, uint32_t n, const seevr_host_state* io,
+                   cudaStream_t st) {
+    if (!io || n == 0) return;
+    const size_t o3 = size_t(b0) * 3, o4 = size_t(b0) * 4;
+    const auto H2D = cudaMemcpyHostToDevice;
+    if (io->pos_in) cudaMemcpyAsync(h->w.pos + o3, io->pos_in + o3, size_t(n) * 12, H2D, st);
+    if (io->quat_in) cudaMemcpyAsync(h->w.quat + o4, io->quat_in + o4, size_t(n) * 16, H2D, st);
+    if (io->vel_in) cudaMemcpyAsync(h->w.vel + o3, io->vel_in + o3, size_t(n) * 12, H2D, st);
+    if (io->omega_in) cudaMemcpyAsync(h->w.omega + o3, io->omega_in + o3, size_t(n) * 12, H2D, st);
+}
+void copy_state_out(const seevr_physics* h, uint32_t b0, uint32_t n, const seevr_host_state* io,
+                    cudaStream_t st) {
+    if (!io || n == 0) return;
+    const size_t o3 = size_t(b0) * 3, o4 = size_t(b0) * 4;
+    const auto D2H = cudaMemcpyDeviceToHost;
+    if (io->pos_out) cudaMemcpyAsync(io->pos_out + o3, h->w.pos + o3, size_t(n) * 12, D2H, st);
+    if (io->quat_out) cudaMemcpyAsync(io->quat_out + o4, h->w.quat + o4, size_t(n) * 16, D2H, st);
+    if (io->vel_out) cudaMemcpyAsync(io->vel_out + o3, h->w.vel + o3, size_t(n) * 12, D2H, st);
+    if (io->omega_out) cudaMemcpyAsync(io->omega_out + o3, h->w.omega + o3, size_t(n) * 12, D2H, st);
+}
+
+// io (seevr_physics_step_io, not with prof): each group's state rows are
+// copied in on the group's stream before its frame and out after it.
 uint64_t issue_frame_groups(seevr_physics* h, uint32_t nv, uint32_t nhv, uint32_t substeps,
-                            float dt, const float g[3], cudaStream_t st, seevr_profile* prof) {
+                            float dt, const float g[3], cudaStream_t st, seevr_profile* prof,
+                            const seevr_host_state* io = nullptr) {
     uint64_t n = 0;
     if (prof) {
         for (auto& G : h->groups)
@@ -493,6 +524,7 @@ uint64_t issue_frame_groups(seevr_physics* h, uint32_t nv, uint32_t nhv, uint32_
         for (auto& G : h->groups) {
             if (!G.h) continue;  // a group of empty scenes
             cudaStreamWaitEvent(G.stream, h->fork, 0);
+            copy_state_in(h, G.b0, G.nb, io, G.stream);
             FrameIssue f(G.h, G.nb, nv, nhv, substeps, dt, g, G.stream, nullptr);
             f.begin();
             for (uint32_t s = 0; s < substeps; ++s) {
@@ -501,6 +533,7 @@ uint64_t issue_frame_groups(seevr_physics* h, uint32_t nv, uint32_t nhv, uint32_
             }
             f.end();
             n += f.n;
+            copy_state_out(h, G.b0, G.nb, io, G.stream);
             cudaEventRecord(G.done, G.stream);
             cudaStreamWaitEvent(st, G.done, 0);
         }
@@ -1052,29 +1085,38 @@ seevr_status seevr_physics_step(seevr_physics* h, uint32_t num_bodies, uint32_t 
     return SEEVR_OK;
 }
 
-seevr_status seevr_physics_step_async(seevr_physics* h, uint32_t num_bodies, uint32_t num_vertices,
-                                      uint32_t num_hull_verts, uint32_t substeps, float dt,
-                                      const float gravity[3], uint32_t frames, void* stream) {
-    if (!h || !gravity) return fail(SEEVR_ERR_INVALID_ARGUMENT, "handle or gravity is NULL");
-    if (num_bodies == 0 || substeps == 0 || frames == 0) return SEEVR_OK;
-    seevr_status st = check_step_args(h, num_bodies, num_vertices, num_hull_verts);
-    if (st != SEEVR_OK) return st;
-    SEEVR_CUDA(cudaSetDevice(h->device));
-    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
-    st = ensure_single_scene(h, num_bodies, s);
-    if (st != SEEVR_OK) return st;
+namespace {
+
+// One frame's kernels, with io's copies (ungrouped: all rows before and
+// after the frame on st; grouped: per group, on the group's stream).
+uint64_t issue_frame_io(seevr_physics* h, uint32_t nb, uint32_t nv, uint32_t nhv,
+                        uint32_t substeps, float dt, const float g[3], cudaStream_t st,
+                        const seevr_host_state* io) {
+    if (!h->groups.empty()) return issue_frame_groups(h, nv, nhv, substeps, dt, g, st, nullptr, io);
+    copy_state_in(h, 0, nb, io, st);
+    const uint64_t n = issue_frame(h, nb, nv, nhv, substeps, dt, g, st, nullptr);
+    copy_state_out(h, 0, nb, io, st);
+    return n;
+}
+
+seevr_status run_frames(seevr_physics* h, uint32_t num_bodies, uint32_t num_vertices,
+                        uint32_t num_hull_verts, uint32_t substeps, float dt,
+                        const float gravity[3], uint32_t frames, cudaStream_t s,
+                        const seevr_host_state* io) {
     if (!(h->params.flags & SEEVR_FLAG_CUDA_GRAPH)) {
         for (uint32_t f = 0; f < frames; ++f)
-            h->launches += h->groups.empty()
-                               ? issue_frame(h, num_bodies, num_vertices, num_hull_verts, substeps,
-                                             dt, gravity, s, nullptr)
-                               : issue_frame_groups(h, num_vertices, num_hull_verts, substeps, dt,
-                                                    gravity, s, nullptr);
+            h->launches += issue_frame_io(h, num_bodies, num_vertices, num_hull_verts, substeps, dt,
+                                          gravity, s, io);
         SEEVR_CUDA(cudaGetLastError());
         return SEEVR_OK;
     }
-    const GraphKey key{num_bodies, num_vertices, num_hull_verts, substeps, dt,
-                       {gravity[0], gravity[1], gravity[2]}};
+    GraphKey key{num_bodies, num_vertices, num_hull_verts, substeps, dt,
+                 {gravity[0], gravity[1], gravity[2]}, {}};
+    if (io) {
+        const void* p[8] = {io->pos_in,  io->quat_in,  io->vel_in,  io->omega_in,
+                            io->pos_out, io->quat_out, io->vel_out, io->omega_out};
+        for (int i = 0; i < 8; ++i) key.io[i] = p[i];
+    }
     if (!h->graph_exec || !(h->graph_key == key)) {
         if (h->graph_exec) {
             cudaGraphExecDestroy(h->graph_exec);
@@ -1085,11 +1127,8 @@ seevr_status seevr_physics_step_async(seevr_physics* h, uint32_t num_bodies, uin
         const cudaStream_t cap = h->stream;
         cudaGraph_t g = nullptr;
         SEEVR_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
-        const uint64_t n = h->groups.empty()
-                               ? issue_frame(h, num_bodies, num_vertices, num_hull_verts, substeps,
-                                             dt, gravity, cap, nullptr)
-                               : issue_frame_groups(h, num_vertices, num_hull_verts, substeps, dt,
-                                                    gravity, cap, nullptr);
+        const uint64_t n = issue_frame_io(h, num_bodies, num_vertices, num_hull_verts, substeps, dt,
+                                          gravity, cap, io);
         cudaError_t e = cudaStreamEndCapture(cap, &g);
         if (e != cudaSuccess) return fail(SEEVR_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
         e = cudaGraphInstantiate(&h->graph_exec, g, 0);
@@ -1101,6 +1140,64 @@ seevr_status seevr_physics_step_async(seevr_physics* h, uint32_t num_bodies, uin
     for (uint32_t f = 0; f < frames; ++f) SEEVR_CUDA(cudaGraphLaunch(h->graph_exec, s));
     h->launches += h->graph_kernels * frames;
     return SEEVR_OK;
+}
+
+bool page_locked(const void* p) {
+    if (!p) return true;
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+}  // namespace
+
+seevr_status seevr_physics_step_async(seevr_physics* h, uint32_t num_bodies, uint32_t num_vertices,
+                                      uint32_t num_hull_verts, uint32_t substeps, float dt,
+                                      const float gravity[3], uint32_t frames, void* stream) {
+    if (!h || !gravity) return fail(SEEVR_ERR_INVALID_ARGUMENT, "handle or gravity is NULL");
+    if (num_bodies == 0 || substeps == 0 || frames == 0) return SEEVR_OK;
+    seevr_status st = check_step_args(h, num_bodies, num_vertices, num_hull_verts);
+    if (st != SEEVR_OK) return st;
+    SEEVR_CUDA(cudaSetDevice(h->device));
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
+    st = ensure_single_scene(h, num_bodies, s);
+    if (st != SEEVR_OK) return st;
+    return run_frames(h, num_bodies, num_vertices, num_hull_verts, substeps, dt, gravity, frames, s,
+                      nullptr);
+}
+
+seevr_status seevr_physics_step_io(seevr_physics* h, uint32_t num_bodies, uint32_t num_vertices,
+                                   uint32_t num_hull_verts, uint32_t substeps, float dt,
+                                   const float gravity[3], const seevr_host_state* io,
+                                   void* stream) {
+    if (!h || !gravity || !io) return fail(SEEVR_ERR_INVALID_ARGUMENT, "handle, gravity or io is NULL");
+    if (num_bodies == 0 || substeps == 0) return SEEVR_OK;
+    seevr_status st = check_step_args(h, num_bodies, num_vertices, num_hull_verts);
+    if (st != SEEVR_OK) return st;
+    SEEVR_CUDA(cudaSetDevice(h->device));
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
+    const void* p[8] = {io->pos_in,  io->quat_in,  io->vel_in,  io->omega_in,
+                        io->pos_out, io->quat_out, io->vel_out, io->omega_out};
+    bool locked = true;
+    for (const void* q : p) locked = locked && page_locked(q);
+    if (!locked) {
+        // pageable memory: one copy after another, each waited for
+        st = seevr_physics_upload_state(h, num_bodies, io->pos_in, io->quat_in, io->vel_in,
+                                        io->omega_in);
+        if (st != SEEVR_OK) return st;
+        st = seevr_physics_step_async(h, num_bodies, num_vertices, num_hull_verts, substeps, dt,
+                                      gravity, 1, s);
+        if (st != SEEVR_OK) return st;
+        SEEVR_CUDA(cudaStreamSynchronize(s));
+        return seevr_physics_download_state(h, num_bodies, io->pos_out, io->quat_out, io->vel_out,
+                                            io->omega_out);
+    }
+    st = ensure_single_scene(h, num_bodies, s);
+    if (st != SEEVR_OK) return st;
+    return run_frames(h, num_bodies, num_vertices, num_hull_verts, substeps, dt, gravity, 1, s, io);
 }
 
 seevr_status seevr_physics_read_counters(seevr_physics* h, uint32_t out[2]) {

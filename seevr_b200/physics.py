@@ -116,6 +116,35 @@ class Physics:
         L.check(L.lib.seevr_physics_download_state(self._h, num_bodies, ptr(pos), ptr(quat),
                                                    ptr(vel), ptr(omega)))
 
+    def step_io(self, num_bodies: int, num_vertices: int, num_hull_verts: int, substeps: int,
+                dt: float, gravity=(0.0, -9.81, 0.0), inputs=None, outputs=None, stream=None,
+                sync: bool = True) -> None:
+        """seevr_physics_step_io: one frame with the state copied in from the
+        host arrays `inputs` and out to `outputs` (dicts of pos, quat, vel,
+        omega: numpy arrays or CPU tensors; a missing key skips that copy).
+        Page-locked arrays (torch's pin_memory) are copied per scene group
+        beside the other groups' kernels.  Ordered on `stream` (None: torch's
+        current stream); sync=True waits for it before returning, so the
+        outputs are ready."""
+        import torch
+
+        if stream is None:
+            stream = torch.cuda.current_stream()
+        ptr = lambda a: None if a is None else (a.ctypes.data if isinstance(a, np.ndarray) else a.data_ptr())
+        i, o = inputs or {}, outputs or {}
+        io = L.HostState(*[ptr(i.get(k)) for k in ("pos", "quat", "vel", "omega")],
+                         *[ptr(o.get(k)) for k in ("pos", "quat", "vel", "omega")])
+        s = getattr(stream, "cuda_stream", stream)
+        if stream is not None and not s:
+            s = 1  # torch's default stream is CUDA's legacy default stream (cudaStreamLegacy)
+        L.check(L.lib.seevr_physics_step_io(self._h, num_bodies, num_vertices, num_hull_verts,
+                                            substeps, dt, L.fptr(gravity, 3), C.byref(io),
+                                            C.c_void_p(s) if s else None))
+        if sync:
+            if not hasattr(stream, "synchronize"):
+                stream = torch.cuda.ExternalStream(s)
+            stream.synchronize()
+
     def read_lbvh(self, n: int):
         """Sorted Morton codes, body order and centroid bounds of the last
         LBVH build (broadphase=BROADPHASE_LBVH handles)."""

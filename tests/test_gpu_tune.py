@@ -68,6 +68,50 @@ def test_scene_groups_in_the_frame_graph(cuda, groups):
         assert np.array_equal(a[k], b[k]), k
 
 
+@pytest.mark.parametrize("groups,flags,pinned", [(1, 2, True), (4, 2, True), (4, 0, True),
+                                                  (4, 2, False)])
+def test_step_io_equals_upload_step_download(cuda, groups, flags, pinned):
+    """seevr_physics_step_io: host copies per scene group around each group's
+    frame (page-locked arrays; frame graph or launched kernels) or one after
+    another (pageable arrays) give the state that upload_state, the step and
+    download_state give, frame after frame, with each input array also the
+    output; the bound buffers hold the same state."""
+    import torch
+
+    d = Data.batch(num_scenes=64, min_bodies=8, max_bodies=256, seed_base=43)
+    caps = Caps.for_data(d, pairs_per_body=8.0, contacts_per_body=4.0)
+    keys = ("pos", "quat", "vel", "omega")
+    finals = []
+    for use_io in (False, True):
+        buf = d.upload(cuda, caps)
+        ph = Physics(buf, make_params(pgs_iterations=10, flags=flags))
+        ph.set_tuning(scene_groups=groups)
+        nb, nv, nhv = buf.num_bodies, buf.num_vertices, buf.num_hull_verts
+        st = read_back(buf)
+        host = {k: np.ascontiguousarray(st[k], dtype=np.float32) for k in keys}
+        if use_io and pinned:
+            host = {k: torch.from_numpy(v).pin_memory() for k, v in host.items()}
+        for _ in range(40):  # the bodies land: contacts at the last frames
+            if use_io:
+                ph.step_io(nb, nv, nhv, 10, DT, G, inputs=host, outputs=host)
+            else:
+                ph.upload_state(nb, *[host[k] for k in keys])
+                ph.step_async(nb, nv, nhv, 10, DT, G, frames=1)
+                torch.cuda.synchronize()
+                ph.download_state(nb, *[host[k] for k in keys])
+        torch.cuda.synchronize()
+        dev = read_back(buf)
+        ph.deinit()
+        out = {k: (v.numpy() if hasattr(v, "numpy") else v) for k, v in host.items()}
+        for k in keys:
+            assert np.array_equal(out[k], dev[k]), (use_io, k)
+        finals.append((out, dev["num_contacts"]))
+    (a, ca), (b, cb) = finals
+    assert ca > 20 and ca == cb
+    for k in keys:
+        assert np.array_equal(a[k], b[k]), k
+
+
 def test_scene_groups_overflow_is_reported(cuda):
     """The merged counters are the batch's true totals: a pair cap below them
     raises ERR_CAPACITY as without groups."""

@@ -145,6 +145,8 @@ struct Scratch {
                             // (NULL: pairs taken in index order)
     uint32_t order_pairs;   // 1: pairs taken grouped by class (scene groups'
                             // handles), 0: in index order
+    uint32_t sweep_warps;   // warps per solver bundle: 2 in scene groups'
+                            // handles (64-wide passes), else 1
     uint32_t* lut_rep;      // [kLutHullMax] first body with a lookup per hull size
     uint32_t* lut_off;      // [max_bodies] lookup offset read by the narrowphase
     // solver, per contact

@@ -677,6 +677,7 @@ seevr_status build_groups(seevr_physics* h) {
         g.h->s.wait_limit = h->s.wait_limit;
         g.h->s.giant_min = h->s.giant_min;
         g.h->s.order_pairs = 1;  // pairs by support path (narrowphase.cu)
+        g.h->s.sweep_warps = 2;  // 64-wide solver passes (solver.cu)
         st = seevr_physics_set_scenes(g.h, lo.data(), s1 - s0);
         if (st != SEEVR_OK) break;
         if (cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking) != cudaSuccess ||

@@ -197,23 +197,32 @@ __global__ void k_bundle_ranges(World w, uint32_t* __restrict__ bundle_c0) {
     }
 }
 
-// ---- warp per bundle --------------------------------------------------------
-// Bundles of up to kWarpMaxBodies bodies: one warp per bundle, __syncwarp
-// between levels.  What a solve round waits on lives in shared memory: the
+// ---- block per bundle -------------------------------------------------------
+// Bundles of up to kWarpMaxBodies bodies: one block of W warps per bundle;
+// one warp builds the levels and records, then the block sweeps passes of up
+// to 32 W same-level contacts, a barrier between passes.
+// What a solve round waits on lives in shared memory: the
 // bundle's velocities and angular velocities, the impulses and the level
 // boundaries.  The per-contact constants are computed directly in level
 // order, so the lanes of a round read consecutive entries.  Levels are
 // assigned 32 contacts at a time: each lane starts from the latest level of
 // its bodies in earlier chunks, then lanes are visited in order and every
 // later lane sharing a dynamic body with lane j moves past lane j's level.
-// one warp per block: the SM places a bundle's 19 KB of shared memory
+// One bundle per block: the SM places a bundle's 19 KB of shared memory
 // wherever it fits beside other kernels (14.05 -> 13.80 ms per frame
-// against four-warp blocks on the 4,096-scene batch, no change with
-// scene groups)
-constexpr uint32_t kWarpsPerBlock = 1;
+// against four bundles per block on the 4,096-scene batch).
+// W = 1 for a handle stepped alone; W = 2 for scene groups' handles, whose
+// solver chains are the frame's critical path while other groups' collision
+// stages fill the GPU: 64-wide passes cut the largest bundles' passes per
+// iteration by about a tenth (frame 12.68 -> 12.13 ms with 8 groups on the
+// 4,096-scene batch), while alone the doubled warps per SM sub-partition
+// slow every pass more than that (12.52 -> 12.89 ms ungrouped).
+constexpr uint32_t kMaxSweepWarps = 2;
 constexpr uint32_t kWarpLamCap = 1024;   // impulses per bundle held in smem
 constexpr uint32_t kWarpLevelCap = 128;  // passes held in smem
-constexpr uint32_t kPassShift = 26, kPassMask = (1u << kPassShift) - 1u;
+// pass entry: start position | count << kPassShift (count <= 128)
+constexpr uint32_t kPassShift = 24, kPassMask = (1u << kPassShift) - 1u;
+static_assert(32 * kMaxSweepWarps < (1u << (32 - kPassShift)), "pass count field too narrow");
 constexpr uint32_t kRegChunks = 8;  // contacts per lane kept in registers by the setup
 
 // A contact's record (kRecWords float4, 160 bytes): n ra rb bias kn mu,
@@ -264,11 +273,13 @@ __device__ __forceinline__ void write_rec(const World& w, const Consts& k, const
 }
 
 // Passes of the positions [beg, pos) of one level, from entry npass on.
+// kPassWidth: contacts a pass solves at once (the block's threads).
+template <uint32_t kPassWidth>
 __device__ __forceinline__ uint32_t write_passes(uint32_t* gpass, uint32_t npass, uint32_t beg,
                                                  uint32_t pos, uint32_t lane) {
-    for (uint32_t q = beg + lane * 32; q < pos; q += 32 * 32)
-        gpass[npass + (q - beg) / 32] = q | (min(32u, pos - q) << kPassShift);
-    return npass + (pos - beg + 31) / 32;
+    for (uint32_t q = beg + lane * kPassWidth; q < pos; q += 32 * kPassWidth)
+        gpass[npass + (q - beg) / kPassWidth] = q | (min(kPassWidth, pos - q) << kPassShift);
+    return npass + (pos - beg + kPassWidth - 1) / kPassWidth;
 }
 
 __device__ __forceinline__ void solve_rec(float* V, float* W, const float4 (&r)[kRecWords], float* lam) {
@@ -285,44 +296,17 @@ __host__ __device__ constexpr uint32_t warp_smem_words(uint32_t nbmax) {
     return 7 * nbmax + kWarpLamCap + kWarpLevelCap;
 }
 
-__global__ void __launch_bounds__(kWarpsPerBlock * 32)
-    k_solver_warp(World w, Consts k, Scratch s, uint32_t mode, float dt, uint32_t nbmax) {
-    // nbmax: bodies per warp held in shared memory; a bundle with more
-    // bodies (a single scene above the bundle size) solves on the bound
-    // velocity buffers in place
-    extern __shared__ float sm[];
-    if (halted(w.status)) return;  // contacts from a scan that gave up
+// Levels, solve positions, pass table and contact records of one bundle,
+// built by one warp (lane = its lane): returns the positions (contacts
+// solved) and the passes written to gpass.
+template <uint32_t kPassWidth>
+__device__ __forceinline__ void bundle_setup(const World& w, const Consts& k, const Scratch& s,
+                                             const BodyView& B, uint32_t mode, float dt,
+                                             uint32_t b0, uint32_t c0, uint32_t c1, uint32_t nbs,
+                                             uint32_t ncb, uint32_t* last, float* lam,
+                                             uint32_t* gpass, uint32_t lane, uint32_t& pos_out,
+                                             uint32_t& npass_out) {
     const unsigned full = 0xFFFFFFFFu;
-    const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
-    const uint32_t bundle = blockIdx.x * kWarpsPerBlock + wid;
-    if (bundle >= w.nbundles) return;
-    const uint32_t b0 = w.bundle_off[bundle], b1 = w.bundle_off[bundle + 1];
-    const uint32_t c0 = s.bundle_c0[bundle], c1 = s.bundle_c0[bundle + 1];
-    if (c0 >= c1) return;
-    const uint32_t nbs = b1 - b0, ncb = c1 - c0;
-    // pass entries hold a position in kPassShift bits: a bundle with more
-    // contacts runs the sequential sweep, which has no pass table and gives
-    // the same result bit for bit
-    if (ncb > kPassMask) mode = 0;
-
-    float* base = sm + size_t(wid) * warp_smem_words(nbmax);
-    const bool in_smem = nbs <= nbmax;
-    float* V = in_smem ? base : w.vel + size_t(b0) * 3;
-    float* Wv = in_smem ? base + 3 * nbmax : w.omega + size_t(b0) * 3;
-    uint32_t* last = in_smem ? reinterpret_cast<uint32_t*>(base + 6 * nbmax) : s.s_last + b0;
-    float* lam = ncb <= kWarpLamCap ? base + 7 * nbmax : s.s_lam + c0;
-    uint32_t* lvl_sm = reinterpret_cast<uint32_t*>(base + 7 * nbmax + kWarpLamCap);
-    for (uint32_t i = lane; i < nbs; i += 32) {
-        if (in_smem) {
-            st3(V, i, ld3(w.vel, b0 + i));
-            st3(Wv, i, ld3(w.omega, b0 + i));
-        }
-        last[i] = 0;
-    }
-    __syncwarp();
-    BodyView B{V, Wv, nullptr, w.inv_inertia + size_t(b0) * 3, w.inv_mass + b0};
-
-    uint32_t* gpass = s.s_lvl_start + c0 + bundle;
     uint32_t maxl = 0, pos = 0, npass = 0;
     if (mode != 2 && ncb <= 32 * kRegChunks && nbs <= 0x10000u) {
         // ---- register path: each lane keeps its contacts (c0 + lane + 32 k)
@@ -376,7 +360,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
                 if (hit) pk[j] = pos + __popc(m & below);
                 pos += __popc(m);
             }
-            npass = write_passes(gpass, npass, beg, pos, lane);
+            npass = write_passes<kPassWidth>(gpass, npass, beg, pos, lane);
         }
 #pragma unroll
         for (uint32_t j = 0; j < kRegChunks; ++j) {
@@ -465,7 +449,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
         for (int off = 16; off > 0; off >>= 1) maxl = max(maxl, __shfl_xor_sync(full, maxl, off));
 
         // ---- positions: contacts grouped by level, index order within a level;
-        // passes: runs of at most 32 positions of one level (start | count << 26),
+        // passes: runs of at most kPassWidth positions of one level,
         // the unit the lanes solve together.  A pass holds at least one contact,
         // so the passes fit in [c0 + bundle, c1 + bundle] of s_lvl_start.
         for (uint32_t l = 0; l < maxl; ++l) {
@@ -477,7 +461,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
                 if (hit) s.s_order[c0 + pos + __popc(m & ((1u << lane) - 1u))] = c;
                 pos += __popc(m);
             }
-            npass = write_passes(gpass, npass, beg, pos, lane);
+            npass = write_passes<kPassWidth>(gpass, npass, beg, pos, lane);
         }
         __syncwarp();
         for (uint32_t i = lane; i < pos; i += 32) {
@@ -486,16 +470,86 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
             lam[i] = 0.0f;
         }
     }
-    __syncwarp();
+    pos_out = pos;
+    npass_out = npass;
+}
+
+// Barrier of a W-warp block.
+template <uint32_t W>
+__device__ __forceinline__ void block_sync() {
+    if (W == 1)
+        __syncwarp();
+    else
+        __syncthreads();
+}
+
+template <uint32_t W>
+__global__ void __launch_bounds__(32 * W)
+    k_solver_warp(World w, Consts k, Scratch s, uint32_t mode, float dt, uint32_t nbmax) {
+    constexpr uint32_t kSweepThreads = 32 * W;
+    // nbmax: bodies per warp held in shared memory; a bundle with more
+    // bodies (a single scene above the bundle size) solves on the bound
+    // velocity buffers in place
+    extern __shared__ float sm[];
+    if (halted(w.status)) return;  // contacts from a scan that gave up
+    const uint32_t t = threadIdx.x, lane = t & 31u, wid = t >> 5;
+    const uint32_t bundle = blockIdx.x;
+    if (bundle >= w.nbundles) return;
+    const uint32_t b0 = w.bundle_off[bundle], b1 = w.bundle_off[bundle + 1];
+    const uint32_t c0 = s.bundle_c0[bundle], c1 = s.bundle_c0[bundle + 1];
+    if (c0 >= c1) return;
+    const uint32_t nbs = b1 - b0, ncb = c1 - c0;
+    // pass entries hold a position in kPassShift bits: a bundle with more
+    // contacts runs the sequential sweep, which has no pass table and gives
+    // the same result bit for bit
+    if (ncb > kPassMask) mode = 0;
+
+    float* base = sm;
+    const bool in_smem = nbs <= nbmax;
+    float* V = in_smem ? base : w.vel + size_t(b0) * 3;
+    float* Wv = in_smem ? base + 3 * nbmax : w.omega + size_t(b0) * 3;
+    uint32_t* last = in_smem ? reinterpret_cast<uint32_t*>(base + 6 * nbmax) : s.s_last + b0;
+    float* lam = ncb <= kWarpLamCap ? base + 7 * nbmax : s.s_lam + c0;
+    uint32_t* lvl_sm = reinterpret_cast<uint32_t*>(base + 7 * nbmax + kWarpLamCap);
+    for (uint32_t i = t; i < nbs; i += kSweepThreads) {
+        if (in_smem) {
+            st3(V, i, ld3(w.vel, b0 + i));
+            st3(Wv, i, ld3(w.omega, b0 + i));
+        }
+        last[i] = 0;
+    }
+    block_sync<W>();
+    BodyView B{V, Wv, nullptr, w.inv_inertia + size_t(b0) * 3, w.inv_mass + b0};
+
+    uint32_t* gpass = s.s_lvl_start + c0 + bundle;
+    uint32_t pos = 0, npass = 0;
+    if (W == 1) {
+        bundle_setup<kSweepThreads>(w, k, s, B, mode, dt, b0, c0, c1, nbs, ncb, last, lam, gpass,
+                                    lane, pos, npass);
+        __syncwarp();
+    } else {
+        __shared__ uint32_t sh_counts[2];
+        if (wid == 0) {
+            bundle_setup<kSweepThreads>(w, k, s, B, mode, dt, b0, c0, c1, nbs, ncb, last, lam,
+                                        gpass, lane, pos, npass);
+            if (lane == 0) {
+                sh_counts[0] = pos;
+                sh_counts[1] = npass;
+            }
+        }
+        __syncthreads();
+        pos = sh_counts[0];
+        npass = sh_counts[1];
+    }
     const bool pass_sm = npass <= kWarpLevelCap;
     if (pass_sm)
-        for (uint32_t j = lane; j < npass; j += 32) lvl_sm[j] = gpass[j];
-    __syncwarp();
+        for (uint32_t j = t; j < npass; j += kSweepThreads) lvl_sm[j] = gpass[j];
+    block_sync<W>();
     const uint32_t* pass = pass_sm ? lvl_sm : gpass;
 
     // ---- Gauss-Seidel sweeps ----
     if (mode == 0) {
-        if (lane == 0) {
+        if (t == 0) {
             float4 r[kRecWords];
             for (uint32_t it = 0; it < k.pgs_iterations; ++it)
                 for (uint32_t i = 0; i < pos; ++i) {
@@ -507,38 +561,40 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
         // the next pass's records are loaded while this pass solves
         float4 cur[kRecWords], nxt[kRecWords];
         uint32_t pe = pass[0];
-        if (lane < (pe >> kPassShift))
-            load_rec(s.s_rec + size_t(c0 + (pe & kPassMask) + lane) * kRecWords, nxt);
+        if (t < (pe >> kPassShift))
+            load_rec(s.s_rec + size_t(c0 + (pe & kPassMask) + t) * kRecWords, nxt);
         const uint32_t total = k.pgs_iterations * npass;
         uint32_t p = 0;
-        for (uint32_t t = 0; t < total; ++t) {
+        for (uint32_t q = 0; q < total; ++q) {
 #pragma unroll
             for (uint32_t j = 0; j < kRecWords; ++j) cur[j] = nxt[j];
             const uint32_t ce = pe;
             p = p + 1 == npass ? 0u : p + 1;
             pe = pass[p];
-            if (t + 1 < total && lane < (pe >> kPassShift))
-                load_rec(s.s_rec + size_t(c0 + (pe & kPassMask) + lane) * kRecWords, nxt);
-            if (lane < (ce >> kPassShift)) solve_rec(V, Wv, cur, &lam[(ce & kPassMask) + lane]);
-            __syncwarp();
+            if (q + 1 < total && t < (pe >> kPassShift))
+                load_rec(s.s_rec + size_t(c0 + (pe & kPassMask) + t) * kRecWords, nxt);
+            if (t < (ce >> kPassShift)) solve_rec(V, Wv, cur, &lam[(ce & kPassMask) + t]);
+            block_sync<W>();
         }
     }
-    __syncwarp();
+    block_sync<W>();
     // ---- results back to the bound buffers ----
     if (in_smem)
-        for (uint32_t i = lane; i < nbs; i += 32) {
+        for (uint32_t i = t; i < nbs; i += kSweepThreads) {
             st3(w.vel, b0 + i, ld3(V, i));
             st3(w.omega, b0 + i, ld3(Wv, i));
         }
-    for (uint32_t i = lane; i < pos; i += 32) w.lambda[s.s_order[c0 + i]] = lam[i];
+    for (uint32_t i = t; i < pos; i += kSweepThreads) w.lambda[s.s_order[c0 + i]] = lam[i];
 }
 
 constexpr uint32_t kSolverMaxSmem = 160 * 1024;
 
 cudaError_t init_solver() {
-    const cudaError_t e = cudaFuncSetAttribute(
-        k_solver_warp, cudaFuncAttributeMaxDynamicSharedMemorySize,
-        int(kWarpsPerBlock * warp_smem_words(kWarpMaxBodies) * sizeof(float)));
+    const int bytes = int(warp_smem_words(kWarpMaxBodies) * sizeof(float));
+    cudaError_t e = cudaFuncSetAttribute(k_solver_warp<1>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_solver_warp<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e != cudaSuccess) return e;
     // opt in to more than 48 KB of dynamic shared memory; done at handle
     // creation so that no attribute call happens during graph capture
@@ -560,9 +616,11 @@ int launch_solver(const World& w, const Consts& k, const Scratch& s, uint32_t mo
     if (max_scene_bodies <= kWarpMaxBodies) {
         uint32_t nbmax = smem_bodies < max_scene_bodies ? smem_bodies : max_scene_bodies;
         if (nbmax == 0) nbmax = 1;
-        const uint32_t blocks = (w.nbundles + kWarpsPerBlock - 1) / kWarpsPerBlock;
-        const size_t smem = size_t(kWarpsPerBlock) * warp_smem_words(nbmax) * sizeof(float);
-        k_solver_warp<<<blocks, kWarpsPerBlock * 32, smem, st>>>(w, k, s, mode, dt, nbmax);
+        const size_t smem = warp_smem_words(nbmax) * sizeof(float);
+        if (s.sweep_warps >= 2)
+            k_solver_warp<2><<<w.nbundles, 64, smem, st>>>(w, k, s, mode, dt, nbmax);
+        else
+            k_solver_warp<1><<<w.nbundles, 32, smem, st>>>(w, k, s, mode, dt, nbmax);
         return 2;
     }
     if (s.isl.parent) return 1 + launch_solver_islands(w, k, s, mode, dt, st);

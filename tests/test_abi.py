@@ -66,4 +66,8 @@ def test_null_handle_calls_fail_cleanly():
     assert L.lib.seevr_physics_read_counters(None, out) == L.ERR_INVALID_ARGUMENT
     g = L.fptr((0, -9.81, 0), 3)
     assert L.lib.seevr_physics_step(None, 1, 0, 0, 1, 0.1, g, None) == L.ERR_INVALID_ARGUMENT
+    io = L.HostState()
+    assert L.lib.seevr_physics_step_io(None, 1, 0, 0, 1, 0.1, g, C.byref(io), None) == \
+        L.ERR_INVALID_ARGUMENT
+    assert b"io is NULL" in L.lib.seevr_last_error()
     L.lib.seevr_physics_destroy(None)
